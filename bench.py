@@ -1,0 +1,361 @@
+"""Benchmark of the ARS(2,2,2) IMEX step: FP64 zone-updates/s.
+
+Workload: Orszag-Tang vortex, 4096^2 periodic on [0, 2pi)^2, FP64, gamma = 5/3, eta = 1e-4, CFL 0.4
+(dt = 0.9 * min(0.4 * h / s_max, h^2 / (4 eta)), chosen on the device every step). One step is one
+full IMEX step (2 explicit stages, 2 implicit CG solves, finalize). One zone-update is one cell
+advanced by one step. The state (805 MB) exceeds the 126 MB L2, so no flush is needed between steps.
+
+Lines printed (rank 0, one JSON line):
+  default             value = device-resident throughput; e2e = through the C ABI with the state
+                      copied host->device and back every step; roofline of the dominant kernel;
+                      cpu_baseline = the reference's own IMEX step (compiled here) on 1 host core.
+  --impl reference    the reference's CPU implementation (oracle/_ref, compiled from the
+                      reference's headers) on the same workload, a bounded sample per step.
+Multi-GPU: replicas only (independent simulations per rank, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 zone-updates/s per IMEX step"
+UNIT = "zone-updates/s"
+N_GRID = 4096
+ETA = 1e-4
+COURANT = 0.4
+WORKLOAD = "orszag_tang_4096x4096_eta1e-4_cfl0.4"
+
+# Algorithmic bytes per zone of each kernel (compulsory-traffic model of the reference algorithm):
+# stage 1 reads U^n (48), writes the accumulator (48), the predictor (48) and the solve's
+# right-hand side (8) = 152; each CG iteration reads and writes x, r, p = 48; stage 2 reads U1*
+# (48), E1 (8), the accumulator (48), writes U2* (48) and the right-hand side (8) = 160; finalize
+# reads B2* (16), E2 (8), hydro for the CFL (32), writes B^{n+1} (16) = 72.
+# Per step: 384 + 48 * (k1 + k2) bytes per zone.
+ALG_BYTES = {"stage1": 152.0, "stage2": 160.0, "finalize": 72.0, "cg_per_iter": 48.0}
+KERNELS = ("stage1", "cg1", "stage2", "cg2", "finalize")
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_state(n):
+    import magnetohydrodynamics_simulator_b200 as m
+
+    dx = m.problems.grid_spacing(n)
+    return m.problems.orszag_tang(n, n, dx, dx), dx
+
+
+def cpu_reference_step_rate(n, steps, warmup=0):
+    """Time `steps` steps of the reference's own driver loop (oracle/_ref: CFL_condition_checker,
+    generate_A_matrix + compute when dt changes -- every step here -- and IMEX) at n^2, after
+    `warmup` untimed steps; returns (zone-updates/s, seconds). Building the initial state is
+    outside the timed region."""
+    from oracle.oracle import Reference, reference_available
+
+    if not reference_available():
+        return None
+    state, dx = make_state(n)
+    ref = Reference(n, n, dx, dx, ETA)
+    ref.set_state(state)
+    if warmup:
+        ref.run(warmup)
+    t0 = time.perf_counter()
+    ref.run(steps)
+    sec = time.perf_counter() - t0
+    return n * n * steps / sec, sec
+
+
+def run_reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from oracle.oracle import reference_available
+
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmhdref.so was not built "
+                          "(the reference sources were absent when __graft_entry__.build() ran)"}))
+        return 0
+    # Each step is a bounded sample of the workload: one IMEX step of the same Orszag-Tang
+    # problem on the largest grid (<= 4096^2) whose K + 1 steps fit in ~150 s on one core,
+    # sized from a timed 512^2 probe step.
+    probe_rate, _ = cpu_reference_step_rate(512, 1)
+    budget = 150.0
+    n = 4096
+    while n > 256 and (args.steps + 1) * n * n / probe_rate > budget:
+        n //= 2
+    rate, sec = cpu_reference_step_rate(n, args.steps, warmup=min(args.warmup, 1))
+    sample = (f"{args.steps} steps of the reference driver loop (its own CFL dt, matrix rebuilt "
+              f"each step, IMEX) on the Orszag-Tang problem at {n}x{n}, eta 1e-4, after "
+              f"{min(args.warmup, 1)} untimed step; reference headers compiled -O3 -ffast-math, "
+              f"single thread")
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "grid": [N_GRID, N_GRID], "sampled_grid": [n, n],
+                   "eta": ETA, "cfl": COURANT, "parallelism": f"replicas{args.gpus}"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu_arm(args):
+    import torch
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        from datetime import timedelta
+
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    import magnetohydrodynamics_simulator_b200 as m
+
+    n = args.grid
+    state, dx = make_state(n)
+    ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
+    ctx.set_state(state)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        ctx.step(0.0)
+    ctx.synchronize()
+
+    # ---- timed region: K steps, device-resident inputs, CFL dt on the device
+    ctx.lib.mhd_set_kernel_timing(ctx.h, 1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            ctx.step(0.0)
+        stop.record(stream)
+        stop.synchronize()
+    barrier()
+    status = ctx.synchronize_status()
+    ms = start.elapsed_time(stop)
+    import ctypes
+
+    kt = (ctypes.c_double * 5)()
+    ksteps = ctypes.c_longlong()
+    ctx.lib.mhd_kernel_times(ctx.h, kt, ctypes.byref(ksteps))
+    ctx.lib.mhd_set_kernel_timing(ctx.h, 0)
+    prods = ctx.last_cg_products()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    zones = float(n) * n
+    value = world * zones * args.steps / (ms_max * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers: H2D state, step, D2H state per step
+    pinned = [torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy() for _ in range(6)]
+    ctx.get_state_into(pinned)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.set_state(pinned)
+        ctx.step(0.0)
+        ctx.get_state_into(pinned)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * zones * e2e_steps / (e2e_ms * 1e-3)
+    status2 = ctx.synchronize_status()
+
+    # ---- roofline of the dominant kernel (per-kernel CUDA events over the timed region)
+    peak, peak_kind = load_peaks()
+    ksum = dict(zip(KERNELS, list(kt)))
+    steps_rec = max(1, ksteps.value)
+    k1, k2 = prods  # CG products of the last step (reported)
+    # average products over the timed steps are not recorded per step by mhd_step; use the last
+    per_kernel = {}
+    for name in KERNELS:
+        avg_ms = ksum[name] / steps_rec
+        if name == "cg1":
+            alg = ALG_BYTES["cg_per_iter"] * k1
+        elif name == "cg2":
+            alg = ALG_BYTES["cg_per_iter"] * k2
+        else:
+            alg = ALG_BYTES[name]
+        gbs = alg * zones / (avg_ms * 1e-3) / 1e9
+        per_kernel[name] = {"ms": avg_ms, "alg_bytes_per_zone": alg, "achieved_gbs": gbs,
+                            "frac": gbs / peak}
+    dominant = max(KERNELS, key=lambda k: per_kernel[k]["ms"])
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "dram_bytes_per_zone.json")
+    if os.path.exists(tr_path):
+        try:
+            with open(tr_path) as f:
+                tr = json.load(f)
+            key = "cg" if dominant.startswith("cg") else dominant
+            if key in tr:
+                per_zone = tr[key]["bytes_per_zone_per_unit"]
+                units = (k1 if dominant == "cg1" else k2) if key == "cg" else 1
+                traffic = per_zone * units * zones
+        except Exception:
+            traffic = None
+    step_alg = (384.0 + 48.0 * (k1 + k2)) * zones
+    step_ms = ms_max / args.steps
+    roofline = {
+        "bound": "hbm", "kernel": dominant,
+        "achieved": per_kernel[dominant]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+        "frac": per_kernel[dominant]["achieved_gbs"] / peak,
+        "traffic": traffic, "peak_source": peak_kind,
+        "step": {"alg_bytes_per_zone": 384.0 + 48.0 * (k1 + k2),
+                 "achieved": step_alg / (step_ms * 1e-3) / 1e9,
+                 "frac": step_alg / (step_ms * 1e-3) / 1e9 / peak},
+        "kernels": per_kernel,
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_step_rate(n, 1)
+        if r is not None:
+            cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"1 step of the reference driver loop (CFL dt, matrix build, IMEX) "
+                             f"on the same {n}x{n} Orszag-Tang state; reference headers compiled "
+                             f"-O3 -ffast-math, single thread, {r[1]:.1f} s"}
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [n, n], "eta": ETA, "cfl": COURANT,
+                   "parallelism": f"replicas{world}", "l2": "inputs exceed L2 (805 MB state)",
+                   "cg_products_last_step": [k1, k2]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
+                "d2h_bytes_per_step": int(6 * zones * 8), "steps": e2e_steps},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": args.steps * ctx.launches_per_step,
+        "status": [status, status2],
+    }
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=N_GRID)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,142 @@
+/* C ABI of the B200-native ARS(2,2,2) IMEX step for 2-D resistive MHD.
+ *
+ * Drop-in replacement for the hot path of RikibabManos/Magnetohydrodynamics_Simulator: its IMEX()
+ * integrator (include/solvers.hpp:491-613), the implicit matrix set-up (solvers.hpp:404-443 +
+ * ConjugateGradient::compute at src/integrator_main.cpp:58-60, 87-95), the CFL time-step selector
+ * (include/diagnostics.hpp:44-88) and the div B diagnostic (diagnostics.hpp:15-42).
+ *
+ * Conventions
+ *  - All arithmetic is IEEE FP64 on the GPU (sm_100a); there is no CPU fallback.
+ *  - A context owns its device memory; the caller owns every host buffer it passes.
+ *  - Field order everywhere: rho, mx, my, E, bxf, byf (conserved state of Grid.hpp:19-22);
+ *    bxf(i,j) is B_x on the left face of cell (i,j), byf(i,j) is B_y on its bottom face.
+ *  - Host layouts: MHD_LAYOUT_DENSE = nx*ny doubles, row-major (j*nx + i), physical cells only;
+ *    MHD_LAYOUT_PADDED = the reference Grid vectors, (nx+2ng)*(ny+2ng) doubles with the first
+ *    physical cell at (ng, ng) (Grid.hpp:29-62).
+ *  - Every call returns an mhd_status. Calls that enqueue work (mhd_step, mhd_run, ...) are
+ *    asynchronous on the context's stream; conditions found on the device (non-finite state, CG
+ *    not converged, barrier timeout) are reported by mhd_synchronize.
+ *  - Grids are periodic; nx, ny >= 2 (the reference's ghost fill needs two physical cells).
+ */
+#ifndef MHD_B200_H
+#define MHD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MHD_OK = 0,
+    MHD_ERR_INVALID_ARGUMENT = 1,
+    MHD_ERR_CUDA = 2,
+    MHD_ERR_NONFINITE = 3,          /* a NaN/Inf appeared in the state or the CG broke down */
+    MHD_ERR_CG_NOT_CONVERGED = 4,   /* an implicit solve hit its iteration cap */
+    MHD_ERR_TIMEOUT = 5,            /* a grid-wide wait of the persistent CG ran out of time */
+    MHD_ERR_NO_DEVICE = 6,          /* no sm_100 device, or the library was not built for it */
+    MHD_ERR_OUT_OF_MEMORY = 7,
+    MHD_ERR_NO_STATE = 8            /* a state must be set before stepping */
+} mhd_status;
+
+typedef enum { MHD_LAYOUT_DENSE = 0, MHD_LAYOUT_PADDED = 1 } mhd_layout;
+
+/* Corner-velocity test of the upwind constrained transport (solvers.hpp:326,333). The reference
+ * calls an unqualified abs() on a double there, which GCC resolves to int abs(int): the face
+ * fields are averaged whenever |v| < 1. MHD_CT_TRUE_ABS applies the literal |v| < 1e-12. */
+typedef enum { MHD_CT_REFERENCE = 0, MHD_CT_TRUE_ABS = 1 } mhd_ct_mode;
+
+typedef struct {
+    int nx, ny;              /* physical cells (Grid::nx, Grid::ny) */
+    double dx, dy;           /* Grid::cell_width, Grid::cell_height */
+    double eta;              /* Grid::resistivity */
+    int ct_mode;             /* mhd_ct_mode */
+    double cg_tol;           /* <= 0: machine epsilon (Eigen's default) */
+    long long cg_max_iters;  /* <= 0: 2*nx*ny (Eigen's default) */
+    double courant;          /* CFL factor (diagnostics.hpp:82 uses 0.5); <= 0 selects 0.5 */
+    double safety;           /* CFL safety (diagnostics.hpp:84 uses 0.9); <= 0 selects 0.9 */
+    double cg_timeout_s;     /* wall-clock limit of one implicit solve; <= 0 selects 30 s */
+} mhd_params;
+
+typedef struct mhd_context mhd_context;
+
+/* Fill *p with the reference's defaults for an nx*ny grid of cell size dx*dy. */
+mhd_status mhd_default_params(mhd_params* p, int nx, int ny, double dx, double dy, double eta);
+
+/* Allocate the device state and workspace: replaces Grid x3 + integrator_reserved_memory +
+ * ReconstructedValues + the Eigen solver (src/integrator_main.cpp:34-48, solvers.hpp:68-193).
+ * stream: a cudaStream_t (NULL = a new non-blocking stream owned by the context). */
+mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out);
+mhd_status mhd_destroy(mhd_context* ctx);
+
+/* Upload / download the conserved state. The upload applies nothing (no floors); like the
+ * reference driver (integrator_main.cpp:52-53) the first step floors the density. */
+mhd_status mhd_set_state(mhd_context* ctx, const double* const fields[6], int layout, int ng);
+mhd_status mhd_get_state(mhd_context* ctx, double* const fields[6], int layout, int ng);
+/* Same, with device pointers to dense nx*ny planes (device-to-device copies). */
+mhd_status mhd_set_state_device(mhd_context* ctx, const double* const fields[6]);
+mhd_status mhd_get_state_device(mhd_context* ctx, double* const fields[6]);
+
+/* Grid::fillGhostPeriodic + computePrimitives of the current state (Grid.hpp:64-136):
+ * rho (floored), vx, vy, p, bxc, byc; any pointer may be NULL. */
+mhd_status mhd_get_primitives(mhd_context* ctx, double* const prims[6], int layout, int ng);
+
+/* generate_A_matrix(grid, workspace, alpha) + ConjugateGradient::compute (solvers.hpp:404-443,
+ * integrator_main.cpp:58-60): the implicit solves use (I - alpha L) until the next call. Until it
+ * is first called, each step uses alpha = dt * eta * (1 - 1/sqrt 2). */
+mhd_status mhd_set_implicit_coefficient(mhd_context* ctx, double alpha);
+
+/* IMEX(grid, ..., dt) (solvers.hpp:491-613): one ARS(2,2,2) step in place. dt <= 0 takes the
+ * CFL step of the current state instead (computed on the device). Asynchronous. */
+mhd_status mhd_step(mhd_context* ctx, double dt);
+
+/* The driver loop of src/integrator_main.cpp:76-112 on the device: nsteps steps, each with
+ * dt = dt_fixed, or the CFL step when dt_fixed <= 0, clipped so the time does not pass t_end
+ * (t_end <= 0: no clipping); the implicit matrix is regenerated only when dt moved by more than
+ * 1e-10 relative, as the reference driver does. Captured into a CUDA graph. dts_out and
+ * cg_products_out (2 per step), if not NULL, are host arrays filled on return (synchronous). */
+mhd_status mhd_run(mhd_context* ctx, int nsteps, double dt_fixed, double t_end, double* dts_out,
+                   long long* cg_products_out);
+
+/* CFL_condition_checker(grid) (diagnostics.hpp:44-88) with the context's courant/safety. */
+mhd_status mhd_cfl_dt(mhd_context* ctx, double* dt);
+
+/* calculate_current_div_B(grid) (diagnostics.hpp:15-42): RMS and max |div B|. Synchronous. */
+mhd_status mhd_divb(mhd_context* ctx, double* rms, double* maxabs);
+
+/* Wait for the context's stream; return and clear the device-side status (first of:
+ * MHD_ERR_TIMEOUT, MHD_ERR_NONFINITE, MHD_ERR_CG_NOT_CONVERGED). */
+mhd_status mhd_synchronize(mhd_context* ctx);
+
+/* Matrix-vector products of the last step's two implicit solves (after mhd_synchronize). */
+mhd_status mhd_last_cg_products(mhd_context* ctx, long long out[2]);
+
+/* Device planes of the current state (dense nx*ny, valid until the next step). */
+mhd_status mhd_state_device_pointers(mhd_context* ctx, double* out[6]);
+
+/* Record CUDA events around every kernel of the following mhd_step calls (enable != 0), for
+ * per-kernel device times; no counterpart in the reference (which only prints a wall-clock total,
+ * src/integrator_main.cpp:114-120). */
+mhd_status mhd_set_kernel_timing(mhd_context* ctx, int enable);
+
+/* Device time of each kernel summed over the steps recorded since timing was enabled or last read,
+ * in ms: out[0] stage 1, out[1] first implicit solve, out[2] stage 2, out[3] second solve,
+ * out[4] finalize. *steps receives the number of steps. Synchronises; clears the record. */
+mhd_status mhd_kernel_times(mhd_context* ctx, double out_ms[5], long long* steps);
+
+/* The stream the context enqueues on (a cudaStream_t). */
+void* mhd_stream(mhd_context* ctx);
+
+/* Number of kernel launches one mhd_step enqueues (for launch accounting). */
+int mhd_launches_per_step(mhd_context* ctx);
+
+const char* mhd_status_string(mhd_status s);
+
+/* 1 when a device this library was built for is present, else 0. */
+int mhd_device_available(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHD_B200_H */

@@ -1,0 +1,248 @@
+"""ctypes binding of the C ABI in include/mhd_b200.h (libmhd_b200.so, built in-tree).
+
+This is the Python mirror of the drop-in boundary. There is no CPU fallback: if the library or an
+sm_100 device is missing, every entry point raises MHDError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmhd_b200.so")
+
+MHD_OK = 0
+STATUS_NAMES = {
+    0: "MHD_OK",
+    1: "MHD_ERR_INVALID_ARGUMENT",
+    2: "MHD_ERR_CUDA",
+    3: "MHD_ERR_NONFINITE",
+    4: "MHD_ERR_CG_NOT_CONVERGED",
+    5: "MHD_ERR_TIMEOUT",
+    6: "MHD_ERR_NO_DEVICE",
+    7: "MHD_ERR_OUT_OF_MEMORY",
+    8: "MHD_ERR_NO_STATE",
+}
+LAYOUT_DENSE = 0
+LAYOUT_PADDED = 1
+CT_REFERENCE = 0
+CT_TRUE_ABS = 1
+FIELDS = ("rho", "mx", "my", "E", "bxf", "byf")
+PRIMITIVES = ("rho", "vx", "vy", "p", "bxc", "byc")
+
+
+class MHDError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int),
+        ("ny", ctypes.c_int),
+        ("dx", ctypes.c_double),
+        ("dy", ctypes.c_double),
+        ("eta", ctypes.c_double),
+        ("ct_mode", ctypes.c_int),
+        ("cg_tol", ctypes.c_double),
+        ("cg_max_iters", ctypes.c_longlong),
+        ("courant", ctypes.c_double),
+        ("safety", ctypes.c_double),
+        ("cg_timeout_s", ctypes.c_double),
+    ]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libmhd_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MHDError(6, f"{LIB_PATH} is missing (run __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    P6 = _dp * 6
+    lib.mhd_default_params.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.mhd_create.argtypes = [ctypes.POINTER(Params), vp, ctypes.POINTER(vp)]
+    lib.mhd_destroy.argtypes = [vp]
+    lib.mhd_set_state.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
+    lib.mhd_get_state.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
+    lib.mhd_set_state_device.argtypes = [vp, P6]
+    lib.mhd_get_state_device.argtypes = [vp, P6]
+    lib.mhd_get_primitives.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
+    lib.mhd_set_implicit_coefficient.argtypes = [vp, ctypes.c_double]
+    lib.mhd_step.argtypes = [vp, ctypes.c_double]
+    lib.mhd_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp,
+                            ctypes.POINTER(ctypes.c_longlong)]
+    lib.mhd_cfl_dt.argtypes = [vp, _dp]
+    lib.mhd_divb.argtypes = [vp, _dp, _dp]
+    lib.mhd_synchronize.argtypes = [vp]
+    lib.mhd_last_cg_products.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.mhd_state_device_pointers.argtypes = [vp, P6]
+    lib.mhd_stream.argtypes = [vp]
+    lib.mhd_stream.restype = vp
+    lib.mhd_launches_per_step.argtypes = [vp]
+    lib.mhd_status_string.argtypes = [ctypes.c_int]
+    lib.mhd_status_string.restype = ctypes.c_char_p
+    lib.mhd_device_available.argtypes = []
+    _lib = lib
+    return lib
+
+
+def _check(status: int, where: str) -> None:
+    if status != MHD_OK:
+        raise MHDError(status, where)
+
+
+def _host_ptrs(arrays: Sequence[np.ndarray]):
+    arr = (_dp * 6)()
+    for k, a in enumerate(arrays):
+        if a is None:
+            arr[k] = None
+        else:
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("fields must be C-contiguous float64 arrays")
+            arr[k] = a.ctypes.data_as(_dp)
+    return arr
+
+
+def _device_ptrs(ptrs: Sequence[int]):
+    arr = (_dp * 6)()
+    for k, p in enumerate(ptrs):
+        arr[k] = ctypes.cast(ctypes.c_void_p(int(p)), _dp) if p else None
+    return arr
+
+
+def device_available() -> bool:
+    return bool(load_library().mhd_device_available())
+
+
+class Context:
+    """One simulation on the GPU: the device-resident counterpart of the reference's Grid +
+    integrator_reserved_memory + solver objects (src/integrator_main.cpp:34-48)."""
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, eta: float, *, ct_mode: int = 0,
+                 cg_tol: float = 0.0, cg_max_iters: int = 0, courant: float = 0.5,
+                 safety: float = 0.9, cg_timeout_s: float = 30.0, stream: int | None = None):
+        self.lib = load_library()
+        self.nx, self.ny = int(nx), int(ny)
+        p = Params()
+        _check(self.lib.mhd_default_params(ctypes.byref(p), nx, ny, dx, dy, eta), "mhd_default_params")
+        p.ct_mode = ct_mode
+        p.cg_tol = cg_tol
+        p.cg_max_iters = cg_max_iters
+        p.courant = courant
+        p.safety = safety
+        p.cg_timeout_s = cg_timeout_s
+        self.params = p
+        h = ctypes.c_void_p()
+        _check(self.lib.mhd_create(ctypes.byref(p), ctypes.c_void_p(stream) if stream else None,
+                                   ctypes.byref(h)), "mhd_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- state
+    def _shape(self, layout, ng):
+        if layout == LAYOUT_DENSE:
+            return (self.ny, self.nx)
+        return (self.ny + 2 * ng, self.nx + 2 * ng)
+
+    def set_state(self, fields: Sequence[np.ndarray], layout: int = LAYOUT_DENSE, ng: int = 2):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+        for f in fs:
+            if f.shape != self._shape(layout, ng):
+                raise ValueError(f"field shape {f.shape} != {self._shape(layout, ng)}")
+        _check(self.lib.mhd_set_state(self.h, _host_ptrs(fs), layout, ng), "mhd_set_state")
+
+    def get_state(self, layout: int = LAYOUT_DENSE, ng: int = 2):
+        out = [np.empty(self._shape(layout, ng)) for _ in range(6)]
+        _check(self.lib.mhd_get_state(self.h, _host_ptrs(out), layout, ng), "mhd_get_state")
+        return out
+
+    def get_state_into(self, out: Sequence[np.ndarray], layout: int = LAYOUT_DENSE, ng: int = 2):
+        _check(self.lib.mhd_get_state(self.h, _host_ptrs(out), layout, ng), "mhd_get_state")
+
+    def set_state_device(self, ptrs: Sequence[int]):
+        _check(self.lib.mhd_set_state_device(self.h, _device_ptrs(ptrs)), "mhd_set_state_device")
+
+    def get_state_device(self, ptrs: Sequence[int]):
+        _check(self.lib.mhd_get_state_device(self.h, _device_ptrs(ptrs)), "mhd_get_state_device")
+
+    def state_device_pointers(self):
+        arr = (_dp * 6)()
+        _check(self.lib.mhd_state_device_pointers(self.h, arr), "mhd_state_device_pointers")
+        return [ctypes.cast(arr[k], ctypes.c_void_p).value for k in range(6)]
+
+    def primitives(self, layout: int = LAYOUT_DENSE, ng: int = 2):
+        out = [np.empty(self._shape(layout, ng)) for _ in range(6)]
+        _check(self.lib.mhd_get_primitives(self.h, _host_ptrs(out), layout, ng), "mhd_get_primitives")
+        return dict(zip(PRIMITIVES, out))
+
+    # ---------------------------------------------------------------- stepping
+    def set_implicit_coefficient(self, alpha: float):
+        _check(self.lib.mhd_set_implicit_coefficient(self.h, alpha), "mhd_set_implicit_coefficient")
+
+    def step(self, dt: float):
+        _check(self.lib.mhd_step(self.h, dt), "mhd_step")
+
+    def run(self, nsteps: int, dt_fixed: float = 0.0, t_end: float = 0.0, record: bool = True):
+        dts = np.zeros(nsteps) if record else None
+        prods = np.zeros((nsteps, 2), dtype=np.int64) if record else None
+        _check(self.lib.mhd_run(self.h, nsteps, dt_fixed, t_end,
+                                dts.ctypes.data_as(_dp) if record else None,
+                                prods.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)) if record else None),
+               "mhd_run")
+        return dts, prods
+
+    def synchronize(self):
+        _check(self.lib.mhd_synchronize(self.h), "mhd_synchronize")
+
+    def synchronize_status(self) -> int:
+        return int(self.lib.mhd_synchronize(self.h))
+
+    def last_cg_products(self):
+        out = (ctypes.c_longlong * 2)()
+        _check(self.lib.mhd_last_cg_products(self.h, out), "mhd_last_cg_products")
+        return int(out[0]), int(out[1])
+
+    def cfl_dt(self) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.mhd_cfl_dt(self.h, ctypes.byref(v)), "mhd_cfl_dt")
+        return v.value
+
+    def divb(self):
+        rms, mx = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.mhd_divb(self.h, ctypes.byref(rms), ctypes.byref(mx)), "mhd_divb")
+        return rms.value, mx.value
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mhd_stream(self.h) or 0
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self.lib.mhd_launches_per_step(self.h))
+
+
+def ars_gamma() -> float:
+    """ARS(2,2,2) implicit diagonal g = 1 - 1/sqrt(2) (solvers.hpp:41)."""
+    return (2.0 - np.sqrt(2.0)) / 2.0

@@ -1,0 +1,713 @@
+// Host side of the C ABI declared in include/mhd_b200.h: device memory plan, launch sequence of
+// one ARS(2,2,2) step, the CUDA-graph driver loop, diagnostics and status reporting.
+//
+// Device memory of a context (all dense nx*ny FP64 planes, periodic, row-major):
+//   S[6]  current state            (rho, mx, my, E, bxf, byf)
+//   T[6]  predictor U1*            (also scratch for primitives read-back between steps)
+//   A[6]  accumulator -> U2*       (its hydro planes become the next state's: pointers swap)
+//   x, r[2], p[2]                  conjugate-gradient vectors on the corner nodes
+// 23 planes, 184 bytes per cell: 3.1 GB at 4096^2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/mhd_b200.h"
+#include "mhd_kernels.cuh"
+
+using namespace mhd;
+
+namespace {
+
+constexpr int kPlanes = 23;
+
+struct RunRecord {
+    double* dts = nullptr;
+    long long* prods = nullptr;
+    int cap = 0;
+};
+
+}  // namespace
+
+struct mhd_context {
+    mhd_params prm{};
+    Domain dom{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int num_sms = 0;
+    size_t n = 0;
+    double* pool = nullptr;
+    double* S[6]{};
+    double* T[6]{};
+    double* A[6]{};
+    double* x = nullptr;
+    double* r[2]{};
+    double* p[2]{};
+    double* partials = nullptr;
+    CgSync* sync = nullptr;
+    DeviceStatus* status = nullptr;
+    StepCoeffs* coeffs = nullptr;
+    double* divb_partial = nullptr;
+    double* divb_out = nullptr;
+    double* host_pinned = nullptr;  // small read-back area
+    double* padded = nullptr;       // staging for padded-layout transfers
+    size_t padded_elems = 0;
+    int divb_blocks = 0;
+    int st_tiles_x = 0, st_ntiles = 0;
+    int fn_tiles_x = 0, fn_ntiles = 0;
+    int cg_tiles_x = 0, cg_ntiles = 0, cg_grid = 0;
+    size_t stage_smem = 0;
+    bool have_state = false;
+    bool alpha_fixed = false;
+    double alpha = 0.0;
+    RunRecord run;
+    double g = 0.0, d = 0.0;  // ARS(2,2,2) constants
+    // kernel timing: 6 events per recorded step (before stage 1, after each of the 5 kernels)
+    bool timing = false;
+    std::vector<cudaEvent_t> events;
+    size_t events_used = 0;
+};
+
+namespace {
+
+mhd_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return MHD_OK;
+    if (e == cudaErrorMemoryAllocation) return MHD_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ||
+        e == cudaErrorNoKernelImageForDevice)
+        return MHD_ERR_NO_DEVICE;
+    return MHD_ERR_CUDA;
+}
+
+#define MHD_TRY(expr)                                   \
+    do {                                                \
+        cudaError_t _e = (expr);                        \
+        if (_e != cudaSuccess) {                        \
+            if (getenv("MHD_B200_VERBOSE"))             \
+                fprintf(stderr, "mhd_b200: %s: %s\n", #expr, cudaGetErrorString(_e)); \
+            return cuda_status(_e);                     \
+        }                                               \
+    } while (0)
+
+int env_int(const char* name, int def) {
+    const char* v = getenv(name);
+    return v ? atoi(v) : def;
+}
+
+// Request for k_step_coeffs, mirroring the decisions of the reference driver.
+mhd_status launch_coeffs(mhd_context* c, double dt, int alpha_mode, double t_end, double* dts_out) {
+    const double hmin = std::min(c->prm.dx, c->prm.dy);
+    k_step_coeffs<<<1, 1, 0, c->stream>>>(c->coeffs, c->status, dt, c->alpha, alpha_mode, c->prm.eta,
+                                           hmin, c->prm.courant, c->prm.safety, c->g, c->d, t_end,
+                                           dts_out);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status launch_cg(mhd_context* c, const double* bxf, const double* byf, int solve_index,
+                     long long* prods_out) {
+    MHD_TRY(cudaMemsetAsync(c->sync, 0, sizeof(CgSync), c->stream));
+    CgArgs a{};
+    a.D = c->dom;
+    a.C = c->coeffs;
+    a.bxf = bxf;
+    a.byf = byf;
+    a.x = c->x;
+    a.r[0] = c->r[0];
+    a.r[1] = c->r[1];
+    a.p[0] = c->p[0];
+    a.p[1] = c->p[1];
+    a.partials = c->partials;
+    a.sync = c->sync;
+    a.st = c->status;
+    a.solve_index = solve_index;
+    a.tiles_x = c->cg_tiles_x;
+    a.ntiles = c->cg_ntiles;
+    a.max_iters = c->prm.cg_max_iters > 0 ? c->prm.cg_max_iters : 2LL * (long long)c->n;
+    a.tol = c->prm.cg_tol > 0 ? c->prm.cg_tol : 2.220446049250313e-16;
+    a.timeout_s = c->prm.cg_timeout_s;
+    a.prods_out = prods_out;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(c->cg_grid);
+    cfg.blockDim = dim3(CG_NT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_solve, a));
+    return MHD_OK;
+}
+
+CPlanes cplanes(double* const* f) {
+    CPlanes p;
+    for (int k = 0; k < 6; ++k) p.f[k] = f[k];
+    return p;
+}
+Planes planes(double* const* f) {
+    Planes p;
+    for (int k = 0; k < 6; ++k) p.f[k] = f[k];
+    return p;
+}
+
+// Record the next timing event of the current step (no-op unless timing is enabled).
+mhd_status mark(mhd_context* c) {
+    if (!c->timing) return MHD_OK;
+    if (c->events_used == c->events.size()) {
+        cudaEvent_t e;
+        MHD_TRY(cudaEventCreate(&e));
+        c->events.push_back(e);
+    }
+    MHD_TRY(cudaEventRecord(c->events[c->events_used++], c->stream));
+    return MHD_OK;
+}
+
+#define MHD_MARK(c)                          \
+    do {                                     \
+        mhd_status _m = mark(c);             \
+        if (_m != MHD_OK) return _m;         \
+    } while (0)
+
+// The kernels of one step after the coefficients kernel.
+mhd_status enqueue_step_body(mhd_context* c, long long* prods_out) {
+    MHD_MARK(c);
+    k_explicit_stage<1><<<c->st_ntiles, ST_NT, c->stage_smem, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->st_tiles_x);
+    MHD_TRY(cudaGetLastError());
+    MHD_MARK(c);
+    mhd_status s = launch_cg(c, c->T[4], c->T[5], 0, prods_out);
+    if (s != MHD_OK) return s;
+    MHD_MARK(c);
+    k_explicit_stage<2><<<c->st_ntiles, ST_NT, c->stage_smem, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->st_tiles_x);
+    MHD_TRY(cudaGetLastError());
+    MHD_MARK(c);
+    s = launch_cg(c, c->A[4], c->A[5], 1, prods_out);
+    if (s != MHD_OK) return s;
+    MHD_TRY(cudaMemsetAsync(&c->status->smax_bits, 0, sizeof(unsigned long long), c->stream));
+    MHD_MARK(c);
+    k_finalize<<<c->fn_ntiles, FN_NT, 0, c->stream>>>(c->dom, c->coeffs, planes(c->A), c->x,
+                                                       c->S[4], c->S[5], c->status, c->fn_tiles_x);
+    MHD_TRY(cudaGetLastError());
+    MHD_MARK(c);
+    // the accumulator's hydro planes now hold U^{n+1}; the old state's become scratch
+    for (int k = 0; k < 4; ++k) std::swap(c->S[k], c->A[k]);
+    return MHD_OK;
+}
+
+mhd_status refresh_cfl(mhd_context* c) {
+    MHD_TRY(cudaMemsetAsync(&c->status->smax_bits, 0, sizeof(unsigned long long), c->stream));
+    const int blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 8));
+    k_cfl_scan<<<blocks, 256, 0, c->stream>>>(c->dom, cplanes(c->S), c->status);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status ensure_padded(mhd_context* c, int ng) {
+    const size_t need = (size_t)(c->dom.nx + 2 * ng) * (size_t)(c->dom.ny + 2 * ng);
+    if (need <= c->padded_elems) return MHD_OK;
+    if (c->padded) cudaFree(c->padded);
+    c->padded = nullptr;
+    c->padded_elems = 0;
+    MHD_TRY(cudaMalloc(&c->padded, need * sizeof(double)));
+    c->padded_elems = need;
+    return MHD_OK;
+}
+
+// Copy one dense device plane to a host plane in the requested layout.
+mhd_status plane_to_host(mhd_context* c, const double* src, double* dst, int layout, int ng) {
+    const int nx = c->dom.nx, ny = c->dom.ny;
+    if (layout == MHD_LAYOUT_DENSE) {
+        MHD_TRY(cudaMemcpyAsync(dst, src, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        return MHD_OK;
+    }
+    mhd_status s = ensure_padded(c, ng);
+    if (s != MHD_OK) return s;
+    const size_t np = (size_t)(nx + 2 * ng) * (ny + 2 * ng);
+    k_pad_plane<<<std::max(1, std::min((int)((np + 255) / 256), c->num_sms * 8)), 256, 0, c->stream>>>(
+        src, c->padded, nx, ny, ng);
+    MHD_TRY(cudaGetLastError());
+    MHD_TRY(cudaMemcpyAsync(dst, c->padded, np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    // the staging plane is reused by the next call: finish this copy first
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    return MHD_OK;
+}
+
+mhd_status check_ctx(mhd_context* c) {
+    if (!c) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(c->device));
+    return MHD_OK;
+}
+
+mhd_status status_from_flags(unsigned flags) {
+    if (flags & kStatusTimeout) return MHD_ERR_TIMEOUT;
+    if (flags & kStatusNonFinite) return MHD_ERR_NONFINITE;
+    if (flags & kStatusCgNotConverged) return MHD_ERR_CG_NOT_CONVERGED;
+    return MHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mhd_status_string(mhd_status s) {
+    switch (s) {
+        case MHD_OK: return "ok";
+        case MHD_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case MHD_ERR_CUDA: return "CUDA error";
+        case MHD_ERR_NONFINITE: return "non-finite value in the state or the implicit solve";
+        case MHD_ERR_CG_NOT_CONVERGED: return "implicit solve reached its iteration cap";
+        case MHD_ERR_TIMEOUT: return "implicit solve exceeded its wall-clock limit";
+        case MHD_ERR_NO_DEVICE: return "no sm_100 CUDA device (or library not built for it)";
+        case MHD_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case MHD_ERR_NO_STATE: return "no state set";
+    }
+    return "unknown status";
+}
+
+int mhd_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_finalize) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return 1;
+}
+
+mhd_status mhd_default_params(mhd_params* p, int nx, int ny, double dx, double dy, double eta) {
+    if (!p) return MHD_ERR_INVALID_ARGUMENT;
+    memset(p, 0, sizeof(*p));
+    p->nx = nx;
+    p->ny = ny;
+    p->dx = dx;
+    p->dy = dy;
+    p->eta = eta;
+    p->ct_mode = MHD_CT_REFERENCE;
+    p->cg_tol = 0.0;
+    p->cg_max_iters = 0;
+    p->courant = 0.5;
+    p->safety = 0.9;
+    p->cg_timeout_s = 30.0;
+    return MHD_OK;
+}
+
+mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
+    if (!p || !out) return MHD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (p->nx < 2 || p->ny < 2 || !(p->dx > 0) || !(p->dy > 0) || !(p->eta >= 0) ||
+        (p->ct_mode != 0 && p->ct_mode != 1) || (long long)p->nx * p->ny > (1LL << 31))
+        return MHD_ERR_INVALID_ARGUMENT;
+    if (!mhd_device_available()) return MHD_ERR_NO_DEVICE;
+    mhd_context* c = new (std::nothrow) mhd_context();
+    if (!c) return MHD_ERR_OUT_OF_MEMORY;
+    c->prm = *p;
+    if (!(c->prm.courant > 0)) c->prm.courant = 0.5;
+    if (!(c->prm.safety > 0)) c->prm.safety = 0.9;
+    if (!(c->prm.cg_timeout_s > 0)) c->prm.cg_timeout_s = 30.0;
+    c->dom.nx = p->nx;
+    c->dom.ny = p->ny;
+    c->dom.dx = p->dx;
+    c->dom.dy = p->dy;
+    c->dom.eta = p->eta;
+    c->dom.ct_mode = p->ct_mode;
+    c->n = (size_t)p->nx * (size_t)p->ny;
+    c->g = (2.0 - sqrt(2.0)) / 2.0;       // solvers.hpp:41
+    c->d = 1.0 - (1.0 / (2.0 * c->g));    // solvers.hpp:42
+    auto fail = [&](mhd_status s) {
+        mhd_destroy(c);
+        return s;
+    };
+    if (cudaGetDevice(&c->device) != cudaSuccess) return fail(MHD_ERR_NO_DEVICE);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return fail(MHD_ERR_NO_DEVICE);
+    c->num_sms = prop.multiProcessorCount;
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(MHD_ERR_CUDA);
+        c->own_stream = true;
+    }
+    // tiles
+    c->st_tiles_x = (p->nx + ST_TX - 1) / ST_TX;
+    c->st_ntiles = c->st_tiles_x * ((p->ny + ST_TY - 1) / ST_TY);
+    c->fn_tiles_x = (p->nx + FN_TX - 1) / FN_TX;
+    c->fn_ntiles = c->fn_tiles_x * ((p->ny + FN_TY - 1) / FN_TY);
+    c->cg_tiles_x = (p->nx + CG_TX - 1) / CG_TX;
+    c->cg_ntiles = c->cg_tiles_x * ((p->ny + CG_TY - 1) / CG_TY);
+    c->stage_smem = sizeof(StageSmem);
+    if (cudaFuncSetAttribute(k_explicit_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)c->stage_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_explicit_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)c->stage_smem) != cudaSuccess)
+        return fail(MHD_ERR_CUDA);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_solve, CG_NT, 0) != cudaSuccess ||
+        occ < 1)
+        return fail(MHD_ERR_CUDA);
+    const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 4)));
+    c->cg_grid = std::max(1, std::min(c->cg_ntiles, per_sm * c->num_sms));
+    c->divb_blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 4));
+    // memory
+    if (cudaMalloc(&c->pool, (size_t)kPlanes * c->n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MHD_ERR_OUT_OF_MEMORY);
+    }
+    double* q = c->pool;
+    for (int k = 0; k < 6; ++k) c->S[k] = q + (size_t)k * c->n;
+    q += 6 * c->n;
+    for (int k = 0; k < 6; ++k) c->T[k] = q + (size_t)k * c->n;
+    q += 6 * c->n;
+    for (int k = 0; k < 6; ++k) c->A[k] = q + (size_t)k * c->n;
+    q += 6 * c->n;
+    c->x = q;
+    c->r[0] = q + c->n;
+    c->r[1] = q + 2 * c->n;
+    c->p[0] = q + 3 * c->n;
+    c->p[1] = q + 4 * c->n;
+    if (cudaMalloc(&c->partials, (size_t)2 * c->cg_grid * 4 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->sync, sizeof(CgSync)) != cudaSuccess ||
+        cudaMalloc(&c->status, sizeof(DeviceStatus)) != cudaSuccess ||
+        cudaMalloc(&c->coeffs, sizeof(StepCoeffs)) != cudaSuccess ||
+        cudaMalloc(&c->divb_partial, (size_t)2 * c->divb_blocks * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->divb_out, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&c->host_pinned, 64 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MHD_ERR_OUT_OF_MEMORY);
+    }
+    if (cudaMemsetAsync(c->status, 0, sizeof(DeviceStatus), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->coeffs, 0, sizeof(StepCoeffs), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->pool, 0, (size_t)kPlanes * c->n * sizeof(double), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return fail(MHD_ERR_CUDA);
+    *out = c;
+    return MHD_OK;
+}
+
+mhd_status mhd_destroy(mhd_context* c) {
+    if (!c) return MHD_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->pool);
+    cudaFree(c->partials);
+    cudaFree(c->sync);
+    cudaFree(c->status);
+    cudaFree(c->coeffs);
+    cudaFree(c->divb_partial);
+    cudaFree(c->divb_out);
+    cudaFree(c->padded);
+    cudaFree(c->run.dts);
+    cudaFree(c->run.prods);
+    if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    cudaGetLastError();
+    delete c;
+    return MHD_OK;
+}
+
+void* mhd_stream(mhd_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int mhd_launches_per_step(mhd_context* c) {
+    (void)c;
+    return 6;  // coefficients, stage 1, CG, stage 2, CG, finalize
+}
+
+mhd_status mhd_set_state(mhd_context* c, const double* const f[6], int layout, int ng) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f || (layout != MHD_LAYOUT_DENSE && layout != MHD_LAYOUT_PADDED) ||
+        (layout == MHD_LAYOUT_PADDED && ng < 0))
+        return MHD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k)
+        if (!f[k]) return MHD_ERR_INVALID_ARGUMENT;
+    const int nx = c->dom.nx, ny = c->dom.ny;
+    for (int k = 0; k < 6; ++k) {
+        if (layout == MHD_LAYOUT_DENSE) {
+            MHD_TRY(cudaMemcpyAsync(c->S[k], f[k], c->n * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->stream));
+        } else {
+            const size_t pitch = (size_t)(nx + 2 * ng) * sizeof(double);
+            const double* src = f[k] + (size_t)ng * (nx + 2 * ng) + ng;
+            MHD_TRY(cudaMemcpy2DAsync(c->S[k], (size_t)nx * sizeof(double), src, pitch,
+                                      (size_t)nx * sizeof(double), ny, cudaMemcpyHostToDevice,
+                                      c->stream));
+        }
+    }
+    c->have_state = true;
+    return refresh_cfl(c);
+}
+
+mhd_status mhd_set_state_device(mhd_context* c, const double* const f[6]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k) {
+        if (!f[k]) return MHD_ERR_INVALID_ARGUMENT;
+        MHD_TRY(cudaMemcpyAsync(c->S[k], f[k], c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    }
+    c->have_state = true;
+    return refresh_cfl(c);
+}
+
+mhd_status mhd_get_state(mhd_context* c, double* const f[6], int layout, int ng) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f || (layout != MHD_LAYOUT_DENSE && layout != MHD_LAYOUT_PADDED) ||
+        (layout == MHD_LAYOUT_PADDED && ng < 0))
+        return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    for (int k = 0; k < 6; ++k) {
+        if (!f[k]) continue;
+        s = plane_to_host(c, c->S[k], f[k], layout, ng);
+        if (s != MHD_OK) return s;
+    }
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    return MHD_OK;
+}
+
+mhd_status mhd_get_state_device(mhd_context* c, double* const f[6]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    for (int k = 0; k < 6; ++k) {
+        if (!f[k]) continue;
+        MHD_TRY(cudaMemcpyAsync(f[k], c->S[k], c->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    }
+    return MHD_OK;
+}
+
+mhd_status mhd_state_device_pointers(mhd_context* c, double* out[6]) {
+    if (!c || !out) return MHD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k) out[k] = c->S[k];
+    return MHD_OK;
+}
+
+mhd_status mhd_get_primitives(mhd_context* c, double* const prim[6], int layout, int ng) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!prim || (layout != MHD_LAYOUT_DENSE && layout != MHD_LAYOUT_PADDED) ||
+        (layout == MHD_LAYOUT_PADDED && ng < 0))
+        return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    const int blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 8));
+    k_primitives<<<blocks, 256, 0, c->stream>>>(c->dom, cplanes(c->S), c->T[0], c->T[1], c->T[2],
+                                                 c->T[3], c->T[4], c->T[5]);
+    MHD_TRY(cudaGetLastError());
+    for (int k = 0; k < 6; ++k) {
+        if (!prim[k]) continue;
+        s = plane_to_host(c, c->T[k], prim[k], layout, ng);
+        if (s != MHD_OK) return s;
+    }
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    return MHD_OK;
+}
+
+mhd_status mhd_set_implicit_coefficient(mhd_context* c, double alpha) {
+    if (!c || !(alpha >= 0) || !std::isfinite(alpha)) return MHD_ERR_INVALID_ARGUMENT;
+    c->alpha = alpha;
+    c->alpha_fixed = true;
+    return MHD_OK;
+}
+
+mhd_status mhd_step(mhd_context* c, double dt) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    if (!std::isfinite(dt)) return MHD_ERR_INVALID_ARGUMENT;
+    s = launch_coeffs(c, dt, c->alpha_fixed ? 0 : 1, 0.0, nullptr);
+    if (s != MHD_OK) return s;
+    return enqueue_step_body(c, nullptr);
+}
+
+mhd_status mhd_run(mhd_context* c, int nsteps, double dt_fixed, double t_end, double* dts_out,
+                   long long* prods_out) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    if (nsteps < 0 || !std::isfinite(dt_fixed) || !std::isfinite(t_end)) return MHD_ERR_INVALID_ARGUMENT;
+    if (nsteps == 0) return MHD_OK;
+    if (nsteps > c->run.cap) {
+        cudaFree(c->run.dts);
+        cudaFree(c->run.prods);
+        c->run.dts = nullptr;
+        c->run.prods = nullptr;
+        c->run.cap = 0;
+        MHD_TRY(cudaMalloc(&c->run.dts, (size_t)nsteps * sizeof(double)));
+        MHD_TRY(cudaMalloc(&c->run.prods, (size_t)nsteps * 2 * sizeof(long long)));
+        c->run.cap = nsteps;
+    }
+    // driver state: time, previous dt, step counter (integrator_main.cpp:55-60, 76-95)
+    k_driver_reset<<<1, 1, 0, c->stream>>>(c->coeffs);
+    MHD_TRY(cudaGetLastError());
+    struct TimingOff {  // per-kernel events are recorded by mhd_step only
+        mhd_context* c;
+        bool saved;
+        ~TimingOff() { c->timing = saved; }
+    } timing_off{c, c->timing};
+    c->timing = false;
+    const int mode = c->alpha_fixed ? 0 : 2;
+    auto one_step = [&]() -> mhd_status {
+        mhd_status r = launch_coeffs(c, dt_fixed, mode, t_end, c->run.dts);
+        if (r != MHD_OK) return r;
+        return enqueue_step_body(c, c->run.prods);
+    };
+    // Two consecutive steps form one CUDA graph (the state's hydro planes swap every step, so
+    // a pair returns to the same buffer assignment); it is replayed nsteps/2 times.
+    int done = 0;
+    const bool use_graph = nsteps >= 4 && env_int("MHD_B200_NO_GRAPH", 0) == 0;
+    if (use_graph) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            mhd_status r1 = one_step();
+            mhd_status r2 = (r1 == MHD_OK) ? one_step() : r1;
+            ok = cudaStreamEndCapture(c->stream, &graph) == cudaSuccess && r1 == MHD_OK && r2 == MHD_OK;
+            // the captured launches did not run: undo the two pointer swaps they made
+            if (r1 == MHD_OK) for (int k = 0; k < 4; ++k) std::swap(c->S[k], c->A[k]);
+            if (r2 == MHD_OK) for (int k = 0; k < 4; ++k) std::swap(c->S[k], c->A[k]);
+        }
+        if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (ok) {
+            for (; done + 2 <= nsteps; done += 2) {
+                if (cudaGraphLaunch(exec, c->stream) != cudaSuccess) {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (!ok && done == 0) {
+            // capture not possible here: plain launches below
+        } else if (!ok) {
+            return MHD_ERR_CUDA;
+        }
+    }
+    for (; done < nsteps; ++done) {
+        s = one_step();
+        if (s != MHD_OK) return s;
+    }
+    if (dts_out || prods_out) {
+        if (dts_out)
+            MHD_TRY(cudaMemcpyAsync(dts_out, c->run.dts, (size_t)nsteps * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        if (prods_out)
+            MHD_TRY(cudaMemcpyAsync(prods_out, c->run.prods, (size_t)nsteps * 2 * sizeof(long long),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        MHD_TRY(cudaStreamSynchronize(c->stream));
+    }
+    return MHD_OK;
+}
+
+mhd_status mhd_cfl_dt(mhd_context* c, double* dt) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!dt) return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    MHD_TRY(cudaMemcpyAsync(c->host_pinned, &c->status->smax_bits, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, c->stream));
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    double smaxv;
+    memcpy(&smaxv, c->host_pinned, sizeof(double));
+    // diagnostics.hpp:52-86
+    const double h = std::min(c->prm.dx, c->prm.dy);
+    double dt_res = INFINITY;
+    if (c->prm.eta != 0.0) dt_res = h * h / (4.0 * c->prm.eta);
+    if (!(smaxv > 1e-8)) smaxv = std::max(smaxv, 1e-8);
+    const double dt_hyp = c->prm.courant * h / smaxv;
+    *dt = std::min(dt_hyp, dt_res) * c->prm.safety;
+    return MHD_OK;
+}
+
+mhd_status mhd_divb(mhd_context* c, double* rms, double* maxabs) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    k_divb_partial<<<c->divb_blocks, 256, 0, c->stream>>>(c->dom, c->S[4], c->S[5], c->divb_partial);
+    MHD_TRY(cudaGetLastError());
+    k_divb_final<<<1, 32, 0, c->stream>>>(c->divb_partial, c->divb_blocks, (long long)c->n, c->divb_out);
+    MHD_TRY(cudaGetLastError());
+    MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->divb_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    if (rms) *rms = c->host_pinned[0];
+    if (maxabs) *maxabs = c->host_pinned[1];
+    return MHD_OK;
+}
+
+mhd_status mhd_synchronize(mhd_context* c) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
+                            c->stream));
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    DeviceStatus st;
+    memcpy(&st, c->host_pinned, sizeof(st));
+    if (st.flags) {
+        MHD_TRY(cudaMemsetAsync(&c->status->flags, 0, sizeof(unsigned int), c->stream));
+        MHD_TRY(cudaStreamSynchronize(c->stream));
+    }
+    return status_from_flags(st.flags);
+}
+
+mhd_status mhd_set_kernel_timing(mhd_context* c, int enable) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    c->timing = enable != 0;
+    c->events_used = 0;
+    return MHD_OK;
+}
+
+mhd_status mhd_kernel_times(mhd_context* c, double out_ms[5], long long* steps) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!out_ms) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 5; ++k) out_ms[k] = 0.0;
+    const size_t nsteps = c->events_used / 6;
+    for (size_t st = 0; st < nsteps; ++st) {
+        for (int k = 0; k < 5; ++k) {
+            float ms = 0.f;
+            MHD_TRY(cudaEventElapsedTime(&ms, c->events[6 * st + k], c->events[6 * st + k + 1]));
+            out_ms[k] += ms;
+        }
+    }
+    if (steps) *steps = (long long)nsteps;
+    c->events_used = 0;
+    return MHD_OK;
+}
+
+mhd_status mhd_last_cg_products(mhd_context* c, long long out[2]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!out) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
+                            c->stream));
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    DeviceStatus st;
+    memcpy(&st, c->host_pinned, sizeof(st));
+    out[0] = st.cg_products[0];
+    out[1] = st.cg_products[1];
+    return MHD_OK;
+}
+
+}  // extern "C"

@@ -97,28 +97,40 @@ public:
 
     template <typename It>
     void setFromTriplets(It begin, It end) {
-        std::vector<std::vector<std::pair<int, Scalar>>> colv(static_cast<size_t>(cols_));
+        // counting sort by column (stable: triplets of one column keep their insertion order),
+        // then a stable sort by row inside each column; duplicates are summed in that order
+        const size_t nc = static_cast<size_t>(cols_);
+        std::vector<size_t> start(nc + 1, 0);
+        size_t total = 0;
+        for (It it = begin; it != end; ++it) {
+            ++start[static_cast<size_t>(it->col()) + 1];
+            ++total;
+        }
+        for (size_t c = 0; c < nc; ++c) start[c + 1] += start[c];
+        std::vector<std::pair<int, Scalar>> buf(total);
+        std::vector<size_t> fill(start.begin(), start.end() - 1);
         for (It it = begin; it != end; ++it)
-            colv[static_cast<size_t>(it->col())].emplace_back(it->row(), it->value());
-        outer_.assign(static_cast<size_t>(cols_) + 1, 0);
+            buf[fill[static_cast<size_t>(it->col())]++] = std::make_pair(it->row(), it->value());
+        outer_.assign(nc + 1, 0);
         inner_.clear();
         val_.clear();
-        for (std::ptrdiff_t c = 0; c < cols_; ++c) {
-            auto& v = colv[static_cast<size_t>(c)];
-            std::stable_sort(v.begin(), v.end(),
+        inner_.reserve(total);
+        val_.reserve(total);
+        for (size_t c = 0; c < nc; ++c) {
+            std::stable_sort(buf.begin() + start[c], buf.begin() + start[c + 1],
                              [](const std::pair<int, Scalar>& a, const std::pair<int, Scalar>& b) {
                                  return a.first < b.first;
                              });
-            for (size_t k = 0; k < v.size(); ++k) {
-                if (!inner_.empty() && static_cast<std::ptrdiff_t>(inner_.size()) > outer_[c] &&
-                    inner_.back() == v[k].first) {
-                    val_.back() += v[k].second;  // duplicates are summed
+            for (size_t k = start[c]; k < start[c + 1]; ++k) {
+                if (static_cast<StorageIndex>(inner_.size()) > outer_[c] &&
+                    inner_.back() == buf[k].first) {
+                    val_.back() += buf[k].second;  // duplicates are summed
                 } else {
-                    inner_.push_back(v[k].first);
-                    val_.push_back(v[k].second);
+                    inner_.push_back(buf[k].first);
+                    val_.push_back(buf[k].second);
                 }
             }
-            outer_[static_cast<size_t>(c) + 1] = static_cast<StorageIndex>(inner_.size());
+            outer_[c + 1] = static_cast<StorageIndex>(inner_.size());
         }
     }
     void makeCompressed() {}
