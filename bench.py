@@ -200,7 +200,10 @@ def run_gpu_arm(args):
 
     n = args.grid
     state, dx = make_state(n)
-    ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
+    # wall-clock limit of one implicit solve (a profiler replaying the persistent solver can
+    # lower it so that no replay pass can wait long)
+    cg_timeout = float(os.environ.get("MHD_B200_CG_TIMEOUT_S", "30"))
+    ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT, cg_timeout_s=cg_timeout)
     ctx.set_state(state)
     stream = torch.cuda.ExternalStream(ctx.stream)
 

@@ -173,13 +173,30 @@ def test_decaying_wave_matches_reference(m):
     assert max(errs) <= RUN_TOL, errs
 
 
+def test_decaying_wave_512_matches_oracle(m):
+    """Configured decaying wave at its full 512^2 size (eta = 10, dt = 1e-4), a few steps
+    against the oracle: the CG-dominated path (tens of products per solve)."""
+    n, eta, dt, steps = 512, 10.0, 1e-4, 3
+    ic, dx = m.problems.sine_wave_config(n)
+    orc, ctx = _pair(m, n, n, dx, dx, eta, ic)
+    p_orc = [orc.step(dt) for _ in range(steps)]
+    _, prods = ctx.run(steps, dt_fixed=dt)
+    ctx.synchronize()
+    errs = _errs(ctx.get_state(), orc.get_state(), floor=1e-6)
+    assert max(errs) <= RUN_TOL, errs
+    assert np.max(np.abs(prods - np.array(p_orc))) <= 1
+    assert prods.min() > 30
+
+
 def test_decaying_wave_512_analytic_decay(m):
     """Configured decaying wave: 512^2, eta = 10, dt = 1e-4, 100 steps.
 
-    B is a single Fourier mode, so each step multiplies it by the ARS(2,2,2) (L-stable SDIRK2)
-    amplification factor R(z) of z = -eta * lam * dt, lam the discrete eigenvalue of the
-    staggered Laplacian; R(z)^n must hold to 1e-9, exp(-eta*lam*t) to the scheme's O(dt^2)
-    error (2e-6 here) and the continuous exp(-2 eta t) to the grid's O(dx^2) error (2e-5 here).
+    B is a single Fourier mode of the staggered Laplacian (eigenvalue lam), and the implicit
+    part multiplies it by the ARS(2,2,2) (L-stable SDIRK2) amplification factor R(z),
+    z = -eta*lam*dt, each step. The explicit part adds the HLL flux's numerical diffusion of the
+    tangential field (order c_f * dx^3 * k^4 * t ~ 3e-7 relative here, the same in the
+    reference), so: R(z)^n to 1e-6, exp(-eta*lam*t) to 2e-6 (plus the scheme's O(dt^2) error)
+    and the continuous exp(-2 eta t) to 2e-5 (the grid's O(dx^2) error).
     """
     n, eta, dt, steps = 512, 10.0, 1e-4, 100
     ic, dx = m.problems.sine_wave_config(n)
@@ -195,12 +212,12 @@ def test_decaying_wave_512_analytic_decay(m):
     y1 = 1.0 / (1.0 - g * z)
     R = (1.0 + (1.0 - g) * z * y1) / (1.0 - g * z)
     t = steps * dt
-    assert abs(amp - R**steps) <= 1e-9 * R**steps, (amp, R**steps)
+    assert abs(amp - R**steps) <= 1e-6 * R**steps, (amp, R**steps)
     assert abs(amp - np.exp(-eta * lam * t)) <= 2e-6 * np.exp(-eta * lam * t)
     assert abs(amp - np.exp(-2 * eta * t)) <= 2e-5 * np.exp(-2 * eta * t)
     rms, mx = ctx.divb()
     assert mx <= 1e-12
-    assert prods.min() > 10  # the CG-dominated configuration
+    assert prods.min() > 30  # the CG-dominated configuration
 
 
 def test_orszag_tang_point_symmetry(m):
