@@ -18,7 +18,9 @@
 #include <vector>
 
 #include "../../include/mhd_b200.h"
+#include "mhd_cg_sweep.cuh"
 #include "mhd_kernels.cuh"
+#include "mhd_sweep.cuh"
 
 using namespace mhd;
 
@@ -59,10 +61,10 @@ struct mhd_context {
     double* padded = nullptr;       // staging for padded-layout transfers
     size_t padded_elems = 0;
     int divb_blocks = 0;
-    int st_tiles_x = 0, st_ntiles = 0;
+    SweepGeom sg{};          // explicit-stage sweep geometry
+    int st_blocks = 0;
     int fn_tiles_x = 0, fn_ntiles = 0;
-    int cg_tiles_x = 0, cg_ntiles = 0, cg_grid = 0;
-    size_t stage_smem = 0;
+    int cg_strips_x = 0, cg_seg_h = 0, cg_nwarps = 0, cg_grid = 0;
     bool have_state = false;
     bool alpha_fixed = false;
     double alpha = 0.0;
@@ -113,7 +115,7 @@ mhd_status launch_coeffs(mhd_context* c, double dt, int alpha_mode, double t_end
 mhd_status launch_cg(mhd_context* c, const double* bxf, const double* byf, int solve_index,
                      long long* prods_out) {
     MHD_TRY(cudaMemsetAsync(c->sync, 0, sizeof(CgSync), c->stream));
-    CgArgs a{};
+    CgSweepArgs a{};
     a.D = c->dom;
     a.C = c->coeffs;
     a.bxf = bxf;
@@ -126,16 +128,17 @@ mhd_status launch_cg(mhd_context* c, const double* bxf, const double* byf, int s
     a.partials = c->partials;
     a.sync = c->sync;
     a.st = c->status;
+    a.prods_out = prods_out;
     a.solve_index = solve_index;
-    a.tiles_x = c->cg_tiles_x;
-    a.ntiles = c->cg_ntiles;
+    a.strips_x = c->cg_strips_x;
+    a.seg_h = c->cg_seg_h;
+    a.nwarps = c->cg_nwarps;
     a.max_iters = c->prm.cg_max_iters > 0 ? c->prm.cg_max_iters : 2LL * (long long)c->n;
     a.tol = c->prm.cg_tol > 0 ? c->prm.cg_tol : 2.220446049250313e-16;
     a.timeout_s = c->prm.cg_timeout_s;
-    a.prods_out = prods_out;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(c->cg_grid);
-    cfg.blockDim = dim3(CG_NT);
+    cfg.blockDim = dim3(CGS_NT);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];
@@ -143,7 +146,7 @@ mhd_status launch_cg(mhd_context* c, const double* bxf, const double* byf, int s
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_solve, a));
+    MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_sweep, a));
     return MHD_OK;
 }
 
@@ -179,15 +182,15 @@ mhd_status mark(mhd_context* c) {
 // The kernels of one step after the coefficients kernel.
 mhd_status enqueue_step_body(mhd_context* c, long long* prods_out) {
     MHD_MARK(c);
-    k_explicit_stage<1><<<c->st_ntiles, ST_NT, c->stage_smem, c->stream>>>(
-        c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->st_tiles_x);
+    k_stage_sweep<1><<<c->st_blocks, 32 * SW_WARPS, 0, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->sg);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     mhd_status s = launch_cg(c, c->T[4], c->T[5], 0, prods_out);
     if (s != MHD_OK) return s;
     MHD_MARK(c);
-    k_explicit_stage<2><<<c->st_ntiles, ST_NT, c->stage_smem, c->stream>>>(
-        c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->st_tiles_x);
+    k_stage_sweep<2><<<c->st_blocks, 32 * SW_WARPS, 0, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->sg);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     s = launch_cg(c, c->A[4], c->A[5], 1, prods_out);
@@ -341,25 +344,43 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
             return fail(MHD_ERR_CUDA);
         c->own_stream = true;
     }
-    // tiles
-    c->st_tiles_x = (p->nx + ST_TX - 1) / ST_TX;
-    c->st_ntiles = c->st_tiles_x * ((p->ny + ST_TY - 1) / ST_TY);
+    // Explicit-stage sweep: strips of SW_OUT columns, each split into row segments so that the
+    // warps of one wave cover the grid.
+    {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, 0) !=
+                cudaSuccess ||
+            occ < 1)
+            return fail(MHD_ERR_CUDA);
+        const long long resident = (long long)occ * c->num_sms * SW_WARPS;
+        SweepGeom& g = c->sg;
+        g.strips_x = (p->nx + SW_OUT - 1) / SW_OUT;
+        const int segs = (int)std::max(1LL, resident / g.strips_x);
+        g.seg_h = std::max(env_int("MHD_B200_STAGE_MIN_ROWS", 16), (p->ny + segs - 1) / segs);
+        g.segs_y = (p->ny + g.seg_h - 1) / g.seg_h;
+        g.nwarps = g.strips_x * g.segs_y;
+        c->st_blocks = (g.nwarps + SW_WARPS - 1) / SW_WARPS;
+    }
     c->fn_tiles_x = (p->nx + FN_TX - 1) / FN_TX;
     c->fn_ntiles = c->fn_tiles_x * ((p->ny + FN_TY - 1) / FN_TY);
-    c->cg_tiles_x = (p->nx + CG_TX - 1) / CG_TX;
-    c->cg_ntiles = c->cg_tiles_x * ((p->ny + CG_TY - 1) / CG_TY);
-    c->stage_smem = sizeof(StageSmem);
-    if (cudaFuncSetAttribute(k_explicit_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->stage_smem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_explicit_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->stage_smem) != cudaSuccess)
-        return fail(MHD_ERR_CUDA);
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_solve, CG_NT, 0) != cudaSuccess ||
-        occ < 1)
-        return fail(MHD_ERR_CUDA);
-    const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 4)));
-    c->cg_grid = std::max(1, std::min(c->cg_ntiles, per_sm * c->num_sms));
+    // Implicit solve: one wave of co-resident blocks; strips of 32 corner columns split into row
+    // segments over all of their warps.
+    {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_sweep, CGS_NT, 0) != cudaSuccess ||
+            occ < 1)
+            return fail(MHD_ERR_CUDA);
+        const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 2)));
+        c->cg_strips_x = (p->nx + 31) / 32;
+        const long long rows_total = (long long)c->cg_strips_x * p->ny;
+        // no more blocks than there are rows of work for their warps
+        const long long max_blocks = std::max(1LL, (rows_total + (CGS_NT / 32) * 4 - 1) / ((CGS_NT / 32) * 4));
+        c->cg_grid = (int)std::max(1LL, std::min((long long)per_sm * c->num_sms, max_blocks));
+        const long long warps = (long long)c->cg_grid * (CGS_NT / 32);
+        const int segs = (int)std::max(1LL, warps / c->cg_strips_x);
+        c->cg_seg_h = std::max(4, (p->ny + segs - 1) / segs);
+        c->cg_nwarps = c->cg_strips_x * ((p->ny + c->cg_seg_h - 1) / c->cg_seg_h);
+    }
     c->divb_blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 4));
     // memory
     if (cudaMalloc(&c->pool, (size_t)kPlanes * c->n * sizeof(double)) != cudaSuccess) {

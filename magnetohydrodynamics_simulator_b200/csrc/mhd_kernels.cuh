@@ -1,13 +1,16 @@
-// Device kernels of one ARS(2,2,2) IMEX step (reference: solvers.hpp:491-613 of
-// RikibabManos/Magnetohydrodynamics_Simulator), for sm_100a, FP64.
+// Shared device code of the ARS(2,2,2) IMEX step (reference: solvers.hpp:491-613 of
+// RikibabManos/Magnetohydrodynamics_Simulator), for sm_100a, FP64: parameter blocks, helpers,
+// the bounded grid barrier, the step-coefficient / driver kernel, the finalize kernel and the
+// diagnostics. The explicit stages live in mhd_sweep.cuh, the implicit solve in mhd_cg_sweep.cuh.
 //
 // HBM layout: every field is a dense, row-major nx*ny plane of doubles (index j*nx + i), periodic in
-// both directions; there are no ghost cells in device memory -- halos are gathered into shared
-// memory with periodic index wrap (the reference's ghost fill, Grid.hpp:143-161, is a periodic
-// copy). bxf(i,j) lives on the left face of cell (i,j), byf(i,j) on its bottom face, and the corner
-// field of the implicit solve at the bottom-left corner.
+// both directions; there are no ghost cells in device memory -- halos are read with periodic index
+// wrap (the reference's ghost fill, Grid.hpp:143-161, is a periodic copy). bxf(i,j) lives on the
+// left face of cell (i,j), byf(i,j) on its bottom face, and the corner field of the implicit solve
+// at the bottom-left corner.
 //
-// One step is five kernels:
+// One step is six kernels:
+//   coeffs     dt (given or CFL), stage weights, matrix coefficient
 //   stage<1>   U^n            -> predictor U1* = U^n + dt*g*f1 and accumulator U^n + dt*d*f1
 //   cg         U1*_B          -> corner field E1 of (I - alpha L) E1 = eta J_z(U1*_B)
 //   stage<2>   U1*, E1, acc   -> U2* = acc + dt(1-d) f2(U1) + dt(1-g) g2(B1)   (in place on acc)
@@ -90,9 +93,13 @@ __device__ __forceinline__ int wrap(int i, int n) {
 }
 
 __device__ __forceinline__ unsigned long long global_timer_ns() {
+#if defined(__CUDA_ARCH__)
     unsigned long long t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
+#else
+    return 0;  // host compilation of the kernel sources has no device timer
+#endif
 }
 
 template <int NT>
@@ -130,6 +137,62 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* red) {
             v[k] = s;
         }
     }
+}
+
+// Grid barrier of a cooperatively launched kernel, with a wall-clock limit: returns false when the
+// caller must stop (time ran out here or in another block); the caller then returns without
+// touching shared state again. The counter is zeroed before each launch.
+__device__ __forceinline__ bool grid_barrier(CgSync* sync, unsigned long long& target,
+                                             unsigned long long deadline, int* sflag) {
+    __syncthreads();
+    target += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&sync->count, 1ULL);
+        int ok = 1;
+        while (true) {
+            const unsigned long long c = atomicAdd(&sync->count, 0ULL);
+            if (c >= target) break;
+            if (*(volatile unsigned int*)&sync->error) { ok = 0; break; }
+            if (global_timer_ns() > deadline) {
+                atomicExch(&sync->error, 1u);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        *sflag = ok;
+    }
+    __syncthreads();
+    return *sflag != 0;
+}
+
+// Sum the K partial slots of every block in a fixed order (all blocks get identical sums).
+template <int K>
+__device__ __forceinline__ void reduce_partials(const double* part, int nblocks, double* out,
+                                                double* scal) {
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        double v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = 0.0;
+        for (int b = l; b < nblocks; b += 32) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] += __ldcg(&part[(size_t)b * 4 + k]);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if (l == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) scal[k] = v[k];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = scal[k];
+    __syncthreads();
 }
 
 // ------------------------------------------------------------------------------------------
@@ -183,227 +246,6 @@ __global__ void k_step_coeffs(StepCoeffs* C, const DeviceStatus* st, double dt, 
     if (dts_out) dts_out[C->step] = dt;
     C->step += 1;
     C->t += dt;
-}
-
-// ------------------------------------------------------------------------------------------
-// Explicit stage: fused halo gather -> primitives -> MUSCL x/y -> HLL x/y -> upwind-CT corner
-// Ez -> flux divergence + curl Ez -> Butcher combination.
-//
-// Tile: TX x TY cells, halo 2 (MUSCL needs cells i-2..i+2 for the faces of a 1-cell ring).
-
-constexpr int ST_TX = 32;
-constexpr int ST_TY = 16;
-constexpr int ST_NT = 256;
-constexpr int ST_RW = ST_TX + 4;           // region width (cells)
-constexpr int ST_RH = ST_TY + 4;           // region height
-constexpr int ST_R = ST_RW * ST_RH;        // region cells
-constexpr int ST_BXW = ST_RW + 1;          // bxf region: one extra face column on the right
-constexpr int ST_BX = ST_BXW * ST_RH;
-constexpr int ST_BYH = ST_RH + 1;          // byf region: one extra face row on top
-constexpr int ST_BY = ST_RW * ST_BYH;
-constexpr int ST_FXW = ST_TX + 1, ST_FXH = ST_TY + 2;  // x faces: right faces of cells -1..TX-1
-constexpr int ST_FX = ST_FXW * ST_FXH;
-constexpr int ST_FYW = ST_TX + 2, ST_FYH = ST_TY + 1;  // y faces: top faces of rows -1..TY-1
-constexpr int ST_FY = ST_FYW * ST_FYH;
-constexpr int ST_CW = ST_TX + 1, ST_CH = ST_TY + 1;    // corners 0..TX x 0..TY
-constexpr int ST_C = ST_CW * ST_CH;
-constexpr int ST_XW = ST_RW + 1, ST_XH = ST_RH + 1;    // solved corner field for B1 (stage 2)
-constexpr int ST_X = ST_XW * ST_XH;
-
-struct StageSmem {
-    double rho[ST_R], vx[ST_R], vy[ST_R], p[ST_R], bxc[ST_R], byc[ST_R];
-    double bxf[ST_BX], byf[ST_BY];
-    union {
-        double x[ST_X];  // stage 2: corner field of the first solve (gather phase only)
-        double fx[5][ST_FX];
-    } u;
-    double fy[5][ST_FY];
-    double ez[ST_C];
-    double jz[ST_C];  // stage 2: eta*J_z(B1) at the corners (explicit resistive rate g2)
-};
-
-template <int MODE>
-__global__ void __launch_bounds__(ST_NT, 2)
-k_explicit_stage(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
-                 const double* __restrict__ xsolve, Planes outA, Planes outB, int tiles_x) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& s = *reinterpret_cast<StageSmem*>(smem_raw);
-    const int tid = threadIdx.x;
-    const int tile = blockIdx.x;
-    const int i0 = (tile % tiles_x) * ST_TX;
-    const int j0 = (tile / tiles_x) * ST_TY;
-    const int nx = D.nx, ny = D.ny;
-
-    // ---- gather: hydro and faces over the halo region (periodic wrap)
-    for (int k = tid; k < ST_R; k += ST_NT) {
-        const int jj = k / ST_RW, ii = k - jj * ST_RW;
-        const size_t g = (size_t)wrap(j0 - 2 + jj, ny) * nx + wrap(i0 - 2 + ii, nx);
-        s.rho[k] = in.f[0][g];
-        s.vx[k] = in.f[1][g];  // momenta / energy until the primitives overwrite them
-        s.vy[k] = in.f[2][g];
-        s.p[k] = in.f[3][g];
-    }
-    for (int k = tid; k < ST_BX; k += ST_NT) {
-        const int jj = k / ST_BXW, ii = k - jj * ST_BXW;
-        s.bxf[k] = in.f[4][(size_t)wrap(j0 - 2 + jj, ny) * nx + wrap(i0 - 2 + ii, nx)];
-    }
-    for (int k = tid; k < ST_BY; k += ST_NT) {
-        const int jj = k / ST_RW, ii = k - jj * ST_RW;
-        s.byf[k] = in.f[5][(size_t)wrap(j0 - 2 + jj, ny) * nx + wrap(i0 - 2 + ii, nx)];
-    }
-    if (MODE == 2) {
-        // B1 = U1*_B + dt*g * (rate of the solved corner field), solvers.hpp:484-485, 528-529
-        for (int k = tid; k < ST_X; k += ST_NT) {
-            const int jj = k / ST_XW, ii = k - jj * ST_XW;
-            s.u.x[k] = xsolve[(size_t)wrap(j0 - 2 + jj, ny) * nx + wrap(i0 - 2 + ii, nx)];
-        }
-        __syncthreads();
-        const double cg = C->c_g;
-        for (int k = tid; k < ST_BX; k += ST_NT) {
-            const int jj = k / ST_BXW, ii = k - jj * ST_BXW;
-            const double rate = -(s.u.x[(jj + 1) * ST_XW + ii] - s.u.x[jj * ST_XW + ii]) / D.dy;
-            s.bxf[k] += rate * cg;
-        }
-        for (int k = tid; k < ST_BY; k += ST_NT) {
-            const int jj = k / ST_RW, ii = k - jj * ST_RW;
-            const double rate = (s.u.x[jj * ST_XW + ii + 1] - s.u.x[jj * ST_XW + ii]) / D.dx;
-            s.byf[k] += rate * cg;
-        }
-    }
-    __syncthreads();
-
-    // ---- primitives on the region (Grid.hpp:82-136)
-    for (int k = tid; k < ST_R; k += ST_NT) {
-        const int jj = k / ST_RW, ii = k - jj * ST_RW;
-        const double bx = (s.bxf[jj * ST_BXW + ii] + s.bxf[jj * ST_BXW + ii + 1]) / 2.0;
-        const double by = (s.byf[jj * ST_RW + ii] + s.byf[(jj + 1) * ST_RW + ii]) / 2.0;
-        double rho = s.rho[k];
-        // Stage 2 sees the predictor after its density was floored in place (solvers.hpp:522-523)
-        if (MODE == 2 && rho < kRhoFloor) rho = kRhoFloor;
-        double vx, vy;
-        const double p = primitives(rho, s.vx[k], s.vy[k], s.p[k], bx, by, vx, vy);
-        s.rho[k] = rho;
-        s.vx[k] = vx;
-        s.vy[k] = vy;
-        s.p[k] = p;
-        s.bxc[k] = bx;
-        s.byc[k] = by;
-    }
-    __syncthreads();
-
-    // ---- x faces (solvers.hpp:224-236, 372): L = upper x-extrapolation of cell ii,
-    //      R = lower x-extrapolation of cell ii+1, normal B = bxf of cell ii+1
-    for (int k = tid; k < ST_FX; k += ST_NT) {
-        const int fj = k / ST_FXW, fi = k - fj * ST_FXW;
-        const int jj = fj + 1, ii = fi + 1;
-        const int c = jj * ST_RW + ii;
-        Prim L, R;
-        L.rho = recon_hi(s.rho[c - 1], s.rho[c], s.rho[c + 1]);
-        L.vx = recon_hi(s.vx[c - 1], s.vx[c], s.vx[c + 1]);
-        L.vy = recon_hi(s.vy[c - 1], s.vy[c], s.vy[c + 1]);
-        L.p = recon_hi(s.p[c - 1], s.p[c], s.p[c + 1]);
-        L.by = recon_hi(s.byc[c - 1], s.byc[c], s.byc[c + 1]);
-        R.rho = recon_lo(s.rho[c], s.rho[c + 1], s.rho[c + 2]);
-        R.vx = recon_lo(s.vx[c], s.vx[c + 1], s.vx[c + 2]);
-        R.vy = recon_lo(s.vy[c], s.vy[c + 1], s.vy[c + 2]);
-        R.p = recon_lo(s.p[c], s.p[c + 1], s.p[c + 2]);
-        R.by = recon_lo(s.byc[c], s.byc[c + 1], s.byc[c + 2]);
-        L.bx = R.bx = s.bxf[jj * ST_BXW + ii + 1];
-        const Flux F = hll<0>(L, R);
-        s.u.fx[0][k] = F.rho;
-        s.u.fx[1][k] = F.mx;
-        s.u.fx[2][k] = F.my;
-        s.u.fx[3][k] = F.E;
-        s.u.fx[4][k] = F.bt;
-    }
-    // ---- y faces (solvers.hpp:238-250, 373): D = upper y-extrapolation of cell jj,
-    //      U = lower y-extrapolation of cell jj+1, normal B = byf of cell jj+1
-    for (int k = tid; k < ST_FY; k += ST_NT) {
-        const int fj = k / ST_FYW, fi = k - fj * ST_FYW;
-        const int jj = fj + 1, ii = fi + 1;
-        const int c = jj * ST_RW + ii;
-        const int W = ST_RW;
-        Prim Dn, Up;
-        Dn.rho = recon_hi(s.rho[c - W], s.rho[c], s.rho[c + W]);
-        Dn.vx = recon_hi(s.vx[c - W], s.vx[c], s.vx[c + W]);
-        Dn.vy = recon_hi(s.vy[c - W], s.vy[c], s.vy[c + W]);
-        Dn.p = recon_hi(s.p[c - W], s.p[c], s.p[c + W]);
-        Dn.bx = recon_hi(s.bxc[c - W], s.bxc[c], s.bxc[c + W]);
-        Up.rho = recon_lo(s.rho[c], s.rho[c + W], s.rho[c + 2 * W]);
-        Up.vx = recon_lo(s.vx[c], s.vx[c + W], s.vx[c + 2 * W]);
-        Up.vy = recon_lo(s.vy[c], s.vy[c + W], s.vy[c + 2 * W]);
-        Up.p = recon_lo(s.p[c], s.p[c + W], s.p[c + 2 * W]);
-        Up.bx = recon_lo(s.bxc[c], s.bxc[c + W], s.bxc[c + 2 * W]);
-        Dn.by = Up.by = s.byf[(jj + 1) * ST_RW + ii];
-        const Flux F = hll<1>(Dn, Up);
-        s.fy[0][k] = F.rho;
-        s.fy[1][k] = F.mx;
-        s.fy[2][k] = F.my;
-        s.fy[3][k] = F.E;
-        s.fy[4][k] = F.bt;
-    }
-    __syncthreads();
-
-    // ---- corners (solvers.hpp:294-346); stage 2 also forms eta*J_z(B1) (solvers.hpp:450-461)
-    for (int k = tid; k < ST_C; k += ST_NT) {
-        const int tj = k / ST_CW, ti = k - tj * ST_CW;
-        const double eN = -s.u.fx[4][(tj + 1) * ST_FXW + ti];
-        const double eS = -s.u.fx[4][tj * ST_FXW + ti];
-        const double eE = s.fy[4][tj * ST_FYW + ti + 1];
-        const double eW = s.fy[4][tj * ST_FYW + ti];
-        const int c = (tj + 2) * ST_RW + ti + 2;
-        const double vxc = 0.25 * (s.vx[c] + s.vx[c - 1] + s.vx[c - ST_RW] + s.vx[c - ST_RW - 1]);
-        const double vyc = 0.25 * (s.vy[c] + s.vy[c - 1] + s.vy[c - ST_RW] + s.vy[c - ST_RW - 1]);
-        s.ez[k] = corner_ez(eN, eS, eE, eW, vxc, vyc, D.ct_mode);
-        if (MODE == 2) {
-            const int cb = (tj + 2) * ST_BXW + ti + 2;
-            const int cy = (tj + 2) * ST_RW + ti + 2;
-            const double dBy_dx = (s.byf[cy] - s.byf[cy - 1]) / D.dx;
-            const double dBx_dy = (s.bxf[cb] - s.bxf[cb - ST_BXW]) / D.dy;
-            s.jz[k] = D.eta * (dBy_dx - dBx_dy);
-        }
-    }
-    __syncthreads();
-
-    // ---- cells: rates (solvers.hpp:253-292) and the Butcher combination
-    for (int k = tid; k < ST_TX * ST_TY; k += ST_NT) {
-        const int tj = k / ST_TX, ti = k - tj * ST_TX;
-        const int i = i0 + ti, j = j0 + tj;
-        if (i >= nx || j >= ny) continue;
-        const size_t g = (size_t)j * nx + i;
-        const int xr = (tj + 1) * ST_FXW + ti + 1, xl = xr - 1;
-        const int yt = (tj + 1) * ST_FYW + ti + 1, yb = yt - ST_FYW;
-        double f[6];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            f[q] = -((s.u.fx[q][xr] - s.u.fx[q][xl]) / D.dx + (s.fy[q][yt] - s.fy[q][yb]) / D.dy);
-        const int e = tj * ST_CW + ti;
-        f[4] = -(s.ez[e + ST_CW] - s.ez[e]) / D.dy;
-        f[5] = (s.ez[e + 1] - s.ez[e]) / D.dx;
-        if (MODE == 1) {
-            const double cg = C->c_g, cd = C->c_d;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const double u = in.f[q][g];
-                outA.f[q][g] = u + f[q] * cg;  // predictor (solvers.hpp:512-517)
-                // accumulator from the density-floored U^n (explicit_rhs floors it in place)
-                const double ua = (q == 0 && u < kRhoFloor) ? kRhoFloor : u;
-                outB.f[q][g] = ua + f[q] * cd;  // (solvers.hpp:548-553 / 590-595)
-            }
-        } else {
-            const double c1md = C->c_1md, c1mg = C->c_1mg;
-            double a[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) a[q] = outB.f[q][g] + f[q] * c1md;  // :555-560 / :597-602
-            // explicit resistive rate of B1 (solvers.hpp:484-485 with Ez = eta J_z)
-            const double g2x = -(s.jz[e + ST_CW] - s.jz[e]) / D.dy;
-            const double g2y = (s.jz[e + 1] - s.jz[e]) / D.dx;
-            a[4] += g2x * c1mg;  // :565-566 / :604-605
-            a[5] += g2y * c1mg;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) outB.f[q][g] = a[q];
-        }
-    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -535,319 +377,6 @@ k_cfl_scan(Domain D, CPlanes u, DeviceStatus* st) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Matrix-free conjugate gradient for (I - alpha L) E = eta J_z(B) on the corner nodes
-// (solvers.hpp:404-489), with Eigen's ConjugateGradient defaults: x0 = 0, Jacobi scaling by the
-// (constant) diagonal, stop when |r|^2 < max(tol^2 |b|^2, DBL_MIN), at most max_iters products.
-//
-// One persistent, cooperatively launched kernel runs the whole solve; its grid-wide barriers spin
-// with a wall-clock limit and report a timeout instead of waiting forever. Each iteration has two
-// phases separated by a barrier:
-//   A: p_k = z_k + beta p_{k-1} on the tile and its 1-ring, q = A p_k, partial p.q   (reads r, p)
-//   B: same p_k, q; x += alpha p_k; r_{k+1} = r_k - alpha q; partial r.r, r.z; writes x, r, p
-// r and p are double-buffered (a phase reads the halo of one copy and writes the other).
-// Partial sums go to per-block slots and every block reduces all slots in the same fixed order,
-// so every block takes the same decisions and the result is deterministic.
-
-constexpr int CG_TX = 64, CG_TY = 8, CG_NT = 256;
-constexpr int CG_HW = CG_TX + 2, CG_HH = CG_TY + 2;  // tile + 1-ring
-constexpr int CG_H = CG_HW * CG_HH;
-constexpr int CG_BXW = CG_TX + 2, CG_BXH = CG_TY + 3;  // bxf over [i0-1, i0+TX] x [j0-2, j0+TY]
-constexpr int CG_BYW = CG_TX + 3, CG_BYH = CG_TY + 2;  // byf over [i0-2, i0+TX] x [j0-1, j0+TY]
-
-struct CgSmem {
-    double r[CG_H];
-    double p[CG_H];
-    double bx[CG_BXW * CG_BXH];
-    double by[CG_BYW * CG_BYH];
-    double red[CG_NT / 32 * 4];
-    double scal[8];
-    int flag;
-};
-
-struct CgArgs {
-    Domain D;
-    const StepCoeffs* C;
-    const double* bxf;  // the B* whose corner current forms the right-hand side
-    const double* byf;
-    double* x;
-    double* r[2];
-    double* p[2];
-    double* partials;  // [2][gridDim.x][4]
-    CgSync* sync;
-    DeviceStatus* st;
-    int solve_index;    // 0 or 1 within the step (for reporting)
-    int tiles_x, ntiles;
-    long long max_iters;
-    double tol;
-    double timeout_s;
-    long long* prods_out;  // optional per-step record [step][2], indexed by C->cur
-};
-
-// Grid barrier with a wall-clock limit. Returns false when the solve must stop (timeout here or
-// in another block); the caller then returns without touching memory again.
-__device__ __forceinline__ bool grid_barrier(CgSync* sync, unsigned long long& target,
-                                             unsigned long long deadline, int* sflag) {
-    __syncthreads();
-    target += gridDim.x;
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(&sync->count, 1ULL);
-        int ok = 1;
-        while (true) {
-            const unsigned long long c = atomicAdd(&sync->count, 0ULL);
-            if (c >= target) break;
-            if (*(volatile unsigned int*)&sync->error) { ok = 0; break; }
-            if (global_timer_ns() > deadline) {
-                atomicExch(&sync->error, 1u);
-                ok = 0;
-                break;
-            }
-            __nanosleep(32);
-        }
-        __threadfence();
-        *sflag = ok;
-    }
-    __syncthreads();
-    return *sflag != 0;
-}
-
-// Sum the K partial slots of every block in a fixed order (all blocks get identical sums).
-template <int K>
-__device__ __forceinline__ void reduce_partials(const double* part, int nblocks, double* out,
-                                                double* scal) {
-    if (threadIdx.x < 32) {
-        const int l = threadIdx.x;
-        double v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = 0.0;
-        for (int b = l; b < nblocks; b += 32) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) v[k] += __ldcg(&part[(size_t)b * 4 + k]);
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-        if (l == 0) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) scal[k] = v[k];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) out[k] = scal[k];
-    __syncthreads();
-}
-
-// (A p)_c with the row's entries summed in increasing column order for interior rows
-// (bottom, left, centre, right, top), as the reference's compressed matrix product does.
-__device__ __forceinline__ double apply_row(const double* p, int c, int W, double cx, double cy,
-                                            double diag) {
-    double acc = 0.0;
-    acc += (-cy) * p[c - W];
-    acc += (-cx) * p[c - 1];
-    acc += diag * p[c];
-    acc += (-cx) * p[c + 1];
-    acc += (-cy) * p[c + W];
-    return acc;
-}
-
-// p_k = z_k + beta p_{k-1} with z_k = r_k / diag, rounded step by step (no contraction) so that
-// phases A and B form bit-identical directions.
-__device__ __forceinline__ double next_direction(double invdiag, double r, double beta, double p) {
-    return __dadd_rn(__dmul_rn(invdiag, r), __dmul_rn(beta, p));
-}
-
-__global__ void __launch_bounds__(CG_NT)
-k_cg_solve(CgArgs a) {
-    __shared__ CgSmem s;
-    const int tid = threadIdx.x;
-    const Domain D = a.D;
-    const int nx = D.nx, ny = D.ny;
-    const double alpha_m = a.C->alpha;
-    const double cx = alpha_m / (D.dx * D.dx), cy = alpha_m / (D.dy * D.dy);
-    const double diag = 1 + 2 * (cx + cy);
-    const double invdiag = (diag == 0.0) ? 1.0 : 1.0 / diag;
-    unsigned long long target = 0;
-    const unsigned long long deadline =
-        global_timer_ns() + (unsigned long long)(a.timeout_s * 1e9);
-    const int G = gridDim.x;
-    double* part[2] = {a.partials, a.partials + (size_t)G * 4};
-    int phase = 0;
-
-    // ---- phase A0: b = eta J_z(B*) on the tile + ring; r0 = b; p0 = b/d; q0 = A p0
-    double acc3[3] = {0.0, 0.0, 0.0};  // b.b, b.z, p.q
-    for (int t = blockIdx.x; t < a.ntiles; t += G) {
-        const int i0 = (t % a.tiles_x) * CG_TX, j0 = (t / a.tiles_x) * CG_TY;
-        for (int k = tid; k < CG_BXW * CG_BXH; k += CG_NT) {
-            const int jj = k / CG_BXW, ii = k - jj * CG_BXW;
-            s.bx[k] = a.bxf[(size_t)wrap(j0 - 2 + jj, ny) * nx + wrap(i0 - 1 + ii, nx)];
-        }
-        for (int k = tid; k < CG_BYW * CG_BYH; k += CG_NT) {
-            const int jj = k / CG_BYW, ii = k - jj * CG_BYW;
-            s.by[k] = a.byf[(size_t)wrap(j0 - 1 + jj, ny) * nx + wrap(i0 - 2 + ii, nx)];
-        }
-        __syncthreads();
-        for (int k = tid; k < CG_H; k += CG_NT) {  // corner (i0-1+hi, j0-1+hj)
-            const int hj = k / CG_HW, hi = k - hj * CG_HW;
-            const int cyy = hj * CG_BYW + hi + 1;          // byf(i, j)
-            const int cxx = (hj + 1) * CG_BXW + hi;        // bxf(i, j)
-            const double dBy_dx = (s.by[cyy] - s.by[cyy - 1]) / D.dx;
-            const double dBx_dy = (s.bx[cxx] - s.bx[cxx - CG_BXW]) / D.dy;
-            const double b = D.eta * (dBy_dx - dBx_dy);
-            s.r[k] = b;
-            s.p[k] = __dmul_rn(invdiag, b);
-        }
-        __syncthreads();
-        for (int k = tid; k < CG_TX * CG_TY; k += CG_NT) {
-            const int tj = k / CG_TX, ti = k - tj * CG_TX;
-            if (i0 + ti >= nx || j0 + tj >= ny) continue;
-            const int c = (tj + 1) * CG_HW + ti + 1;
-            const double b = s.r[c], pz = s.p[c];
-            const double q = apply_row(s.p, c, CG_HW, cx, cy, diag);
-            acc3[0] += b * b;
-            acc3[1] += b * pz;
-            acc3[2] += pz * q;
-            a.r[0][(size_t)(j0 + tj) * nx + i0 + ti] = b;
-        }
-        __syncthreads();
-    }
-    block_sum<CG_NT, 3>(acc3, s.red);
-    if (tid == 0) {
-        part[phase & 1][(size_t)blockIdx.x * 4 + 0] = acc3[0];
-        part[phase & 1][(size_t)blockIdx.x * 4 + 1] = acc3[1];
-        part[phase & 1][(size_t)blockIdx.x * 4 + 2] = acc3[2];
-    }
-    if (!grid_barrier(a.sync, target, deadline, &s.flag)) {
-        if (tid == 0 && blockIdx.x == 0) atomicOr(&a.st->flags, (unsigned)kStatusTimeout);
-        return;
-    }
-    double sums[3];
-    reduce_partials<3>(part[phase & 1], G, sums, s.scal);
-    ++phase;
-    const double bb = sums[0];
-    double absNew = sums[1];
-    double pq = sums[2];
-    const double tol = a.tol;
-    const double threshold = smax(tol * tol * bb, 2.2250738585072014e-308);
-    long long products = 0;
-    bool zero_solution = (bb == 0.0) || (bb < threshold);
-    bool breakdown = !isfinite(bb);
-    double rr_final = 0.0;
-    bool converged = zero_solution;
-
-    if (!zero_solution && !breakdown) {
-        double beta = 0.0;  // beta_{k-1}; phase A of k = 0 already done
-        for (long long k = 0; k < a.max_iters; ++k) {
-            const double* rk = a.r[k & 1];
-            double* rk1 = a.r[(k + 1) & 1];
-            const double* pkm1 = a.p[(k + 1) & 1];  // p_{k-1} (unused when k == 0)
-            double* pk = a.p[k & 1];
-            if (k > 0) {
-                // ---- phase A_k: p_k and p.Ap
-                double acc1[1] = {0.0};
-                for (int t = blockIdx.x; t < a.ntiles; t += G) {
-                    const int i0 = (t % a.tiles_x) * CG_TX, j0 = (t / a.tiles_x) * CG_TY;
-                    for (int q = tid; q < CG_H; q += CG_NT) {
-                        const int hj = q / CG_HW, hi = q - hj * CG_HW;
-                        const size_t g = (size_t)wrap(j0 - 1 + hj, ny) * nx + wrap(i0 - 1 + hi, nx);
-                        s.p[q] = next_direction(invdiag, __ldcg(&rk[g]), beta, __ldcg(&pkm1[g]));
-                    }
-                    __syncthreads();
-                    for (int q = tid; q < CG_TX * CG_TY; q += CG_NT) {
-                        const int tj = q / CG_TX, ti = q - tj * CG_TX;
-                        if (i0 + ti >= nx || j0 + tj >= ny) continue;
-                        const int c = (tj + 1) * CG_HW + ti + 1;
-                        acc1[0] += s.p[c] * apply_row(s.p, c, CG_HW, cx, cy, diag);
-                    }
-                    __syncthreads();
-                }
-                block_sum<CG_NT, 1>(acc1, s.red);
-                if (tid == 0) part[phase & 1][(size_t)blockIdx.x * 4] = acc1[0];
-                if (!grid_barrier(a.sync, target, deadline, &s.flag)) {
-                    if (tid == 0 && blockIdx.x == 0) atomicOr(&a.st->flags, (unsigned)kStatusTimeout);
-                    return;
-                }
-                double v[1];
-                reduce_partials<1>(part[phase & 1], G, v, s.scal);
-                ++phase;
-                pq = v[0];
-            }
-            const double alpha = absNew / pq;
-            // ---- phase B_k: updates
-            double acc2[2] = {0.0, 0.0};
-            for (int t = blockIdx.x; t < a.ntiles; t += G) {
-                const int i0 = (t % a.tiles_x) * CG_TX, j0 = (t / a.tiles_x) * CG_TY;
-                for (int q = tid; q < CG_H; q += CG_NT) {
-                    const int hj = q / CG_HW, hi = q - hj * CG_HW;
-                    const size_t g = (size_t)wrap(j0 - 1 + hj, ny) * nx + wrap(i0 - 1 + hi, nx);
-                    const double rv = __ldcg(&rk[g]);
-                    s.r[q] = rv;
-                    s.p[q] = (k == 0) ? __dmul_rn(invdiag, rv)
-                                      : next_direction(invdiag, rv, beta, __ldcg(&pkm1[g]));
-                }
-                __syncthreads();
-                for (int q = tid; q < CG_TX * CG_TY; q += CG_NT) {
-                    const int tj = q / CG_TX, ti = q - tj * CG_TX;
-                    if (i0 + ti >= nx || j0 + tj >= ny) continue;
-                    const int c = (tj + 1) * CG_HW + ti + 1;
-                    const size_t g = (size_t)(j0 + tj) * nx + i0 + ti;
-                    const double pv = s.p[c];
-                    const double qv = apply_row(s.p, c, CG_HW, cx, cy, diag);
-                    const double xv = (k == 0) ? alpha * pv : __ldcg(&a.x[g]) + alpha * pv;
-                    const double rn = s.r[c] - alpha * qv;
-                    a.x[g] = xv;
-                    rk1[g] = rn;
-                    pk[g] = pv;
-                    acc2[0] += rn * rn;
-                    acc2[1] += rn * (invdiag * rn);
-                }
-                __syncthreads();
-            }
-            block_sum<CG_NT, 2>(acc2, s.red);
-            if (tid == 0) {
-                part[phase & 1][(size_t)blockIdx.x * 4 + 0] = acc2[0];
-                part[phase & 1][(size_t)blockIdx.x * 4 + 1] = acc2[1];
-            }
-            if (!grid_barrier(a.sync, target, deadline, &s.flag)) {
-                if (tid == 0 && blockIdx.x == 0) atomicOr(&a.st->flags, (unsigned)kStatusTimeout);
-                return;
-            }
-            double v2[2];
-            reduce_partials<2>(part[phase & 1], G, v2, s.scal);
-            ++phase;
-            ++products;
-            const double rr = v2[0];
-            rr_final = rr;
-            if (!isfinite(rr) || !isfinite(alpha)) { breakdown = true; break; }
-            if (rr < threshold) { converged = true; break; }
-            const double absOld = absNew;
-            absNew = v2[1];
-            beta = absNew / absOld;
-        }
-    }
-    if (zero_solution || breakdown) {
-        // x = 0 (Eigen returns the zero vector when b == 0); on breakdown the field is zeroed
-        // too and the status says so.
-        for (int t = blockIdx.x; t < a.ntiles; t += G) {
-            const int i0 = (t % a.tiles_x) * CG_TX, j0 = (t / a.tiles_x) * CG_TY;
-            for (int q = tid; q < CG_TX * CG_TY; q += CG_NT) {
-                const int tj = q / CG_TX, ti = q - tj * CG_TX;
-                if (i0 + ti >= nx || j0 + tj >= ny) continue;
-                a.x[(size_t)(j0 + tj) * nx + i0 + ti] = 0.0;
-            }
-        }
-    }
-    if (blockIdx.x == 0 && tid == 0) {
-        a.st->cg_products[a.solve_index] = products;
-        if (a.prods_out) a.prods_out[2 * a.C->cur + a.solve_index] = products;
-        a.st->cg_products_total += products;
-        a.st->cg_last_rr[a.solve_index] = (bb > 0.0) ? rr_final / bb : 0.0;
-        if (breakdown) atomicOr(&a.st->flags, (unsigned)(kStatusCgBreakdown | kStatusNonFinite));
-        else if (!converged) atomicOr(&a.st->flags, (unsigned)kStatusCgNotConverged);
-    }
-}
-
-// ------------------------------------------------------------------------------------------
 // Diagnostics
 
 // diagnostics.hpp:15-42: per-block sum of div^2 and max |div| over physical cells.
@@ -919,13 +448,6 @@ k_pad_plane(const double* __restrict__ src, double* __restrict__ dst, int nx, in
         const int pj = (int)(g / W), pi = (int)(g - (size_t)pj * W);
         dst[g] = src[(size_t)wrap(pj - ng, ny) * nx + wrap(pi - ng, nx)];
     }
-}
-
-// Density floor in place (what Grid::computePrimitives does to the stored state).
-__global__ void k_floor_density(double* rho, size_t n) {
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x)
-        if (rho[g] < kRhoFloor) rho[g] = kRhoFloor;
 }
 
 }  // namespace mhd

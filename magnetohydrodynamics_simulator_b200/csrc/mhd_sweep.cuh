@@ -1,0 +1,289 @@
+// Explicit stage as a warp column sweep.
+//
+// A warp owns a strip of SW_OUT = 28 output columns [c0, c0+28): lane l holds column
+// i = c0 - 2 + l (the 2-cell MUSCL halo on each side is covered by lanes 0-1 and 30-31). The warp
+// sweeps the rows of its strip upwards; every quantity that the reference computes on whole
+// planes (solvers.hpp:393-402) is computed here one row at a time, with
+//   * the y-direction stencil (rows c-1 .. c+2) held in registers as a rolling window,
+//   * the x-direction stencil (columns i-1 .. i+2) read from neighbouring lanes by shuffles,
+//   * the next row's loads issued one iteration before they are used.
+// No shared memory and no block-level barrier is used in the sweep.
+//
+// Pipeline at sweep row c (all rows periodic):
+//   arrive  row c+3 of the input (stage 2: B1 = U1*_B + dt*g*rate(E1) of row c+3)
+//   PRIM    row c+2      (Grid.hpp:82-136)
+//   YFACE   top face of row c: HLL of the y-reconstructions of rows c-1..c+2 (solvers.hpp:238-250)
+//   XFACE   right face of column i in row c (solvers.hpp:224-236)
+//   CORNER  corner Ez at the bottom-left of cell (i, c) (solvers.hpp:294-346)
+//   OUT     hydro rates of row c, B rates of row c-1 (solvers.hpp:253-292) + Butcher weights
+// Lane validity: PRIM lanes 0-31, XFACE lanes 1-29, YFACE lanes 0-30, CORNER lanes 2-30, outputs
+// lanes 2-29; other lanes compute values that are never used.
+#pragma once
+
+#include "mhd_kernels.cuh"
+
+namespace mhd {
+
+constexpr int SW_OUT = 28;       // output columns per warp
+constexpr int SW_WARPS = 4;      // warps (independent strips) per block
+constexpr int SW_PRE = 5;        // rows swept before the first output row of a strip
+
+struct SweepGeom {
+    int strips_x;  // column strips
+    int seg_h;     // rows per strip segment
+    int segs_y;    // segments per column strip
+    int nwarps;    // strips_x * segs_y
+};
+
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+#ifndef MHD_SWEEP_MIN_BLOCKS
+#define MHD_SWEEP_MIN_BLOCKS 2  // 2 blocks of 4 warps per SM: ~200 registers, no spills
+#endif
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * SW_WARPS, MHD_SWEEP_MIN_BLOCKS)
+k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
+              const double* __restrict__ xsolve, Planes outA, Planes outB, SweepGeom G) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
+    if (w >= G.nwarps) return;
+    const int nx = D.nx, ny = D.ny;
+    const int sx = w % G.strips_x, sy = w / G.strips_x;
+    const int c0 = sx * SW_OUT;
+    const int r0 = sy * G.seg_h;
+    const int r1 = min(r0 + G.seg_h, ny);
+    if (r0 >= r1) return;
+    const int i = c0 - 2 + lane;
+    const int iw = wrap(i, nx);
+    const bool out_lane = lane >= 2 && lane < 2 + SW_OUT && i < nx;
+    const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
+    const double cg = C->c_g;
+    const double cA = (MODE == 1) ? C->c_g : C->c_1md;   // outA weight (stage 1: predictor)
+    const double cB = (MODE == 1) ? C->c_d : C->c_1md;   // outB weight
+    const double c1mg = C->c_1mg;
+    // column of the lane to the right (for stage 2's B1 of lane 31)
+    const int iw_r = wrap(i + 1, nx);
+
+    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
+
+    // ---- windows (index 0 = oldest row)
+    double Prho[4], Pvx[4], Pvy[4], Pp[4], Pbxc[4];  // rows c-1 .. c+2
+    double Pbyc[3];                                   // rows c .. c+2
+    double Wbx[5];                                    // bxf rows c-1 .. c+3 (B1 in stage 2)
+    double Wby[5];                                    // byf rows c-1 .. c+3
+    double bxr_prev = 0.0;                            // bxf(i+1) of row c+2 (cell-centred bx)
+    double pend[4];                                   // conserved hydro of row c+2
+    double arr[6];                                    // arriving input row (c+3)
+    double arr_bxr = 0.0;                             // lane 31: bxf one column to the right
+    double ax_cur = 0.0, ax_nxt = 0.0;                // stage 2: E1 rows c+3, c+4
+    double axr_cur = 0.0, axr_nxt = 0.0;              // lane 31: E1 one column to the right
+    double fy_prev[5];                                // y-face flux of row c-1
+    double fxbt_prev = 0.0, ez_prev = 0.0, jz_prev = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; pend[k] = 0.0; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Pbyc[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) { Wbx[k] = 0.0; Wby[k] = 0.0; fy_prev[k] = 0.0; }
+
+    const int cstart = r0 - SW_PRE;
+    // preload: input row cstart+3 arrives at the first iteration; E1 rows one ahead
+    {
+        const size_t rp = rowp(cstart + 3);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) arr[q] = __ldg(&in.f[q][rp + iw]);
+        arr_bxr = (lane == 31) ? __ldg(&in.f[4][rp + iw_r]) : 0.0;
+        if (MODE == 2) {
+            ax_cur = __ldg(&xsolve[rp + iw]);
+            axr_cur = (lane == 31) ? __ldg(&xsolve[rp + iw_r]) : 0.0;
+            const size_t rn = rowp(cstart + 4);
+            ax_nxt = __ldg(&xsolve[rn + iw]);
+            axr_nxt = (lane == 31) ? __ldg(&xsolve[rn + iw_r]) : 0.0;
+        }
+    }
+
+    for (int c = cstart; c <= r1; ++c) {
+        // ---- arrive row c+3; issue the loads of row c+4 (and E1 row c+5)
+        double a[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) a[q] = arr[q];
+        const double a_bxr = arr_bxr;
+        double ax0 = ax_cur, ax1 = ax_nxt, axr0 = axr_cur, axr1 = axr_nxt;
+        {
+            const size_t rp = rowp(c + 4);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) arr[q] = __ldg(&in.f[q][rp + iw]);
+            arr_bxr = (lane == 31) ? __ldg(&in.f[4][rp + iw_r]) : 0.0;
+            if (MODE == 2) {
+                ax_cur = ax_nxt;
+                axr_cur = axr_nxt;
+                const size_t rn = rowp(c + 5);
+                ax_nxt = __ldg(&xsolve[rn + iw]);
+                axr_nxt = (lane == 31) ? __ldg(&xsolve[rn + iw_r]) : 0.0;
+            }
+        }
+        // ---- B faces of row c+3 (and bxf one column to the right, for the cell-centred bx;
+        //      lane 31 has its own copy of that column)
+        double bx3 = a[4], by3 = a[5];
+        double bxr3 = a_bxr;
+        if (MODE == 2) {
+            // B1 = U1*_B + dt*g*(rate of E1) (solvers.hpp:484-485, 528-529)
+            double axr = shdn(ax0, 1);
+            if (lane == 31) axr = axr0;
+            const double rbx = -(ax1 - ax0) / D.dy;
+            const double rby = (axr - ax0) / D.dx;
+            bx3 += rbx * cg;
+            by3 += rby * cg;
+            if (lane == 31) bxr3 += (-(axr1 - axr0) / D.dy) * cg;
+        }
+        {
+            const double right = shdn(bx3, 1);
+            if (lane != 31) bxr3 = right;
+        }
+        // shift the face windows: new row c+3 enters at index 4
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { Wbx[k] = Wbx[k + 1]; Wby[k] = Wby[k + 1]; }
+        Wbx[4] = bx3;
+        Wby[4] = by3;
+
+        // ---- PRIM row c+2 (faces: bxf rows index 3, byf rows index 3 and 4)
+        double nrho, nvx, nvy, np, nbxc, nbyc;
+        {
+            nbxc = (Wbx[3] + bxr_prev) / 2.0;
+            nbyc = (Wby[3] + Wby[4]) / 2.0;
+            double rho = pend[0];
+            if (MODE == 2 && rho < kRhoFloor) rho = kRhoFloor;  // floored in place (solvers.hpp:522-523)
+            np = primitives(rho, pend[1], pend[2], pend[3], nbxc, nbyc, nvx, nvy);
+            nrho = rho;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) pend[q] = a[q];  // conserved row c+3 becomes the next PRIM input
+        bxr_prev = bxr3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            Prho[k] = Prho[k + 1]; Pvx[k] = Pvx[k + 1]; Pvy[k] = Pvy[k + 1];
+            Pp[k] = Pp[k + 1]; Pbxc[k] = Pbxc[k + 1];
+        }
+        Prho[3] = nrho; Pvx[3] = nvx; Pvy[3] = nvy; Pp[3] = np; Pbxc[3] = nbxc;
+        Pbyc[0] = Pbyc[1]; Pbyc[1] = Pbyc[2]; Pbyc[2] = nbyc;
+        // window rows now: P*[0..3] = c-1 .. c+2, Pbyc[0..2] = c .. c+2,
+        //                  Wbx/Wby[0..4] = c-1 .. c+3
+
+        // ---- YFACE: top face of (i, c); D = upper y-extrapolation of row c, U = lower of c+1
+        Flux fy;
+        {
+            Prim Dn, Up;
+            Dn.rho = recon_hi(Prho[0], Prho[1], Prho[2]);
+            Dn.vx = recon_hi(Pvx[0], Pvx[1], Pvx[2]);
+            Dn.vy = recon_hi(Pvy[0], Pvy[1], Pvy[2]);
+            Dn.p = recon_hi(Pp[0], Pp[1], Pp[2]);
+            Dn.bx = recon_hi(Pbxc[0], Pbxc[1], Pbxc[2]);
+            Up.rho = recon_lo(Prho[1], Prho[2], Prho[3]);
+            Up.vx = recon_lo(Pvx[1], Pvx[2], Pvx[3]);
+            Up.vy = recon_lo(Pvy[1], Pvy[2], Pvy[3]);
+            Up.p = recon_lo(Pp[1], Pp[2], Pp[3]);
+            Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
+            Dn.by = Up.by = Wby[2];  // byf of row c+1
+            fy = hll<1>(Dn, Up);
+        }
+        // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of i+1
+        Flux fx;
+        {
+            const double r_m = shup(Prho[1], 1), r_p = shdn(Prho[1], 1), r_pp = shdn(Prho[1], 2);
+            const double u_m = shup(Pvx[1], 1), u_p = shdn(Pvx[1], 1), u_pp = shdn(Pvx[1], 2);
+            const double v_m = shup(Pvy[1], 1), v_p = shdn(Pvy[1], 1), v_pp = shdn(Pvy[1], 2);
+            const double p_m = shup(Pp[1], 1), p_p = shdn(Pp[1], 1), p_pp = shdn(Pp[1], 2);
+            const double b_m = shup(Pbyc[0], 1), b_p = shdn(Pbyc[0], 1), b_pp = shdn(Pbyc[0], 2);
+            Prim L, R;
+            L.rho = recon_hi(r_m, Prho[1], r_p);
+            L.vx = recon_hi(u_m, Pvx[1], u_p);
+            L.vy = recon_hi(v_m, Pvy[1], v_p);
+            L.p = recon_hi(p_m, Pp[1], p_p);
+            L.by = recon_hi(b_m, Pbyc[0], b_p);
+            R.rho = recon_lo(Prho[1], r_p, r_pp);
+            R.vx = recon_lo(Pvx[1], u_p, u_pp);
+            R.vy = recon_lo(Pvy[1], v_p, v_pp);
+            R.p = recon_lo(Pp[1], p_p, p_pp);
+            R.by = recon_lo(Pbyc[0], b_p, b_pp);
+            L.bx = R.bx = shdn(Wbx[1], 1);  // bxf(i+1, c)
+            fx = hll<0>(L, R);
+        }
+        // ---- CORNER (i, c): eN = -Fx^By(i-1, c), eS = -Fx^By(i-1, c-1), eE = Fy^Bx(i, c-1),
+        //      eW = Fy^Bx(i-1, c-1); corner velocity = mean of the 4 cells
+        double ez;
+        {
+            const double eN = -shup(fx.bt, 1);
+            const double eS = -shup(fxbt_prev, 1);
+            const double eE = fy_prev[4];
+            const double eW = shup(fy_prev[4], 1);
+            const double vxc = 0.25 * (Pvx[1] + shup(Pvx[1], 1) + Pvx[0] + shup(Pvx[0], 1));
+            const double vyc = 0.25 * (Pvy[1] + shup(Pvy[1], 1) + Pvy[0] + shup(Pvy[0], 1));
+            ez = corner_ez(eN, eS, eE, eW, vxc, vyc, D.ct_mode);
+        }
+        double jz = 0.0;
+        if (MODE == 2) {  // eta*J_z(B1) at corner (i, c) (solvers.hpp:450-461)
+            const double dBy_dx = (Wby[1] - shup(Wby[1], 1)) / D.dx;
+            const double dBx_dy = (Wbx[1] - Wbx[0]) / D.dy;
+            jz = D.eta * (dBy_dx - dBx_dy);
+        }
+        // ---- hydro rates of row c
+        {
+            double f[4];
+            f[0] = -((fx.rho - shup(fx.rho, 1)) * idx + (fy.rho - fy_prev[0]) * idy);
+            f[1] = -((fx.mx - shup(fx.mx, 1)) * idx + (fy.mx - fy_prev[1]) * idy);
+            f[2] = -((fx.my - shup(fx.my, 1)) * idx + (fy.my - fy_prev[2]) * idy);
+            f[3] = -((fx.E - shup(fx.E, 1)) * idx + (fy.E - fy_prev[3]) * idy);
+            if (out_lane && c >= r0 && c < r1) {
+                const size_t g = (size_t)c * nx + i;
+                if (MODE == 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const double u = __ldg(&in.f[q][g]);
+                        outA.f[q][g] = u + f[q] * cA;                       // predictor
+                        const double ua = (q == 0 && u < kRhoFloor) ? kRhoFloor : u;
+                        outB.f[q][g] = ua + f[q] * cB;                      // accumulator
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) outB.f[q][g] = outB.f[q][g] + f[q] * cB;
+                }
+            }
+        }
+        // ---- B rates of row c-1: -(Ez(i, c) - Ez(i, c-1))/dy, (Ez(i+1, c-1) - Ez(i, c-1))/dx
+        {
+            const double fbx = -(ez - ez_prev) * idy;
+            const double fby = (shdn(ez_prev, 1) - ez_prev) * idx;
+            double g2x = 0.0, g2y = 0.0;
+            if (MODE == 2) {
+                g2x = -(jz - jz_prev) / D.dy;
+                g2y = (shdn(jz_prev, 1) - jz_prev) / D.dx;
+            }
+            if (out_lane && c - 1 >= r0 && c - 1 < r1) {
+                const size_t g = (size_t)(c - 1) * nx + i;
+                if (MODE == 1) {
+                    const double ubx = Wbx[0], uby = Wby[0];  // U^n faces of row c-1
+                    outA.f[4][g] = ubx + fbx * cA;
+                    outA.f[5][g] = uby + fby * cA;
+                    outB.f[4][g] = ubx + fbx * cB;
+                    outB.f[5][g] = uby + fby * cB;
+                } else {
+                    double ax = outB.f[4][g] + fbx * cB;
+                    double ay = outB.f[5][g] + fby * cB;
+                    ax += g2x * c1mg;
+                    ay += g2y * c1mg;
+                    outB.f[4][g] = ax;
+                    outB.f[5][g] = ay;
+                }
+            }
+        }
+        // ---- carry to the next row
+        fy_prev[0] = fy.rho; fy_prev[1] = fy.mx; fy_prev[2] = fy.my; fy_prev[3] = fy.E; fy_prev[4] = fy.bt;
+        fxbt_prev = fx.bt;
+        ez_prev = ez;
+        jz_prev = jz;
+    }
+}
+
+}  // namespace mhd
