@@ -20,6 +20,7 @@
 #include "../../include/mhd_b200.h"
 #include "mhd_cg_sweep.cuh"
 #include "mhd_kernels.cuh"
+#include "mhd_finalize_sweep.cuh"
 #include "mhd_sweep.cuh"
 
 using namespace mhd;
@@ -61,9 +62,10 @@ struct mhd_context {
     double* padded = nullptr;       // staging for padded-layout transfers
     size_t padded_elems = 0;
     int divb_blocks = 0;
-    SweepGeom sg{};          // explicit-stage sweep geometry
-    int st_blocks = 0;
-    int fn_tiles_x = 0, fn_ntiles = 0;
+    SweepGeom sg[2]{};       // explicit-stage sweep geometry (stage 1, stage 2)
+    int st_blocks[2]{};
+    SweepGeom fg{};          // finalize sweep geometry
+    int fn_blocks = 0;
     int cg_strips_x = 0, cg_seg_h = 0, cg_nwarps = 0, cg_grid = 0;
     bool have_state = false;
     bool alpha_fixed = false;
@@ -182,23 +184,23 @@ mhd_status mark(mhd_context* c) {
 // The kernels of one step after the coefficients kernel.
 mhd_status enqueue_step_body(mhd_context* c, long long* prods_out) {
     MHD_MARK(c);
-    k_stage_sweep<1><<<c->st_blocks, 32 * SW_WARPS, 0, c->stream>>>(
-        c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->sg);
+    k_stage_sweep<1><<<c->st_blocks[0], 32 * SW_WARPS, 0, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->sg[0]);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     mhd_status s = launch_cg(c, c->T[4], c->T[5], 0, prods_out);
     if (s != MHD_OK) return s;
     MHD_MARK(c);
-    k_stage_sweep<2><<<c->st_blocks, 32 * SW_WARPS, 0, c->stream>>>(
-        c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->sg);
+    k_stage_sweep<2><<<c->st_blocks[1], 32 * SW_WARPS, 0, c->stream>>>(
+        c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->sg[1]);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     s = launch_cg(c, c->A[4], c->A[5], 1, prods_out);
     if (s != MHD_OK) return s;
     MHD_TRY(cudaMemsetAsync(&c->status->smax_bits, 0, sizeof(unsigned long long), c->stream));
     MHD_MARK(c);
-    k_finalize<<<c->fn_ntiles, FN_NT, 0, c->stream>>>(c->dom, c->coeffs, planes(c->A), c->x,
-                                                       c->S[4], c->S[5], c->status, c->fn_tiles_x);
+    k_finalize_sweep<<<c->fn_blocks, 32 * FS_WARPS, 0, c->stream>>>(
+        c->dom, c->coeffs, planes(c->A), c->x, c->S[4], c->S[5], c->status, c->fg);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     // the accumulator's hydro planes now hold U^{n+1}; the old state's become scratch
@@ -346,23 +348,36 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
     }
     // Explicit-stage sweep: strips of SW_OUT columns, each split into row segments so that the
     // warps of one wave cover the grid.
-    {
+    for (int mode = 0; mode < 2; ++mode) {
         int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, 0) !=
-                cudaSuccess ||
-            occ < 1)
-            return fail(MHD_ERR_CUDA);
+        const cudaError_t e = mode == 0
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<1>, 32 * SW_WARPS, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, 0);
+        if (e != cudaSuccess || occ < 1) return fail(MHD_ERR_CUDA);
         const long long resident = (long long)occ * c->num_sms * SW_WARPS;
-        SweepGeom& g = c->sg;
+        SweepGeom& g = c->sg[mode];
         g.strips_x = (p->nx + SW_OUT - 1) / SW_OUT;
         const int segs = (int)std::max(1LL, resident / g.strips_x);
         g.seg_h = std::max(env_int("MHD_B200_STAGE_MIN_ROWS", 16), (p->ny + segs - 1) / segs);
         g.segs_y = (p->ny + g.seg_h - 1) / g.seg_h;
         g.nwarps = g.strips_x * g.segs_y;
-        c->st_blocks = (g.nwarps + SW_WARPS - 1) / SW_WARPS;
+        c->st_blocks[mode] = (g.nwarps + SW_WARPS - 1) / SW_WARPS;
     }
-    c->fn_tiles_x = (p->nx + FN_TX - 1) / FN_TX;
-    c->fn_ntiles = c->fn_tiles_x * ((p->ny + FN_TY - 1) / FN_TY);
+    {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_finalize_sweep, 32 * FS_WARPS, 0) !=
+                cudaSuccess ||
+            occ < 1)
+            return fail(MHD_ERR_CUDA);
+        const long long resident = (long long)occ * c->num_sms * FS_WARPS;
+        SweepGeom& g = c->fg;
+        g.strips_x = (p->nx + FS_OUT - 1) / FS_OUT;
+        const int segs = (int)std::max(1LL, resident / g.strips_x);
+        g.seg_h = std::max(16, (p->ny + segs - 1) / segs);
+        g.segs_y = (p->ny + g.seg_h - 1) / g.seg_h;
+        g.nwarps = g.strips_x * g.segs_y;
+        c->fn_blocks = (g.nwarps + FS_WARPS - 1) / FS_WARPS;
+    }
     // Implicit solve: one wave of co-resident blocks; strips of 32 corner columns split into row
     // segments over all of their warps.
     {
@@ -370,7 +385,7 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_sweep, CGS_NT, 0) != cudaSuccess ||
             occ < 1)
             return fail(MHD_ERR_CUDA);
-        const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 2)));
+        const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 1)));
         c->cg_strips_x = (p->nx + 31) / 32;
         const long long rows_total = (long long)c->cg_strips_x * p->ny;
         // no more blocks than there are rows of work for their warps

@@ -20,7 +20,7 @@
 
 namespace mhd {
 
-constexpr int CGS_NT = 512;  // threads per block (16 warps)
+constexpr int CGS_NT = 512;  // threads per block (16 warps); one block per SM
 
 struct CgSweepArgs {
     Domain D;
@@ -63,20 +63,32 @@ __device__ __forceinline__ double cg_dir(double invdiag, double r, double beta, 
     return __dadd_rn(__dmul_rn(invdiag, r), __dmul_rn(beta, p));
 }
 
-// eta * J_z(B*) at corner (col, j) (solvers.hpp:450-461); byl = byf(col-1, j).
-__device__ __forceinline__ double corner_rhs(const Domain& D, double by, double byl, double bx,
-                                             double bxb) {
-    const double dBy_dx = (by - byl) / D.dx;
-    const double dBx_dy = (bx - bxb) / D.dy;
+// eta * J_z(B*) at corner (col, j) (solvers.hpp:450-461); byl = byf(col-1, j); idx = 1/dx,
+// idy = 1/dy (a multiplication by the hoisted reciprocal is within 1 ulp of the quotient).
+__device__ __forceinline__ double corner_rhs(const Domain& D, double idx, double idy, double by,
+                                             double byl, double bx, double bxb) {
+    const double dBy_dx = (by - byl) * idx;
+    const double dBx_dy = (bx - bxb) * idy;
     return D.eta * (dBy_dx - dBx_dy);
 }
 
+// Raw loads of one row for the value of p at this lane's column and (edge lanes) the halo column:
+// A0 reads 8 face values, A_k reads r and p (own + halo), B_0 reads r, B_k also reads x.
+template <int N>
+struct CgRaw {
+    double v[N];
+};
+template <int PH>
+constexpr int cg_raw_n() { return PH == 0 ? 8 : (PH == 3 ? 5 : 4); }
+
 // One sweep over the warp's segment. PH: 0 = A0 (right-hand side, r0 = b, p0 = b/d),
-// 1 = A_k (k >= 1), 2 = B_0, 3 = B_k. acc[] receives this lane's partial sums.
+// 1 = A_k (k >= 1), 2 = B_0, 3 = B_k. acc[] receives this lane's partial sums. The loads of a row
+// are issued DEPTH rows before the row enters the stencil window.
 template <int PH>
 __device__ __forceinline__ void cg_sweep_segment(const CgSweepArgs& a, const CgScal& s, int w,
                                                  int dir, const double* rk, const double* pkm1,
                                                  double* rk1, double* pk, double (&acc)[3]) {
+    constexpr int DEPTH = (PH == 0) ? 2 : 4;
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
     const int sx = w % a.strips_x, sy = w / a.strips_x;
@@ -90,97 +102,131 @@ __device__ __forceinline__ void cg_sweep_segment(const CgSweepArgs& a, const CgS
     // halo column of the edge lanes: c0-1 for lane 0, c0+32 for lane 31
     const bool edge = (lane == 0) || (lane == 31);
     const int ih = wrap(lane == 0 ? c0 - 1 : c0 + 32, nx);
+    const int ihl = wrap(lane == 0 ? c0 - 2 : c0 + 31, nx);  // left of the halo column (A0)
+    const int il0 = wrap(c0 - 1, nx);                         // left of lane 0 (A0)
+    const double idx = 1.0 / a.D.dx, idy = 1.0 / a.D.dy;
     auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
 
-    // value of p at (column, row j) for this lane's own column and (edge lanes) the halo column;
-    // also returns r at the own column
-    auto p_row = [&](int j, double& p_own, double& p_halo, double& r_own) {
+    using Raw = CgRaw<cg_raw_n<PH>()>;
+    auto load_raw = [&](int j) {
+        Raw q{};
         const size_t rp = rowp(j);
-        if (PH == 0) {
+        if constexpr (PH == 0) {
             const size_t rb = rowp(j - 1);
-            const double by = __ldg(&a.byf[rp + iw]);
-            const double bx = __ldg(&a.bxf[rp + iw]);
-            const double bxb = __ldg(&a.bxf[rb + iw]);
-            double byl = __shfl_up_sync(0xffffffffu, by, 1);
-            if (lane == 0) byl = __ldg(&a.byf[rp + wrap(c0 - 1, nx)]);
-            const double b = corner_rhs(a.D, by, byl, bx, bxb);
+            q.v[0] = __ldg(&a.byf[rp + iw]);
+            q.v[1] = __ldg(&a.bxf[rp + iw]);
+            q.v[2] = __ldg(&a.bxf[rb + iw]);
+            q.v[3] = (lane == 0) ? __ldg(&a.byf[rp + il0]) : 0.0;
+            q.v[4] = edge ? __ldg(&a.byf[rp + ih]) : 0.0;
+            q.v[5] = edge ? __ldg(&a.byf[rp + ihl]) : 0.0;
+            q.v[6] = edge ? __ldg(&a.bxf[rp + ih]) : 0.0;
+            q.v[7] = edge ? __ldg(&a.bxf[rb + ih]) : 0.0;
+        } else {
+            q.v[0] = __ldcg(&rk[rp + iw]);
+            q.v[2] = edge ? __ldcg(&rk[rp + ih]) : 0.0;
+            if (PH != 2) {
+                q.v[1] = __ldcg(&pkm1[rp + iw]);
+                q.v[3] = edge ? __ldcg(&pkm1[rp + ih]) : 0.0;
+            }
+            if constexpr (PH == 3) q.v[4] = __ldcg(&a.x[rp + iw]);
+        }
+        return q;
+    };
+    // p (own column), p (halo column) and r (own column) of a row from its raw loads
+    auto compute = [&](const Raw& q, double& p_own, double& p_halo, double& r_own) {
+        if constexpr (PH == 0) {
+            double byl = __shfl_up_sync(0xffffffffu, q.v[0], 1);
+            if (lane == 0) byl = q.v[3];
+            const double b = corner_rhs(a.D, idx, idy, q.v[0], byl, q.v[1], q.v[2]);
             r_own = b;
             p_own = __dmul_rn(s.invdiag, b);
-            double ph = 0.0;
-            if (edge) {
-                const int ihl = wrap(lane == 0 ? c0 - 2 : c0 + 31, nx);
-                const double hby = __ldg(&a.byf[rp + ih]);
-                const double hbyl = __ldg(&a.byf[rp + ihl]);
-                const double hbx = __ldg(&a.bxf[rp + ih]);
-                const double hbxb = __ldg(&a.bxf[rb + ih]);
-                ph = __dmul_rn(s.invdiag, corner_rhs(a.D, hby, hbyl, hbx, hbxb));
-            }
-            p_halo = ph;
+            p_halo = edge ? __dmul_rn(s.invdiag, corner_rhs(a.D, idx, idy, q.v[4], q.v[5], q.v[6], q.v[7])) : 0.0;
+        } else if (PH == 2) {
+            r_own = q.v[0];
+            p_own = __dmul_rn(s.invdiag, q.v[0]);
+            p_halo = __dmul_rn(s.invdiag, q.v[2]);
         } else {
-            const double rv = __ldcg(&rk[rp + iw]);
-            r_own = rv;
-            if (PH == 2) {
-                p_own = __dmul_rn(s.invdiag, rv);
-                p_halo = edge ? __dmul_rn(s.invdiag, __ldcg(&rk[rp + ih])) : 0.0;
-            } else {
-                p_own = cg_dir(s.invdiag, rv, s.beta, __ldcg(&pkm1[rp + iw]));
-                p_halo = edge ? cg_dir(s.invdiag, __ldcg(&rk[rp + ih]), s.beta, __ldcg(&pkm1[rp + ih]))
-                              : 0.0;
-            }
+            r_own = q.v[0];
+            p_own = cg_dir(s.invdiag, q.v[0], s.beta, q.v[1]);
+            p_halo = cg_dir(s.invdiag, q.v[2], s.beta, q.v[3]);
         }
     };
 
     const int jfirst = (dir > 0) ? r0 : r1 - 1;
     const int jlast = (dir > 0) ? r1 - 1 : r0;
-    // window: p at rows j - dir (behind), j (current), j + dir (ahead)
-    double pb, pc, pa, hb, hc, ha, rb_, rc, ra;
-    p_row(jfirst - dir, pb, hb, rb_);
-    p_row(jfirst, pc, hc, rc);
-    p_row(jfirst + dir, pa, ha, ra);
-    (void)hb;
-    (void)rb_;
-    double xn = 0.0;
-    if (PH == 3) xn = __ldcg(&a.x[rowp(jfirst) + iw]);
-    for (int j = jfirst;; j += dir) {
-        // x neighbours of the current row
-        double pl = __shfl_up_sync(0xffffffffu, pc, 1);
-        double pr = __shfl_down_sync(0xffffffffu, pc, 1);
-        if (lane == 0) pl = hc;
-        if (lane == 31) pr = hc;
-        const double p_lo = (dir > 0) ? pb : pa;  // row j-1
-        const double p_hi = (dir > 0) ? pa : pb;  // row j+1
-        const double q = stencil(p_lo, pl, pc, pr, p_hi, s);
-        const double xcur = xn;
-        const bool more = (j != jlast);
-        // prefetch the row two ahead while this one is finished
-        double pn = 0.0, hn = 0.0, rn = 0.0;
-        if (more) {
-            p_row(j + 2 * dir, pn, hn, rn);
-            if (PH == 3) xn = __ldcg(&a.x[rowp(j + dir) + iw]);
+    const int nrows = r1 - r0;
+    // window: p at rows j - dir (behind), j (current), j + dir (ahead); x of the current row
+    double pb, pc, pa, hc, ha, rc, ra, xc = 0.0, xa = 0.0, dummy_h, dummy_r;
+    {
+        const Raw q0 = load_raw(jfirst - dir);
+        const Raw q1 = load_raw(jfirst);
+        const Raw q2 = load_raw(jfirst + dir);
+        compute(q0, pb, dummy_h, dummy_r);
+        compute(q1, pc, hc, rc);
+        compute(q2, pa, ha, ra);
+        if constexpr (PH == 3) {
+            xc = q1.v[4];
+            xa = q2.v[4];
         }
-        if (valid) {
-            const size_t g = (size_t)j * nx + i;
-            if (PH == 0) {
-                acc[0] += rc * rc;
-                acc[1] += rc * pc;
-                acc[2] += pc * q;
-                rk1[g] = rc;  // r0 = b
-            } else if (PH == 1) {
-                acc[0] += pc * q;
-            } else {
-                const double xv = (PH == 2) ? s.alpha * pc : xcur + s.alpha * pc;
-                const double rnew = rc - s.alpha * q;
-                a.x[g] = xv;
-                rk1[g] = rnew;
-                pk[g] = pc;
-                acc[0] += rnew * rnew;
-                acc[1] += rnew * __dmul_rn(s.invdiag, rnew);
+    }
+    (void)dummy_h;
+    (void)dummy_r;
+    Raw fifo[DEPTH];  // rows j + 2dir .. j + (DEPTH+1) dir
+#pragma unroll
+    for (int d = 0; d < DEPTH; ++d)
+        fifo[d] = (d + 2 <= nrows) ? load_raw(jfirst + (d + 2) * dir) : Raw{};
+    // The row loop is unrolled by DEPTH so that FIFO slot u is a fixed register set: a slot is
+    // consumed and refilled in the same unrolled step, and its load has DEPTH steps to arrive
+    // (a rotating copy would wait on the load at the first move).
+    bool done = false;
+    for (int t0 = 0; !done; t0 += DEPTH) {
+#pragma unroll
+        for (int u = 0; u < DEPTH; ++u) {
+            if (done) break;
+            const int t = t0 + u;
+            const int j = jfirst + t * dir;
+            // x neighbours of the current row
+            double pl = __shfl_up_sync(0xffffffffu, pc, 1);
+            double pr = __shfl_down_sync(0xffffffffu, pc, 1);
+            if (lane == 0) pl = hc;
+            if (lane == 31) pr = hc;
+            const double p_lo = (dir > 0) ? pb : pa;  // row j-1
+            const double p_hi = (dir > 0) ? pa : pb;  // row j+1
+            const double q = stencil(p_lo, pl, pc, pr, p_hi, s);
+            if (valid) {
+                const size_t g = (size_t)j * nx + i;
+                if (PH == 0) {
+                    acc[0] += rc * rc;
+                    acc[1] += rc * pc;
+                    acc[2] += pc * q;
+                    rk1[g] = rc;  // r0 = b
+                } else if (PH == 1) {
+                    acc[0] += pc * q;
+                } else {
+                    const double xv = (PH == 2) ? s.alpha * pc : xc + s.alpha * pc;
+                    const double rnew = rc - s.alpha * q;
+                    a.x[g] = xv;
+                    rk1[g] = rnew;
+                    pk[g] = pc;
+                    acc[0] += rnew * rnew;
+                    acc[1] += rnew * __dmul_rn(s.invdiag, rnew);
+                }
             }
+            if (j == jlast) {
+                done = true;
+                break;
+            }
+            // advance: row j + 2dir (slot u) enters the window; slot u is refilled
+            double pn, hn, rn;
+            compute(fifo[u], pn, hn, rn);
+            double xn = 0.0;
+            if constexpr (PH == 3) xn = fifo[u].v[4];
+            fifo[u] = (t + DEPTH + 2 <= nrows) ? load_raw(j + (DEPTH + 2) * dir) : Raw{};
+            pb = pc; pc = pa; pa = pn;
+            hc = ha; ha = hn;
+            rc = ra; ra = rn;
+            xc = xa; xa = xn;
         }
-        if (!more) break;
-        pb = pc; pc = pa; pa = pn;
-        hc = ha; ha = hn;
-        rc = ra; ra = rn;
     }
 }
 
@@ -204,7 +250,7 @@ __device__ __forceinline__ void publish(double (&acc)[3], double* slot, double* 
     }
 }
 
-__global__ void __launch_bounds__(CGS_NT)
+__global__ void __launch_bounds__(CGS_NT, 1)
 k_cg_sweep(CgSweepArgs a) {
     __shared__ double red[CGS_NT / 32 * 4];
     __shared__ double scal[8];
@@ -225,7 +271,11 @@ k_cg_sweep(CgSweepArgs a) {
     unsigned long long target = 0;
     const unsigned long long deadline =
         global_timer_ns() + (unsigned long long)(a.timeout_s * 1e9);
-    double* part[2] = {a.partials, a.partials + (size_t)G * 4};
+    double* const part0 = a.partials;
+    double* const part1 = a.partials + (size_t)G * 4;
+    // (conditional selects instead of indexing small arrays by a runtime value, which would put
+    // them in local memory)
+    auto part = [&](int ph) { return (ph & 1) ? part1 : part0; };
     int phase = 0;
     int dir = 1;
 
@@ -240,11 +290,11 @@ k_cg_sweep(CgSweepArgs a) {
         double acc[3] = {0.0, 0.0, 0.0};
         for (int w = wfirst; w < a.nwarps; w += wstride)
             cg_sweep_segment<0>(a, s, w, dir, nullptr, nullptr, a.r[0], nullptr, acc);
-        publish<3>(acc, part[phase & 1] + (size_t)blockIdx.x * 4, red);
+        publish<3>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
     }
     if (!barrier_or_quit()) return;
     double sums[3];
-    reduce_partials<3>(part[phase & 1], G, sums, scal);
+    reduce_partials<3>(part(phase), G, sums, scal);
     ++phase;
     dir = -dir;
     const double bb = sums[0];
@@ -259,18 +309,19 @@ k_cg_sweep(CgSweepArgs a) {
 
     if (!zero_solution && !breakdown) {
         for (long long k = 0; k < a.max_iters; ++k) {
-            const double* rk = a.r[k & 1];
-            double* rk1 = a.r[(k + 1) & 1];
-            const double* pkm1 = a.p[(k + 1) & 1];
-            double* pk = a.p[k & 1];
+            const bool odd = (k & 1) != 0;
+            const double* rk = odd ? a.r[1] : a.r[0];
+            double* rk1 = odd ? a.r[0] : a.r[1];
+            const double* pkm1 = odd ? a.p[0] : a.p[1];
+            double* pk = odd ? a.p[1] : a.p[0];
             if (k > 0) {
                 double acc[3] = {0.0, 0.0, 0.0};
                 for (int w = wfirst; w < a.nwarps; w += wstride)
                     cg_sweep_segment<1>(a, s, w, dir, rk, pkm1, nullptr, nullptr, acc);
-                publish<1>(acc, part[phase & 1] + (size_t)blockIdx.x * 4, red);
+                publish<1>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
                 if (!barrier_or_quit()) return;
                 double v[1];
-                reduce_partials<1>(part[phase & 1], G, v, scal);
+                reduce_partials<1>(part(phase), G, v, scal);
                 ++phase;
                 dir = -dir;
                 pq = v[0];
@@ -282,11 +333,11 @@ k_cg_sweep(CgSweepArgs a) {
                     if (k == 0) cg_sweep_segment<2>(a, s, w, dir, rk, pkm1, rk1, pk, acc);
                     else cg_sweep_segment<3>(a, s, w, dir, rk, pkm1, rk1, pk, acc);
                 }
-                publish<2>(acc, part[phase & 1] + (size_t)blockIdx.x * 4, red);
+                publish<2>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
             }
             if (!barrier_or_quit()) return;
             double v2[2];
-            reduce_partials<2>(part[phase & 1], G, v2, scal);
+            reduce_partials<2>(part(phase), G, v2, scal);
             ++phase;
             dir = -dir;
             ++products;

@@ -83,6 +83,14 @@ struct CgSync {
     unsigned int pad;
 };
 
+// Work split of a warp column sweep: column strips, each cut into row segments (one per warp).
+struct SweepGeom {
+    int strips_x;  // column strips
+    int seg_h;     // rows per strip segment
+    int segs_y;    // segments per column strip
+    int nwarps;    // strips_x * segs_y
+};
+
 // ------------------------------------------------------------------------------------------
 // Small helpers
 
@@ -151,7 +159,9 @@ __device__ __forceinline__ bool grid_barrier(CgSync* sync, unsigned long long& t
         atomicAdd(&sync->count, 1ULL);
         int ok = 1;
         while (true) {
-            const unsigned long long c = atomicAdd(&sync->count, 0ULL);
+            // poll with a plain load: read-modify-writes here would queue in front of the
+            // other blocks' arrivals at the same L2 address
+            const unsigned long long c = *(volatile unsigned long long*)&sync->count;
             if (c >= target) break;
             if (*(volatile unsigned int*)&sync->error) { ok = 0; break; }
             if (global_timer_ns() > deadline) {

@@ -46,8 +46,11 @@ __device__ __forceinline__ double recon_hi(double fm, double f0, double fp) {
 // Returns the (floored) pressure.
 __device__ __forceinline__ double primitives(double& rho, double mx, double my, double E,
                                              double bxc, double byc, double& vx, double& vy) {
-    vx = mx / rho;
-    vy = my / rho;
+    // one reciprocal instead of two divisions (<= 1 ulp from m/rho; the reference's fast-math
+    // build is free to do the same)
+    const double ir = 1.0 / rho;
+    vx = mx * ir;
+    vy = my * ir;
     if (rho < kRhoFloor) rho = kRhoFloor;
     const double kin = 0.5 * rho * (vx * vx + vy * vy);
     const double mag = (bxc * bxc + byc * byc) / 2;
@@ -60,9 +63,10 @@ __device__ __forceinline__ double primitives(double& rho, double mx, double my, 
 // HLL.hpp:107-122 fast magnetosonic speed
 __device__ __forceinline__ double fast_speed(const Prim& w, double bn) {
     const double b2 = w.bx * w.bx + w.by * w.by;
-    const double a2 = kGammaGas * w.p / w.rho;
-    const double t2 = b2 / w.rho;
-    const double n2 = bn * bn / w.rho;
+    const double ir = 1.0 / w.rho;  // one reciprocal for the three quotients by rho
+    const double a2 = kGammaGas * w.p * ir;
+    const double t2 = b2 * ir;
+    const double n2 = bn * bn * ir;
     const double sum = t2 + a2;
     const double term = sum * sum - 4.0 * a2 * n2;
     return sqrt(0.5 * (sum + sqrt(term > 0.0 ? term : 0.0)));
@@ -159,8 +163,9 @@ __device__ __forceinline__ double cfl_speed(double rho_f, double vx, double vy, 
                                             double bxc, double byc) {
     const double r = smax(rho_f, 1e-8);
     const double pr = smax(p, 1e-8);
-    const double a2 = kGammaGas * pr / r;
-    const double b2 = (bxc * bxc + byc * byc) / r;
+    const double ir = 1.0 / r;
+    const double a2 = kGammaGas * pr * ir;
+    const double b2 = (bxc * bxc + byc * byc) * ir;
     return sqrt(a2 + b2) + sqrt(vx * vx + vy * vy);
 }
 

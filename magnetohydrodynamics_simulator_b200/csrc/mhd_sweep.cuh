@@ -28,22 +28,20 @@ constexpr int SW_OUT = 28;       // output columns per warp
 constexpr int SW_WARPS = 4;      // warps (independent strips) per block
 constexpr int SW_PRE = 5;        // rows swept before the first output row of a strip
 
-struct SweepGeom {
-    int strips_x;  // column strips
-    int seg_h;     // rows per strip segment
-    int segs_y;    // segments per column strip
-    int nwarps;    // strips_x * segs_y
-};
-
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
-#ifndef MHD_SWEEP_MIN_BLOCKS
-#define MHD_SWEEP_MIN_BLOCKS 2  // 2 blocks of 4 warps per SM: ~200 registers, no spills
+// Blocks of 4 warps resident per SM: stage 1 fits 3 (~170 registers), stage 2 carries more state
+// and is kept at 2 (~220 registers) to avoid spills.
+#ifndef MHD_SWEEP_MIN_BLOCKS_1
+#define MHD_SWEEP_MIN_BLOCKS_1 3
+#endif
+#ifndef MHD_SWEEP_MIN_BLOCKS_2
+#define MHD_SWEEP_MIN_BLOCKS_2 2
 #endif
 
 template <int MODE>
-__global__ void __launch_bounds__(32 * SW_WARPS, MHD_SWEEP_MIN_BLOCKS)
+__global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
 k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
               const double* __restrict__ xsolve, Planes outA, Planes outB, SweepGeom G) {
     const int lane = threadIdx.x & 31;
@@ -81,6 +79,8 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
     double axr_cur = 0.0, axr_nxt = 0.0;              // lane 31: E1 one column to the right
     double fy_prev[5];                                // y-face flux of row c-1
     double fxbt_prev = 0.0, ez_prev = 0.0, jz_prev = 0.0;
+    double accH[4] = {0.0, 0.0, 0.0, 0.0};            // stage 2: accumulator hydro of row c
+    double accB[2] = {0.0, 0.0};                      // stage 2: accumulator faces of row c-1
 #pragma unroll
     for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; pend[k] = 0.0; }
 #pragma unroll
@@ -124,6 +124,20 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
                 axr_nxt = (lane == 31) ? __ldg(&xsolve[rn + iw_r]) : 0.0;
             }
         }
+        // stage 2: accumulator of the rows written next iteration (hydro row c+1, faces row c)
+        double nH[4] = {0.0, 0.0, 0.0, 0.0}, nB[2] = {0.0, 0.0};
+        if (MODE == 2 && out_lane) {
+            if (c + 1 >= r0 && c + 1 < r1) {
+                const size_t g = (size_t)(c + 1) * nx + i;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) nH[q] = outB.f[q][g];
+            }
+            if (c >= r0 && c < r1) {
+                const size_t g = (size_t)c * nx + i;
+                nB[0] = outB.f[4][g];
+                nB[1] = outB.f[5][g];
+            }
+        }
         // ---- B faces of row c+3 (and bxf one column to the right, for the cell-centred bx;
         //      lane 31 has its own copy of that column)
         double bx3 = a[4], by3 = a[5];
@@ -132,11 +146,11 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
             // B1 = U1*_B + dt*g*(rate of E1) (solvers.hpp:484-485, 528-529)
             double axr = shdn(ax0, 1);
             if (lane == 31) axr = axr0;
-            const double rbx = -(ax1 - ax0) / D.dy;
-            const double rby = (axr - ax0) / D.dx;
+            const double rbx = -(ax1 - ax0) * idy;
+            const double rby = (axr - ax0) * idx;
             bx3 += rbx * cg;
             by3 += rby * cg;
-            if (lane == 31) bxr3 += (-(axr1 - axr0) / D.dy) * cg;
+            if (lane == 31) bxr3 += (-(axr1 - axr0) * idy) * cg;
         }
         {
             const double right = shdn(bx3, 1);
@@ -224,8 +238,8 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
         }
         double jz = 0.0;
         if (MODE == 2) {  // eta*J_z(B1) at corner (i, c) (solvers.hpp:450-461)
-            const double dBy_dx = (Wby[1] - shup(Wby[1], 1)) / D.dx;
-            const double dBx_dy = (Wbx[1] - Wbx[0]) / D.dy;
+            const double dBy_dx = (Wby[1] - shup(Wby[1], 1)) * idx;
+            const double dBx_dy = (Wbx[1] - Wbx[0]) * idy;
             jz = D.eta * (dBy_dx - dBx_dy);
         }
         // ---- hydro rates of row c
@@ -247,7 +261,7 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
                     }
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) outB.f[q][g] = outB.f[q][g] + f[q] * cB;
+                    for (int q = 0; q < 4; ++q) outB.f[q][g] = accH[q] + f[q] * cB;
                 }
             }
         }
@@ -257,8 +271,8 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
             const double fby = (shdn(ez_prev, 1) - ez_prev) * idx;
             double g2x = 0.0, g2y = 0.0;
             if (MODE == 2) {
-                g2x = -(jz - jz_prev) / D.dy;
-                g2y = (shdn(jz_prev, 1) - jz_prev) / D.dx;
+                g2x = -(jz - jz_prev) * idy;
+                g2y = (shdn(jz_prev, 1) - jz_prev) * idx;
             }
             if (out_lane && c - 1 >= r0 && c - 1 < r1) {
                 const size_t g = (size_t)(c - 1) * nx + i;
@@ -269,8 +283,8 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
                     outB.f[4][g] = ubx + fbx * cB;
                     outB.f[5][g] = uby + fby * cB;
                 } else {
-                    double ax = outB.f[4][g] + fbx * cB;
-                    double ay = outB.f[5][g] + fby * cB;
+                    double ax = accB[0] + fbx * cB;
+                    double ay = accB[1] + fby * cB;
                     ax += g2x * c1mg;
                     ay += g2y * c1mg;
                     outB.f[4][g] = ax;
@@ -283,6 +297,12 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
         fxbt_prev = fx.bt;
         ez_prev = ez;
         jz_prev = jz;
+        if (MODE == 2) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) accH[q] = nH[q];
+            accB[0] = nB[0];
+            accB[1] = nB[1];
+        }
     }
 }
 
