@@ -141,7 +141,7 @@ mhd_status launch_cg(mhd_context* c, const double* bxf, const double* byf, int s
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(c->cg_grid);
     cfg.blockDim = dim3(CGS_NT);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = kCgRingBytes;
     cfg.stream = c->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -382,11 +382,14 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
     // segments over all of their warps.
     {
         int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_sweep, CGS_NT, 0) != cudaSuccess ||
+        if (cudaFuncSetAttribute(k_cg_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kCgRingBytes) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_sweep, CGS_NT, kCgRingBytes) !=
+                cudaSuccess ||
             occ < 1)
             return fail(MHD_ERR_CUDA);
         const int per_sm = std::max(1, std::min(occ, env_int("MHD_B200_CG_BLOCKS_PER_SM", 1)));
-        c->cg_strips_x = (p->nx + 31) / 32;
+        c->cg_strips_x = (p->nx + CG_W - 1) / CG_W;
         const long long rows_total = (long long)c->cg_strips_x * p->ny;
         // no more blocks than there are rows of work for their warps
         const long long max_blocks = std::max(1LL, (rows_total + (CGS_NT / 32) * 4 - 1) / ((CGS_NT / 32) * 4));

@@ -3,9 +3,10 @@
 // scaling by the constant diagonal, stop when |r|^2 < max(tol^2 |b|^2, DBL_MIN), at most max_iters
 // matrix-vector products).
 //
-// Each warp owns a strip of 32 corner columns and a segment of rows; lane l holds column c0 + l and
-// lanes 0 / 31 also evaluate the halo column on their side. The 5-point product is formed from a
-// 3-row register window (y neighbours) and shuffles (x neighbours). Per iteration:
+// Each warp owns a strip of 30 corner columns and a segment of rows; its 32 lanes hold the strip and
+// one halo column on each side. The 5-point product is formed from a 3-row register window
+// (y neighbours) and shuffles (x neighbours); rows are prefetched 8 deep into shared memory with
+// cp.async. Per iteration:
 //   phase A: p_k = r_k/d + beta p_{k-1} (rows j-1..j+1), q = A p_k, partial p.q          reads r, p
 //   phase B: the same p_k and q; x += alpha p_k; r_{k+1} = r_k - alpha q; partial r.r, r.z;
 //            writes x, r_{k+1}, p_k                                              reads r, p, x
@@ -20,7 +21,10 @@
 
 namespace mhd {
 
-constexpr int CGS_NT = 512;  // threads per block (16 warps); one block per SM
+constexpr int CGS_NT = 512;  // threads per block (16 warps)
+#ifndef MHD_CG_MIN_BLOCKS
+#define MHD_CG_MIN_BLOCKS 1      // blocks per SM (the prefetch lives in shared memory)
+#endif
 
 struct CgSweepArgs {
     Domain D;
@@ -72,162 +76,154 @@ __device__ __forceinline__ double corner_rhs(const Domain& D, double idx, double
     return D.eta * (dBy_dx - dBx_dy);
 }
 
-// Raw loads of one row for the value of p at this lane's column and (edge lanes) the halo column:
-// A0 reads 8 face values, A_k reads r and p (own + halo), B_0 reads r, B_k also reads x.
+// Asynchronous 8-byte global -> shared copy (cp.async), its commit and its wait.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+#if defined(__CUDA_ARCH__)
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+#else
+    *smem = *gmem;  // host compilation of the kernel sources: a plain copy
+#endif
+}
+__device__ __forceinline__ void cp_async_commit() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
 template <int N>
-struct CgRaw {
-    double v[N];
-};
-template <int PH>
-constexpr int cg_raw_n() { return PH == 0 ? 8 : (PH == 3 ? 5 : 4); }
+__device__ __forceinline__ void cp_async_wait() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+#endif
+}
+
+// Per-warp ring of prefetched rows in shared memory. A slot holds, for one row, up to 3 vectors at
+// the warp's 32 columns (lane l's element at v*32 + l) and, in the right-hand-side phase, lane 0's
+// extra face value at 96. Every lane reads back only what it copied itself, so
+// cp.async.wait_group alone orders the accesses.
+constexpr int CG_RING = 8;    // rows in flight per warp (power of two)
+constexpr int CG_SLOT = 104;  // doubles per slot (832 bytes, 16-byte multiple)
+constexpr int CG_W = 30;      // output columns per warp: lanes 1..30; lanes 0 and 31 are halo
+constexpr size_t kCgRingBytes = (size_t)(CGS_NT / 32) * CG_RING * CG_SLOT * sizeof(double);
 
 // One sweep over the warp's segment. PH: 0 = A0 (right-hand side, r0 = b, p0 = b/d),
-// 1 = A_k (k >= 1), 2 = B_0, 3 = B_k. acc[] receives this lane's partial sums. The loads of a row
-// are issued DEPTH rows before the row enters the stencil window.
+// 1 = A_k (k >= 1), 2 = B_0, 3 = B_k. acc[] receives this lane's partial sums. Lane l holds corner
+// column c0 - 1 + l; every lane does the same work and lanes 1..30 own the results. Row k of the
+// sweep (k = 0 is the row behind the first one) is copied into slot k % CG_RING, CG_RING - 3 rows
+// before it enters the 3-row stencil window.
 template <int PH>
 __device__ __forceinline__ void cg_sweep_segment(const CgSweepArgs& a, const CgScal& s, int w,
                                                  int dir, const double* rk, const double* pkm1,
-                                                 double* rk1, double* pk, double (&acc)[3]) {
-    constexpr int DEPTH = (PH == 0) ? 2 : 4;
+                                                 double* rk1, double* pk, double* ring,
+                                                 double (&acc)[3]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
     const int sx = w % a.strips_x, sy = w / a.strips_x;
-    const int c0 = sx * 32;
+    const int c0 = sx * CG_W;
     const int r0 = sy * a.seg_h;
     const int r1 = min(r0 + a.seg_h, ny);
     if (r0 >= r1) return;
-    const int i = c0 + lane;
-    const bool valid = i < nx;
+    const int i = c0 - 1 + lane;
+    const bool owner = lane >= 1 && lane <= CG_W && i < nx;
     const int iw = wrap(i, nx);
-    // halo column of the edge lanes: c0-1 for lane 0, c0+32 for lane 31
-    const bool edge = (lane == 0) || (lane == 31);
-    const int ih = wrap(lane == 0 ? c0 - 1 : c0 + 32, nx);
-    const int ihl = wrap(lane == 0 ? c0 - 2 : c0 + 31, nx);  // left of the halo column (A0)
-    const int il0 = wrap(c0 - 1, nx);                         // left of lane 0 (A0)
+    const int iwl = wrap(i - 1, nx);  // lane 0's left neighbour (right-hand-side phase)
     const double idx = 1.0 / a.D.dx, idy = 1.0 / a.D.dy;
-    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
-
-    using Raw = CgRaw<cg_raw_n<PH>()>;
-    auto load_raw = [&](int j) {
-        Raw q{};
-        const size_t rp = rowp(j);
-        if constexpr (PH == 0) {
-            const size_t rb = rowp(j - 1);
-            q.v[0] = __ldg(&a.byf[rp + iw]);
-            q.v[1] = __ldg(&a.bxf[rp + iw]);
-            q.v[2] = __ldg(&a.bxf[rb + iw]);
-            q.v[3] = (lane == 0) ? __ldg(&a.byf[rp + il0]) : 0.0;
-            q.v[4] = edge ? __ldg(&a.byf[rp + ih]) : 0.0;
-            q.v[5] = edge ? __ldg(&a.byf[rp + ihl]) : 0.0;
-            q.v[6] = edge ? __ldg(&a.bxf[rp + ih]) : 0.0;
-            q.v[7] = edge ? __ldg(&a.bxf[rb + ih]) : 0.0;
-        } else {
-            q.v[0] = __ldcg(&rk[rp + iw]);
-            q.v[2] = edge ? __ldcg(&rk[rp + ih]) : 0.0;
-            if (PH != 2) {
-                q.v[1] = __ldcg(&pkm1[rp + iw]);
-                q.v[3] = edge ? __ldcg(&pkm1[rp + ih]) : 0.0;
-            }
-            if constexpr (PH == 3) q.v[4] = __ldcg(&a.x[rp + iw]);
-        }
-        return q;
-    };
-    // p (own column), p (halo column) and r (own column) of a row from its raw loads
-    auto compute = [&](const Raw& q, double& p_own, double& p_halo, double& r_own) {
-        if constexpr (PH == 0) {
-            double byl = __shfl_up_sync(0xffffffffu, q.v[0], 1);
-            if (lane == 0) byl = q.v[3];
-            const double b = corner_rhs(a.D, idx, idy, q.v[0], byl, q.v[1], q.v[2]);
-            r_own = b;
-            p_own = __dmul_rn(s.invdiag, b);
-            p_halo = edge ? __dmul_rn(s.invdiag, corner_rhs(a.D, idx, idy, q.v[4], q.v[5], q.v[6], q.v[7])) : 0.0;
-        } else if (PH == 2) {
-            r_own = q.v[0];
-            p_own = __dmul_rn(s.invdiag, q.v[0]);
-            p_halo = __dmul_rn(s.invdiag, q.v[2]);
-        } else {
-            r_own = q.v[0];
-            p_own = cg_dir(s.invdiag, q.v[0], s.beta, q.v[1]);
-            p_halo = cg_dir(s.invdiag, q.v[2], s.beta, q.v[3]);
-        }
-    };
-
     const int jfirst = (dir > 0) ? r0 : r1 - 1;
     const int jlast = (dir > 0) ? r1 - 1 : r0;
     const int nrows = r1 - r0;
-    // window: p at rows j - dir (behind), j (current), j + dir (ahead); x of the current row
-    double pb, pc, pa, hc, ha, rc, ra, xc = 0.0, xa = 0.0, dummy_h, dummy_r;
-    {
-        const Raw q0 = load_raw(jfirst - dir);
-        const Raw q1 = load_raw(jfirst);
-        const Raw q2 = load_raw(jfirst + dir);
-        compute(q0, pb, dummy_h, dummy_r);
-        compute(q1, pc, hc, rc);
-        compute(q2, pa, ha, ra);
-        if constexpr (PH == 3) {
-            xc = q1.v[4];
-            xa = q2.v[4];
-        }
-    }
-    (void)dummy_h;
-    (void)dummy_r;
-    Raw fifo[DEPTH];  // rows j + 2dir .. j + (DEPTH+1) dir
-#pragma unroll
-    for (int d = 0; d < DEPTH; ++d)
-        fifo[d] = (d + 2 <= nrows) ? load_raw(jfirst + (d + 2) * dir) : Raw{};
-    // The row loop is unrolled by DEPTH so that FIFO slot u is a fixed register set: a slot is
-    // consumed and refilled in the same unrolled step, and its load has DEPTH steps to arrive
-    // (a rotating copy would wait on the load at the first move).
-    bool done = false;
-    for (int t0 = 0; !done; t0 += DEPTH) {
-#pragma unroll
-        for (int u = 0; u < DEPTH; ++u) {
-            if (done) break;
-            const int t = t0 + u;
-            const int j = jfirst + t * dir;
-            // x neighbours of the current row
-            double pl = __shfl_up_sync(0xffffffffu, pc, 1);
-            double pr = __shfl_down_sync(0xffffffffu, pc, 1);
-            if (lane == 0) pl = hc;
-            if (lane == 31) pr = hc;
-            const double p_lo = (dir > 0) ? pb : pa;  // row j-1
-            const double p_hi = (dir > 0) ? pa : pb;  // row j+1
-            const double q = stencil(p_lo, pl, pc, pr, p_hi, s);
-            if (valid) {
-                const size_t g = (size_t)j * nx + i;
-                if (PH == 0) {
-                    acc[0] += rc * rc;
-                    acc[1] += rc * pc;
-                    acc[2] += pc * q;
-                    rk1[g] = rc;  // r0 = b
-                } else if (PH == 1) {
-                    acc[0] += pc * q;
-                } else {
-                    const double xv = (PH == 2) ? s.alpha * pc : xc + s.alpha * pc;
-                    const double rnew = rc - s.alpha * q;
-                    a.x[g] = xv;
-                    rk1[g] = rnew;
-                    pk[g] = pc;
-                    acc[0] += rnew * rnew;
-                    acc[1] += rnew * __dmul_rn(s.invdiag, rnew);
-                }
+    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
+    auto slot = [&](int k) { return ring + (unsigned)(k & (CG_RING - 1)) * CG_SLOT; };
+
+    // copy sweep row k (grid row jfirst + (k-1) dir) into its slot and commit one group
+    auto issue = [&](int k) {
+        if (k <= nrows + 1) {
+            double* sl = slot(k);
+            const int j = jfirst + (k - 1) * dir;
+            const size_t rp = rowp(j);
+            if constexpr (PH == 0) {
+                const size_t rb = rowp(j - 1);
+                cp_async8(&sl[lane], &a.byf[rp + iw]);
+                cp_async8(&sl[32 + lane], &a.bxf[rp + iw]);
+                cp_async8(&sl[64 + lane], &a.bxf[rb + iw]);
+                if (lane == 0) cp_async8(&sl[96], &a.byf[rp + iwl]);
+            } else {
+                cp_async8(&sl[lane], &rk[rp + iw]);
+                if constexpr (PH != 2) cp_async8(&sl[32 + lane], &pkm1[rp + iw]);
+                if constexpr (PH == 3) cp_async8(&sl[64 + lane], &a.x[rp + iw]);
             }
-            if (j == jlast) {
-                done = true;
-                break;
-            }
-            // advance: row j + 2dir (slot u) enters the window; slot u is refilled
-            double pn, hn, rn;
-            compute(fifo[u], pn, hn, rn);
-            double xn = 0.0;
-            if constexpr (PH == 3) xn = fifo[u].v[4];
-            fifo[u] = (t + DEPTH + 2 <= nrows) ? load_raw(j + (DEPTH + 2) * dir) : Raw{};
-            pb = pc; pc = pa; pa = pn;
-            hc = ha; ha = hn;
-            rc = ra; ra = rn;
-            xc = xa; xa = xn;
         }
+        cp_async_commit();
+    };
+    // p, r and x at this lane's column of sweep row k, from its slot
+    auto compute = [&](int k, double& p_own, double& r_own, double& x_own) {
+        const double* sl = slot(k);
+        if constexpr (PH == 0) {
+            const double by = sl[lane];
+            double byl = __shfl_up_sync(0xffffffffu, by, 1);
+            if (lane == 0) byl = sl[96];
+            const double b = corner_rhs(a.D, idx, idy, by, byl, sl[32 + lane], sl[64 + lane]);
+            r_own = b;
+            p_own = __dmul_rn(s.invdiag, b);
+        } else if constexpr (PH == 2) {
+            r_own = sl[lane];
+            p_own = __dmul_rn(s.invdiag, r_own);
+        } else {
+            r_own = sl[lane];
+            p_own = cg_dir(s.invdiag, r_own, s.beta, sl[32 + lane]);
+        }
+        if constexpr (PH == 3) x_own = sl[64 + lane];
+        else x_own = 0.0;
+    };
+
+#pragma unroll
+    for (int k = 0; k < CG_RING; ++k) issue(k);
+    cp_async_wait<CG_RING - 3>();  // rows 0, 1, 2 have landed
+    // window: p at rows j - dir (behind), j (current), j + dir (ahead)
+    double pb, pc, pa, rc, ra, xc, xa, dr, dx_;
+    compute(0, pb, dr, dx_);
+    compute(1, pc, rc, xc);
+    compute(2, pa, ra, xa);
+    (void)dr;
+    (void)dx_;
+    size_t g = (size_t)jfirst * nx + i;  // owner lanes' element of the current row
+    const long long gstep = (long long)dir * nx;
+    for (int t = 0;; ++t) {
+        issue(t + CG_RING);  // slot of row t, which entered the window three rows ago
+        const double pl = __shfl_up_sync(0xffffffffu, pc, 1);
+        const double pr = __shfl_down_sync(0xffffffffu, pc, 1);
+        const double p_lo = (dir > 0) ? pb : pa;  // row j-1
+        const double p_hi = (dir > 0) ? pa : pb;  // row j+1
+        const double q = stencil(p_lo, pl, pc, pr, p_hi, s);
+        if (owner) {
+            if constexpr (PH == 0) {
+                acc[0] += rc * rc;
+                acc[1] += rc * pc;
+                acc[2] += pc * q;
+                rk1[g] = rc;  // r0 = b
+            } else if constexpr (PH == 1) {
+                acc[0] += pc * q;
+            } else {
+                const double xv = (PH == 2) ? s.alpha * pc : xc + s.alpha * pc;
+                const double rnew = rc - s.alpha * q;
+                a.x[g] = xv;
+                rk1[g] = rnew;
+                pk[g] = pc;
+                acc[0] += rnew * rnew;
+                acc[1] += rnew * __dmul_rn(s.invdiag, rnew);
+            }
+        }
+        if (t == nrows - 1) break;
+        g += gstep;
+        // row t+3 (j + 2dir) enters the window
+        cp_async_wait<CG_RING - 3>();
+        double pn, rn, xn;
+        compute(t + 3, pn, rn, xn);
+        pb = pc; pc = pa; pa = pn;
+        rc = ra; ra = rn;
+        xc = xa; xa = xn;
     }
+    (void)jlast;
+    cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
 // Block-reduce NV partial sums (fixed order) and publish them in this block's slot.
@@ -250,11 +246,18 @@ __device__ __forceinline__ void publish(double (&acc)[3], double* slot, double* 
     }
 }
 
-__global__ void __launch_bounds__(CGS_NT, 1)
+__global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
 k_cg_sweep(CgSweepArgs a) {
     __shared__ double red[CGS_NT / 32 * 4];
     __shared__ double scal[8];
     __shared__ int sflag;
+#if defined(__CUDA_ARCH__)
+    extern __shared__ __align__(16) double cg_ring_mem[];
+#else
+    // host compilation of the kernel sources (single-block logic tests): one shared copy
+    static double cg_ring_mem[(CGS_NT / 32) * CG_RING * CG_SLOT];
+#endif
+    double* const ring = cg_ring_mem + (size_t)(threadIdx.x >> 5) * CG_RING * CG_SLOT;
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     const int warps_per_block = CGS_NT / 32;
@@ -289,7 +292,7 @@ k_cg_sweep(CgSweepArgs a) {
     {
         double acc[3] = {0.0, 0.0, 0.0};
         for (int w = wfirst; w < a.nwarps; w += wstride)
-            cg_sweep_segment<0>(a, s, w, dir, nullptr, nullptr, a.r[0], nullptr, acc);
+            cg_sweep_segment<0>(a, s, w, dir, nullptr, nullptr, a.r[0], nullptr, ring, acc);
         publish<3>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
     }
     if (!barrier_or_quit()) return;
@@ -317,7 +320,7 @@ k_cg_sweep(CgSweepArgs a) {
             if (k > 0) {
                 double acc[3] = {0.0, 0.0, 0.0};
                 for (int w = wfirst; w < a.nwarps; w += wstride)
-                    cg_sweep_segment<1>(a, s, w, dir, rk, pkm1, nullptr, nullptr, acc);
+                    cg_sweep_segment<1>(a, s, w, dir, rk, pkm1, nullptr, nullptr, ring, acc);
                 publish<1>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
                 if (!barrier_or_quit()) return;
                 double v[1];
@@ -330,8 +333,8 @@ k_cg_sweep(CgSweepArgs a) {
             {
                 double acc[3] = {0.0, 0.0, 0.0};
                 for (int w = wfirst; w < a.nwarps; w += wstride) {
-                    if (k == 0) cg_sweep_segment<2>(a, s, w, dir, rk, pkm1, rk1, pk, acc);
-                    else cg_sweep_segment<3>(a, s, w, dir, rk, pkm1, rk1, pk, acc);
+                    if (k == 0) cg_sweep_segment<2>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    else cg_sweep_segment<3>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
                 }
                 publish<2>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
             }
