@@ -98,6 +98,18 @@ mhd_status mhd_step(mhd_context* ctx, double dt);
 mhd_status mhd_run(mhd_context* ctx, int nsteps, double dt_fixed, double t_end, double* dts_out,
                    long long* cg_products_out);
 
+/* resistive_B_term(grid, bx_rate, by_rate, solver, workspace, solve_implicitly)
+ * (solvers.hpp:445-489) on device arrays: the rate of the face field, -curl E, from the corner field
+ * E = eta*J_z(B) (solve_implicitly == 0) or the solution of (I - alpha L) E = eta*J_z(B)
+ * (solve_implicitly != 0; the reference's matrix of generate_A_matrix(grid, workspace, alpha)).
+ * bxf, byf, bx_rate, by_rate are device pointers to dense nx*ny planes of the context's grid.
+ * cg_products (host, may be NULL) receives the solve's matrix-vector products; when it is given
+ * the call waits for the result. Uses the context's solver workspace (not concurrent with a step
+ * on another stream). */
+mhd_status mhd_resistive_rate(mhd_context* ctx, int solve_implicitly, double alpha,
+                              const double* bxf, const double* byf, double* bx_rate,
+                              double* by_rate, long long* cg_products);
+
 /* CFL_condition_checker(grid) (diagnostics.hpp:44-88) with the context's courant/safety. */
 mhd_status mhd_cfl_dt(mhd_context* ctx, double* dt);
 

@@ -83,6 +83,10 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_step.argtypes = [vp, ctypes.c_double]
     lib.mhd_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp,
                             ctypes.POINTER(ctypes.c_longlong)]
+    lib.mhd_resistive_rate.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, vp,
+                                       ctypes.POINTER(ctypes.c_longlong)]
+    lib.mhd_set_kernel_timing.argtypes = [vp, ctypes.c_int]
+    lib.mhd_kernel_times.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.mhd_cfl_dt.argtypes = [vp, _dp]
     lib.mhd_divb.argtypes = [vp, _dp, _dp]
     lib.mhd_synchronize.argtypes = [vp]
@@ -223,6 +227,17 @@ class Context:
         out = (ctypes.c_longlong * 2)()
         _check(self.lib.mhd_last_cg_products(self.h, out), "mhd_last_cg_products")
         return int(out[0]), int(out[1])
+
+    def resistive_rate(self, bxf: int, byf: int, bx_rate: int, by_rate: int, *,
+                       solve_implicitly: bool, alpha: float = 0.0) -> int:
+        """resistive_B_term (solvers.hpp:445-489) on device planes given by their addresses;
+        returns the implicit solve's matrix-vector products."""
+        prods = ctypes.c_longlong()
+        _check(self.lib.mhd_resistive_rate(self.h, int(solve_implicitly), alpha, ctypes.c_void_p(bxf),
+                                           ctypes.c_void_p(byf), ctypes.c_void_p(bx_rate),
+                                           ctypes.c_void_p(by_rate), ctypes.byref(prods)),
+               "mhd_resistive_rate")
+        return int(prods.value)
 
     def cfl_dt(self) -> float:
         v = ctypes.c_double()

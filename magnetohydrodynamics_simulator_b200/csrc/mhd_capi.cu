@@ -657,6 +657,40 @@ mhd_status mhd_run(mhd_context* c, int nsteps, double dt_fixed, double t_end, do
     return MHD_OK;
 }
 
+mhd_status mhd_resistive_rate(mhd_context* c, int solve_implicitly, double alpha,
+                              const double* bxf, const double* byf, double* bx_rate,
+                              double* by_rate, long long* cg_products) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!bxf || !byf || !bx_rate || !by_rate || (solve_implicitly && !(alpha >= 0)) ||
+        !std::isfinite(alpha))
+        return MHD_ERR_INVALID_ARGUMENT;
+    const int blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 8));
+    if (solve_implicitly) {
+        k_set_alpha<<<1, 1, 0, c->stream>>>(c->coeffs, alpha);
+        MHD_TRY(cudaGetLastError());
+        s = launch_cg(c, bxf, byf, 0, nullptr);
+        if (s != MHD_OK) return s;
+        k_corner_rates<<<blocks, 256, 0, c->stream>>>(c->dom, c->x, nullptr, nullptr, bx_rate, by_rate);
+    } else {
+        k_corner_rates<<<blocks, 256, 0, c->stream>>>(c->dom, nullptr, bxf, byf, bx_rate, by_rate);
+    }
+    MHD_TRY(cudaGetLastError());
+    if (cg_products) {
+        if (!solve_implicitly) {
+            *cg_products = 0;
+        } else {
+            MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->status, sizeof(DeviceStatus),
+                                    cudaMemcpyDeviceToHost, c->stream));
+            MHD_TRY(cudaStreamSynchronize(c->stream));
+            DeviceStatus st;
+            memcpy(&st, c->host_pinned, sizeof(st));
+            *cg_products = st.cg_products[0];
+        }
+    }
+    return MHD_OK;
+}
+
 mhd_status mhd_cfl_dt(mhd_context* c, double* dt) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;

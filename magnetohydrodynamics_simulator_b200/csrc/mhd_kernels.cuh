@@ -448,6 +448,35 @@ k_primitives(Domain D, CPlanes u, double* rho_f, double* vx, double* vy, double*
     }
 }
 
+// Rate of the face field from a corner field E (solvers.hpp:472-488): bx' = -(E(i,j+1) - E(i,j))/dy,
+// by' = (E(i+1,j) - E(i,j))/dx. With E == nullptr the corner field is eta*J_z(bxf, byf) itself
+// (the explicit resistive term, solvers.hpp:450-463 and :470).
+__global__ void __launch_bounds__(256)
+k_corner_rates(Domain D, const double* __restrict__ E, const double* __restrict__ bxf,
+               const double* __restrict__ byf, double* __restrict__ bx_rate,
+               double* __restrict__ by_rate) {
+    const int nx = D.nx, ny = D.ny;
+    const size_t n = (size_t)nx * ny;
+    auto ez = [&](int i, int j) -> double {
+        const size_t g = (size_t)wrap(j, ny) * nx + wrap(i, nx);
+        if (E) return E[g];
+        const double dBy_dx = (byf[g] - byf[(size_t)wrap(j, ny) * nx + wrap(i - 1, nx)]) / D.dx;
+        const double dBx_dy = (bxf[g] - bxf[(size_t)wrap(j - 1, ny) * nx + wrap(i, nx)]) / D.dy;
+        return D.eta * (dBy_dx - dBx_dy);
+    };
+    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+         g += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+        const double e = ez(i, j);
+        bx_rate[g] = -(ez(i, j + 1) - e) / D.dy;
+        by_rate[g] = (ez(i + 1, j) - e) / D.dx;
+    }
+}
+
+__global__ void k_set_alpha(StepCoeffs* C, double alpha) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) C->alpha = alpha;
+}
+
 // Dense periodic plane -> padded plane with ng periodic ghost layers (Grid.hpp:143-161).
 __global__ void __launch_bounds__(256)
 k_pad_plane(const double* __restrict__ src, double* __restrict__ dst, int nx, int ny, int ng) {

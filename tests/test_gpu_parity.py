@@ -246,6 +246,41 @@ def test_orszag_tang_point_symmetry(m):
         assert np.max(np.abs(pr[k] + refl(pr[k]))) <= 1e-10 * scale[k], k
 
 
+def test_resistive_rate_matches_reference(m):
+    """resistive_B_term on device arrays: implicit rate against the reference's own (golden) solve,
+    explicit rate against the oracle."""
+    import torch
+
+    d = load_golden("random40x24_ref.npz")
+    nx, ny, dx, dy, eta = int(d["nx"]), int(d["ny"]), float(d["dx"]), float(d["dy"]), float(d["eta"])
+    ctx = m.Context(nx, ny, dx, dy, eta)
+    bxf = torch.tensor(d["ic_bxf"], device="cuda")
+    byf = torch.tensor(d["ic_byf"], device="cuda")
+    bx = torch.empty_like(bxf)
+    by = torch.empty_like(byf)
+    torch.cuda.synchronize()
+    prods = ctx.resistive_rate(bxf.data_ptr(), byf.data_ptr(), bx.data_ptr(), by.data_ptr(),
+                               solve_implicitly=True, alpha=float(d["implicit_alpha"]))
+    ctx.synchronize()
+    assert prods > 0
+    errs = _errs([bx.cpu().numpy(), by.cpu().numpy()], [d["implicit_bx"], d["implicit_by"]])
+    assert max(errs) <= STEP_TOL, errs
+    # explicit
+    orc = Oracle(nx, ny, dx, dy, eta)
+    want_x = np.zeros((ny, nx))
+    want_y = np.zeros((ny, nx))
+    import ctypes
+    from oracle.oracle import _ptr
+
+    ic = [np.ascontiguousarray(d["ic_bxf"]), np.ascontiguousarray(d["ic_byf"])]
+    orc.lib.orc_resistive_rate(ctypes.byref(orc.p), _ptr(ic[0]), _ptr(ic[1]), -1.0, _ptr(want_x), _ptr(want_y))
+    assert ctx.resistive_rate(bxf.data_ptr(), byf.data_ptr(), bx.data_ptr(), by.data_ptr(),
+                              solve_implicitly=False) == 0
+    ctx.synchronize()
+    errs = _errs([bx.cpu().numpy(), by.cpu().numpy()], [want_x, want_y])
+    assert max(errs) <= STEP_TOL, errs
+
+
 def test_cfl_primitives_and_divb_match_oracle(m):
     d = load_golden("random40x24_ref.npz")
     nx, ny, dx, dy, eta = int(d["nx"]), int(d["ny"]), float(d["dx"]), float(d["dy"]), float(d["eta"])
