@@ -36,7 +36,8 @@ typedef enum {
     MHD_ERR_TIMEOUT = 5,            /* a grid-wide wait of the persistent CG ran out of time */
     MHD_ERR_NO_DEVICE = 6,          /* no sm_100 device, or the library was not built for it */
     MHD_ERR_OUT_OF_MEMORY = 7,
-    MHD_ERR_NO_STATE = 8            /* a state must be set before stepping */
+    MHD_ERR_NO_STATE = 8,           /* a state must be set before stepping */
+    MHD_ERR_TOO_LARGE = 9           /* grid larger than the fixed scratch of the no-alloc call */
 } mhd_status;
 
 typedef enum { MHD_LAYOUT_DENSE = 0, MHD_LAYOUT_PADDED = 1 } mhd_layout;
@@ -109,6 +110,29 @@ mhd_status mhd_run(mhd_context* ctx, int nsteps, double dt_fixed, double t_end, 
 mhd_status mhd_resistive_rate(mhd_context* ctx, int solve_implicitly, double alpha,
                               const double* bxf, const double* byf, double* bx_rate,
                               double* by_rate, long long* cg_products);
+
+/* Allocation-free variant of mhd_resistive_rate (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory where they need the solve: plugins whose host
+ * application owns every device buffer and hands out only its own, processes running under a
+ * device-memory budget where a new allocation fails or is not allowed, and latency-sensitive loops
+ * in which cudaMalloc/cudaFree would stall on an implicit device synchronisation. It takes no
+ * context; the caller passes the inputs and outputs (device pointers to dense nx*ny planes) and
+ * the grid parameters (nx, ny, dx, dy, eta, cg_tol, cg_max_iters, cg_timeout_s are used).
+ *
+ * Scratch lives in one file-scope device array sized for at most MHD_NOALLOC_MAX_CELLS cells
+ * (256 x 256; about 2.7 MB, held on every device that loads this library until the process
+ * exits). Larger grids are rejected with MHD_ERR_TOO_LARGE. The function calls no cudaMalloc,
+ * cudaFree or allocating library routine. The first call on a device resolves the array's device
+ * address (cudaGetSymbolAddress) and sets up the solver kernel; make that first call before any
+ * stream capture. All calls share the one array: calls that overlap on the GPU (other streams,
+ * other threads) race on it, so serialise them. stream: a cudaStream_t (NULL = legacy default).
+ * cg_products (host, may be NULL) receives the matrix-vector products; the call waits for the
+ * result and returns the solve's device status. */
+#define MHD_NOALLOC_MAX_CELLS 65536
+mhd_status mhd_resistive_rate_noalloc(const mhd_params* p, int solve_implicitly, double alpha,
+                                      const double* bxf, const double* byf, double* bx_rate,
+                                      double* by_rate, long long* cg_products, void* stream);
 
 /* CFL_condition_checker(grid) (diagnostics.hpp:44-88) with the context's courant/safety. */
 mhd_status mhd_cfl_dt(mhd_context* ctx, double* dt);

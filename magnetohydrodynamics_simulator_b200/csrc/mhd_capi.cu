@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <vector>
 
 #include "../../include/mhd_b200.h"
@@ -274,6 +275,7 @@ const char* mhd_status_string(mhd_status s) {
         case MHD_ERR_NO_DEVICE: return "no sm_100 CUDA device (or library not built for it)";
         case MHD_ERR_OUT_OF_MEMORY: return "out of device memory";
         case MHD_ERR_NO_STATE: return "no state set";
+        case MHD_ERR_TOO_LARGE: return "grid exceeds the fixed scratch of the allocation-free call";
     }
     return "unknown status";
 }
@@ -784,3 +786,155 @@ mhd_status mhd_last_cg_products(mhd_context* c, long long out[2]) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free implicit resistive rate (mhd_resistive_rate_noalloc in mhd_b200.h).
+//
+// All scratch of the solve -- the CG vectors x, r[2], p[2], the per-block partial sums and the
+// small control blocks (barrier counter, status, coefficients) -- is carved out of the one
+// file-scope array below. In host code g_noalloc_scratch is only a host-side stand-in for the
+// symbol; its device address is obtained per device with cudaGetSymbolAddress and passed to the
+// kernels.
+
+namespace {
+
+constexpr size_t kNoAllocCells = MHD_NOALLOC_MAX_CELLS;
+constexpr int kNoAllocMaxBlocks = 1024;
+constexpr size_t kNoAllocVecDoubles = 5 * kNoAllocCells;             // x, r0, r1, p0, p1
+constexpr size_t kNoAllocPartialDoubles = 2 * 4 * (size_t)kNoAllocMaxBlocks;
+constexpr size_t kNoAllocControlDoubles = 64;                        // CgSync, DeviceStatus, StepCoeffs
+constexpr size_t kNoAllocDoubles = kNoAllocVecDoubles + kNoAllocPartialDoubles + kNoAllocControlDoubles;
+static_assert(sizeof(CgSync) + sizeof(DeviceStatus) + sizeof(StepCoeffs) <= 8 * kNoAllocControlDoubles,
+              "control blocks exceed their reserved space");
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+struct NoAllocDevice {
+    bool ready = false;
+    double* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int grid = 0;               // co-resident blocks of the solver kernel
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+// Once per device, with that device current: resolve the array's address, size the solver grid.
+mhd_status noalloc_setup(int dev, NoAllocDevice** out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return MHD_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* addr = nullptr;
+        MHD_TRY(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+        MHD_TRY(cudaFuncSetAttribute(k_cg_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kCgRingBytes));
+        int occ = 0, sms = 0;
+        MHD_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_sweep, CGS_NT, kCgRingBytes));
+        MHD_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (occ < 1) return MHD_ERR_CUDA;
+        d.scratch = static_cast<double*>(addr);
+        d.grid = std::max(1, std::min(occ * sms, kNoAllocMaxBlocks));
+        d.ready = true;
+    }
+    *out = &d;
+    return MHD_OK;
+}
+
+}  // namespace
+
+extern "C" mhd_status mhd_resistive_rate_noalloc(const mhd_params* p, int solve_implicitly,
+                                                 double alpha, const double* bxf,
+                                                 const double* byf, double* bx_rate,
+                                                 double* by_rate, long long* cg_products,
+                                                 void* stream_ptr) {
+    if (!p || !bxf || !byf || !bx_rate || !by_rate) return MHD_ERR_INVALID_ARGUMENT;
+    if (p->nx < 2 || p->ny < 2 || !(p->dx > 0) || !(p->dy > 0) || !(p->eta >= 0) ||
+        !std::isfinite(alpha) || (solve_implicitly && !(alpha >= 0)))
+        return MHD_ERR_INVALID_ARGUMENT;
+    const size_t n = (size_t)p->nx * (size_t)p->ny;
+    if (n > kNoAllocCells) return MHD_ERR_TOO_LARGE;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    Domain D{p->nx, p->ny, p->dx, p->dy, p->eta, p->ct_mode};
+    int dev = 0;
+    MHD_TRY(cudaGetDevice(&dev));
+    NoAllocDevice* nd = nullptr;
+    mhd_status s = noalloc_setup(dev, &nd);
+    if (s != MHD_OK) return s;
+    int sms = 0;
+    MHD_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = std::max(1, std::min((int)((n + 255) / 256), sms * 8));
+    if (!solve_implicitly) {
+        k_corner_rates<<<blocks, 256, 0, stream>>>(D, nullptr, bxf, byf, bx_rate, by_rate);
+        MHD_TRY(cudaGetLastError());
+        if (cg_products) *cg_products = 0;
+        return MHD_OK;
+    }
+    // carve the scratch array
+    double* base = nd->scratch;
+    double* x = base;
+    double* r0 = base + kNoAllocCells;
+    double* r1 = base + 2 * kNoAllocCells;
+    double* p0 = base + 3 * kNoAllocCells;
+    double* p1 = base + 4 * kNoAllocCells;
+    double* partials = base + kNoAllocVecDoubles;
+    unsigned char* ctrl = reinterpret_cast<unsigned char*>(partials + kNoAllocPartialDoubles);
+    CgSync* sync = reinterpret_cast<CgSync*>(ctrl);
+    DeviceStatus* st = reinterpret_cast<DeviceStatus*>(ctrl + 64);
+    StepCoeffs* coeffs = reinterpret_cast<StepCoeffs*>(ctrl + 64 + 128);
+    static_assert(sizeof(CgSync) <= 64 && sizeof(DeviceStatus) <= 128 &&
+                      64 + 128 + sizeof(StepCoeffs) <= 8 * kNoAllocControlDoubles,
+                  "control block layout");
+    // what must start at zero: the barrier counter, the status and the coefficient block (the
+    // array keeps the previous call's contents)
+    MHD_TRY(cudaMemsetAsync(ctrl, 0, 8 * kNoAllocControlDoubles, stream));
+    k_set_alpha<<<1, 1, 0, stream>>>(coeffs, alpha);
+    MHD_TRY(cudaGetLastError());
+    // solver geometry as for a context (strips of CG_W columns, one wave of warps)
+    const int grid = std::max(1, std::min(nd->grid, (int)std::max<size_t>(1, (n + 63) / 64)));
+    const int strips_x = (p->nx + CG_W - 1) / CG_W;
+    const long long warps = (long long)grid * (CGS_NT / 32);
+    const int segs = (int)std::max(1LL, warps / strips_x);
+    const int seg_h = std::max(4, (p->ny + segs - 1) / segs);
+    CgSweepArgs a{};
+    a.D = D;
+    a.C = coeffs;
+    a.bxf = bxf;
+    a.byf = byf;
+    a.x = x;
+    a.r[0] = r0;
+    a.r[1] = r1;
+    a.p[0] = p0;
+    a.p[1] = p1;
+    a.partials = partials;
+    a.sync = sync;
+    a.st = st;
+    a.prods_out = nullptr;
+    a.solve_index = 0;
+    a.strips_x = strips_x;
+    a.seg_h = seg_h;
+    a.nwarps = strips_x * ((p->ny + seg_h - 1) / seg_h);
+    a.max_iters = p->cg_max_iters > 0 ? p->cg_max_iters : 2LL * (long long)n;
+    a.tol = p->cg_tol > 0 ? p->cg_tol : 2.220446049250313e-16;
+    a.timeout_s = p->cg_timeout_s > 0 ? p->cg_timeout_s : 30.0;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(CGS_NT);
+    cfg.dynamicSmemBytes = kCgRingBytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_sweep, a));
+    k_corner_rates<<<blocks, 256, 0, stream>>>(D, x, nullptr, nullptr, bx_rate, by_rate);
+    MHD_TRY(cudaGetLastError());
+    if (cg_products) {
+        DeviceStatus hs;
+        MHD_TRY(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+        MHD_TRY(cudaStreamSynchronize(stream));
+        *cg_products = hs.cg_products[0];
+        return status_from_flags(hs.flags);
+    }
+    return MHD_OK;
+}
