@@ -166,6 +166,63 @@ void* mhd_stream(mhd_context* ctx);
 /* Number of kernel launches one mhd_step enqueues (for launch accounting). */
 int mhd_launches_per_step(mhd_context* ctx);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched stepping (no counterpart in the reference, which advances one Grid per process):
+ * `count` independent periodic simulations, each with its own mhd_params (size, spacing, eta,
+ * courant, safety, ct_mode, solver tolerance), advanced together. Each step is one launch per
+ * stage for the whole batch (coefficients, stage 1, implicit solve, stage 2, implicit solve,
+ * finalize; the solves take one launch per 64 instances). Every instance gets exactly the step
+ * it would get from its own mhd_context: its own CFL dt, its own matrix coefficient, its own CG
+ * convergence. States are dense nx*ny planes in the order rho, mx, my, E, bxf, byf. */
+typedef struct mhd_batch mhd_batch;
+
+/* Work decomposition of the batch kernels, chosen by mhd_batch_autotune. */
+typedef struct mhd_batch_tuning {
+    int stage_rows;  /* rows per work item of the explicit stages and the finalize (>= 1) */
+    int cg_rows;     /* rows per work item of the implicit solve (>= 1) */
+    int cg_order;    /* solver items dealt to warps 0: instance by instance, 1: interleaved */
+    int pad;
+    double stage_ms; /* device time of the explicit kernels in the tuning step (output only) */
+    double cg_ms;    /* device time of the solver launches in the tuning step (output only) */
+} mhd_batch_tuning;
+
+/* params: count parameter blocks. stream: a cudaStream_t (NULL = a new non-blocking stream). */
+mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, mhd_batch** out);
+mhd_status mhd_batch_destroy(mhd_batch* b);
+int mhd_batch_count(mhd_batch* b);
+/* Upload / download instance `index`'s state: host (or device) pointers to dense planes. */
+mhd_status mhd_batch_set_state(mhd_batch* b, int index, const double* const fields[6]);
+mhd_status mhd_batch_get_state(mhd_batch* b, int index, double* const fields[6]);
+mhd_status mhd_batch_set_state_device(mhd_batch* b, int index, const double* const fields[6]);
+mhd_status mhd_batch_get_state_device(mhd_batch* b, int index, double* const fields[6]);
+/* As mhd_set_implicit_coefficient, for one instance. */
+mhd_status mhd_batch_set_implicit_coefficient(mhd_batch* b, int index, double alpha);
+/* One step of every instance; dts: host array of count steps (<= 0: that instance's CFL step),
+ * or NULL for CFL steps throughout. Asynchronous. */
+mhd_status mhd_batch_step(mhd_batch* b, const double* dts);
+/* mhd_run for every instance at once (the driver loop of src/integrator_main.cpp:76-112 per
+ * instance), captured as a CUDA graph. dts_out[count][nsteps] and
+ * cg_products_out[count][nsteps][2], if not NULL, are host arrays filled on return. */
+mhd_status mhd_batch_run(mhd_batch* b, int nsteps, double dt_fixed, double t_end, double* dts_out,
+                         long long* cg_products_out);
+/* Time one step of the current states under candidate decompositions and keep the fastest
+ * (the states, times and step counters are restored afterwards). All states must be set.
+ * *out (may be NULL) receives the choice. Synchronous. */
+mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out);
+mhd_status mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t);
+mhd_status mhd_batch_get_tuning(mhd_batch* b, mhd_batch_tuning* t);
+/* Wait; return the worst device status over the batch and clear it. per_instance (may be NULL)
+ * receives count statuses. */
+mhd_status mhd_batch_synchronize(mhd_batch* b, mhd_status* per_instance);
+/* Matrix-vector products of each instance's last two solves: out[count][2] (after synchronize). */
+mhd_status mhd_batch_last_cg_products(mhd_batch* b, long long* out);
+/* As mhd_cfl_dt and mhd_divb, for one instance. */
+mhd_status mhd_batch_cfl_dt(mhd_batch* b, int index, double* dt);
+mhd_status mhd_batch_divb(mhd_batch* b, int index, double* rms, double* maxabs);
+void* mhd_batch_stream(mhd_batch* b);
+/* Kernel launches one mhd_batch_step enqueues. */
+int mhd_batch_launches_per_step(mhd_batch* b);
+
 const char* mhd_status_string(mhd_status s);
 
 /* 1 when a device this library was built for is present, else 0. */

@@ -4,6 +4,7 @@ The product is the shared library ``libmhd_b200.so`` (CUDA kernels + the C ABI o
 ``include/mhd_b200.h``); this package is its Python mirror:
 
 * :class:`Context` -- one device-resident simulation (set_state / step / run / cfl_dt / divb);
+* :class:`Batch` -- many independent simulations of uneven sizes stepped together;
 * :mod:`problems` -- the benchmark initial conditions.
 """
 from .capi import (  # noqa: F401
@@ -12,6 +13,7 @@ from .capi import (  # noqa: F401
     FIELDS,
     LAYOUT_DENSE,
     LAYOUT_PADDED,
+    Batch,
     Context,
     MHDError,
     ars_gamma,
@@ -21,6 +23,7 @@ from .capi import (  # noqa: F401
 from . import problems  # noqa: F401
 
 __all__ = [
+    "Batch",
     "Context",
     "MHDError",
     "FIELDS",

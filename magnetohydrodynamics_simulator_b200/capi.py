@@ -25,6 +25,7 @@ STATUS_NAMES = {
     6: "MHD_ERR_NO_DEVICE",
     7: "MHD_ERR_OUT_OF_MEMORY",
     8: "MHD_ERR_NO_STATE",
+    9: "MHD_ERR_TOO_LARGE",
 }
 LAYOUT_DENSE = 0
 LAYOUT_PADDED = 1
@@ -53,6 +54,17 @@ class Params(ctypes.Structure):
         ("courant", ctypes.c_double),
         ("safety", ctypes.c_double),
         ("cg_timeout_s", ctypes.c_double),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("stage_rows", ctypes.c_int),
+        ("cg_rows", ctypes.c_int),
+        ("cg_order", ctypes.c_int),
+        ("pad", ctypes.c_int),
+        ("stage_ms", ctypes.c_double),
+        ("cg_ms", ctypes.c_double),
     ]
 
 
@@ -98,6 +110,31 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_status_string.argtypes = [ctypes.c_int]
     lib.mhd_status_string.restype = ctypes.c_char_p
     lib.mhd_device_available.argtypes = []
+    ip = ctypes.POINTER(ctypes.c_int)
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    tp = ctypes.POINTER(BatchTuning)
+    lib.mhd_batch_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, vp, ctypes.POINTER(vp)]
+    lib.mhd_batch_destroy.argtypes = [vp]
+    lib.mhd_batch_count.argtypes = [vp]
+    lib.mhd_batch_set_state.argtypes = [vp, ctypes.c_int, P6]
+    lib.mhd_batch_get_state.argtypes = [vp, ctypes.c_int, P6]
+    lib.mhd_batch_set_state_device.argtypes = [vp, ctypes.c_int, P6]
+    lib.mhd_batch_get_state_device.argtypes = [vp, ctypes.c_int, P6]
+    lib.mhd_batch_set_implicit_coefficient.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    lib.mhd_batch_step.argtypes = [vp, _dp]
+    lib.mhd_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, llp]
+    lib.mhd_batch_autotune.argtypes = [vp, tp]
+    lib.mhd_batch_set_tuning.argtypes = [vp, tp]
+    lib.mhd_batch_get_tuning.argtypes = [vp, tp]
+    lib.mhd_batch_synchronize.argtypes = [vp, ip]
+    lib.mhd_batch_last_cg_products.argtypes = [vp, llp]
+    lib.mhd_batch_cfl_dt.argtypes = [vp, ctypes.c_int, _dp]
+    lib.mhd_batch_divb.argtypes = [vp, ctypes.c_int, _dp, _dp]
+    lib.mhd_batch_stream.argtypes = [vp]
+    lib.mhd_batch_stream.restype = vp
+    lib.mhd_batch_launches_per_step.argtypes = [vp]
+    lib.mhd_resistive_rate_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_double,
+                                               vp, vp, vp, vp, llp, vp]
     _lib = lib
     return lib
 
@@ -256,6 +293,144 @@ class Context:
     @property
     def launches_per_step(self) -> int:
         return int(self.lib.mhd_launches_per_step(self.h))
+
+
+class Batch:
+    """Many independent periodic simulations of uneven sizes stepped together (one launch per
+    stage for the whole batch). Each instance is specified like a Context: a dict with keys
+    nx, ny, dx, dy, eta and optionally ct_mode, cg_tol, cg_max_iters, courant, safety,
+    cg_timeout_s."""
+
+    def __init__(self, instances: Sequence[dict], stream: int | None = None):
+        self.lib = load_library()
+        n = len(instances)
+        arr = (Params * n)()
+        self.shapes = []
+        for k, spec in enumerate(instances):
+            p = arr[k]
+            _check(self.lib.mhd_default_params(ctypes.byref(p), int(spec["nx"]), int(spec["ny"]),
+                                               float(spec["dx"]), float(spec["dy"]),
+                                               float(spec["eta"])), "mhd_default_params")
+            for key in ("ct_mode", "cg_tol", "cg_max_iters", "courant", "safety", "cg_timeout_s"):
+                if key in spec:
+                    setattr(p, key, spec[key])
+            self.shapes.append((int(spec["ny"]), int(spec["nx"])))
+        self.params = arr
+        h = ctypes.c_void_p()
+        _check(self.lib.mhd_batch_create(arr, n, ctypes.c_void_p(stream) if stream else None,
+                                         ctypes.byref(h)), "mhd_batch_create")
+        self.h = h
+        self.count = n
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return self.count
+
+    def set_state(self, index: int, fields: Sequence[np.ndarray]):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+        for f in fs:
+            if f.shape != self.shapes[index]:
+                raise ValueError(f"field shape {f.shape} != {self.shapes[index]}")
+        _check(self.lib.mhd_batch_set_state(self.h, index, _host_ptrs(fs)), "mhd_batch_set_state")
+
+    def get_state(self, index: int):
+        out = [np.empty(self.shapes[index]) for _ in range(6)]
+        _check(self.lib.mhd_batch_get_state(self.h, index, _host_ptrs(out)), "mhd_batch_get_state")
+        return out
+
+    def get_state_into(self, index: int, out: Sequence[np.ndarray]):
+        _check(self.lib.mhd_batch_get_state(self.h, index, _host_ptrs(out)), "mhd_batch_get_state")
+
+    def set_state_device(self, index: int, ptrs: Sequence[int]):
+        _check(self.lib.mhd_batch_set_state_device(self.h, index, _device_ptrs(ptrs)),
+               "mhd_batch_set_state_device")
+
+    def get_state_device(self, index: int, ptrs: Sequence[int]):
+        _check(self.lib.mhd_batch_get_state_device(self.h, index, _device_ptrs(ptrs)),
+               "mhd_batch_get_state_device")
+
+    def set_implicit_coefficient(self, index: int, alpha: float):
+        _check(self.lib.mhd_batch_set_implicit_coefficient(self.h, index, alpha),
+               "mhd_batch_set_implicit_coefficient")
+
+    def step(self, dts: Sequence[float] | None = None):
+        if dts is None:
+            _check(self.lib.mhd_batch_step(self.h, None), "mhd_batch_step")
+            return
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        if d.shape != (self.count,):
+            raise ValueError("dts must hold one dt per instance")
+        _check(self.lib.mhd_batch_step(self.h, d.ctypes.data_as(_dp)), "mhd_batch_step")
+
+    def run(self, nsteps: int, dt_fixed: float = 0.0, t_end: float = 0.0, record: bool = True):
+        """Returns dts[count, nsteps] and cg_products[count, nsteps, 2] (None, None unless
+        record)."""
+        dts = np.zeros((self.count, nsteps)) if record else None
+        prods = np.zeros((self.count, nsteps, 2), dtype=np.int64) if record else None
+        _check(self.lib.mhd_batch_run(
+            self.h, nsteps, dt_fixed, t_end, dts.ctypes.data_as(_dp) if record else None,
+            prods.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)) if record else None),
+            "mhd_batch_run")
+        return dts, prods
+
+    def autotune(self) -> dict:
+        t = BatchTuning()
+        _check(self.lib.mhd_batch_autotune(self.h, ctypes.byref(t)), "mhd_batch_autotune")
+        return {k: getattr(t, k) for k in ("stage_rows", "cg_rows", "cg_order", "stage_ms", "cg_ms")}
+
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        _check(self.lib.mhd_batch_get_tuning(self.h, ctypes.byref(t)), "mhd_batch_get_tuning")
+        return {k: getattr(t, k) for k in ("stage_rows", "cg_rows", "cg_order", "stage_ms", "cg_ms")}
+
+    def set_tuning(self, stage_rows: int, cg_rows: int, cg_order: int = 0):
+        t = BatchTuning(stage_rows, cg_rows, cg_order, 0, 0.0, 0.0)
+        _check(self.lib.mhd_batch_set_tuning(self.h, ctypes.byref(t)), "mhd_batch_set_tuning")
+
+    def synchronize_status(self):
+        """(worst status, per-instance statuses); clears the device statuses."""
+        per = (ctypes.c_int * self.count)()
+        worst = int(self.lib.mhd_batch_synchronize(self.h, per))
+        return worst, [int(v) for v in per]
+
+    def synchronize(self):
+        worst, _ = self.synchronize_status()
+        _check(worst, "mhd_batch_synchronize")
+
+    def last_cg_products(self) -> np.ndarray:
+        out = np.zeros((self.count, 2), dtype=np.int64)
+        _check(self.lib.mhd_batch_last_cg_products(
+            self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))), "mhd_batch_last_cg_products")
+        return out
+
+    def cfl_dt(self, index: int) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.mhd_batch_cfl_dt(self.h, index, ctypes.byref(v)), "mhd_batch_cfl_dt")
+        return v.value
+
+    def divb(self, index: int):
+        rms, mx = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.mhd_batch_divb(self.h, index, ctypes.byref(rms), ctypes.byref(mx)),
+               "mhd_batch_divb")
+        return rms.value, mx.value
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mhd_batch_stream(self.h) or 0
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self.lib.mhd_batch_launches_per_step(self.h))
 
 
 def ars_gamma() -> float:

@@ -1,0 +1,764 @@
+// Host side of the batched C ABI (mhd_batch_* in include/mhd_b200.h): device memory plan of a
+// batch of independent periodic simulations, the work-item lists of the batch kernels
+// (mhd_batch.cuh), the launch sequence of one batched step, the CUDA-graph driver loop, the
+// autotuner and per-instance diagnostics.
+//
+// Device memory: instance i owns 23 dense nx_i*ny_i FP64 planes in one pool (the same plan as a
+// single context: S[6] state, T[6] predictor, A[6] accumulator, x, r[2], p[2]) plus its own
+// StepCoeffs and DeviceStatus. The descriptor array (BatchInst) is kept for even and odd steps,
+// which differ only in the trading hydro planes of S and A.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "mhd_batch.cuh"
+#include "mhd_host_util.h"
+
+using namespace mhd;
+
+namespace {
+
+constexpr int kBatchPlanes = 23;
+constexpr int kQueues = 3;  // work counters: stage 1, stage 2, finalize
+
+// Candidate decompositions the autotuner times (rows per work item; solver dealing order).
+constexpr int kStageRowsCand[] = {16, 32, 64, 128, 256};
+constexpr int kCgRowsCand[] = {8, 16, 32, 64, 128};
+
+}  // namespace
+
+struct mhd_batch {
+    int count = 0;
+    std::vector<mhd_params> prm;
+    std::vector<size_t> ncell;
+    size_t total_cells = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int num_sms = 0;
+    double* pool = nullptr;
+    StepCoeffs* coeffs = nullptr;    // [count]
+    DeviceStatus* status = nullptr;  // [count]
+    BatchInst* d_insts[2] = {nullptr, nullptr};
+    std::vector<BatchInst> h_insts[2];
+    int parity = 0;  // descriptor array of the next step
+    // work items: explicit stages / finalize, then the solver's (chunk by chunk)
+    WorkItem* d_items = nullptr;
+    size_t items_cap = 0;
+    int n_stage_items = 0;
+    int n_cg_items = 0;
+    int nchunks = 0;
+    std::vector<int> chunk_item0, chunk_nitems;
+    int stage_occ[2] = {0, 0}, fin_occ = 0, cg_occ = 0;
+    int stage_grid[2] = {0, 0}, fin_grid = 0, cg_grid = 0;
+    double* partials = nullptr;  // [2][CGB_MAX_INST][cg_occ * num_sms][4]
+    CgSync* syncs = nullptr;     // [2 * nchunks]
+    int* queues = nullptr;       // [kQueues]
+    double* dt_dev = nullptr;    // [count] per-instance dt of mhd_batch_step
+    double* divb_partial = nullptr;
+    double* divb_out = nullptr;
+    int divb_blocks = 0;
+    DeviceStatus* host_status = nullptr;  // pinned [count]
+    double* host_small = nullptr;         // pinned [8]
+    std::vector<char> have_state;
+    mhd_batch_tuning tuning{};
+    double g = 0.0, d = 0.0;
+    double timeout_s = 30.0;
+    double* rec_dts = nullptr;       // [count][rec_cap]
+    long long* rec_prods = nullptr;  // [count][rec_cap][2]
+    int rec_cap = 0;
+};
+
+namespace {
+
+mhd_status check_batch(mhd_batch* b) {
+    if (!b) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(b->device));
+    return MHD_OK;
+}
+
+mhd_status check_index(mhd_batch* b, int index) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    return (index >= 0 && index < b->count) ? MHD_OK : MHD_ERR_INVALID_ARGUMENT;
+}
+
+bool all_states_set(const mhd_batch* b) {
+    for (char h : b->have_state)
+        if (!h) return false;
+    return true;
+}
+
+int grid_for(int occ_blocks, int num_sms, int nitems, int warps_per_block) {
+    const long long need = ((long long)nitems + warps_per_block - 1) / warps_per_block;
+    return (int)std::max(1LL, std::min((long long)occ_blocks * num_sms, need));
+}
+
+// Build the work-item lists and the descriptors' decomposition for tuning t, and upload both.
+mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
+    if (t.stage_rows < 1 || t.cg_rows < 1 || (t.cg_order != 0 && t.cg_order != 1))
+        return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaStreamSynchronize(b->stream));  // in-flight steps still read the old lists
+    std::vector<WorkItem> st_items, cg_items;
+    std::vector<int> st_rows;
+    std::vector<int> cg_nw(b->count);
+    for (int i = 0; i < b->count; ++i) {
+        const int nx = b->prm[i].nx, ny = b->prm[i].ny;
+        SweepGeom sg;
+        sg.strips_x = (nx + SW_OUT - 1) / SW_OUT;
+        sg.seg_h = std::min(t.stage_rows, ny);
+        sg.segs_y = (ny + sg.seg_h - 1) / sg.seg_h;
+        sg.nwarps = sg.strips_x * sg.segs_y;
+        const int cg_strips = (nx + CG_W - 1) / CG_W;
+        const int cg_seg = std::min(t.cg_rows, ny);
+        cg_nw[i] = cg_strips * ((ny + cg_seg - 1) / cg_seg);
+        for (int p = 0; p < 2; ++p) {
+            BatchInst& I = b->h_insts[p][i];
+            I.sg = sg;
+            I.cg_strips_x = cg_strips;
+            I.cg_seg_h = cg_seg;
+        }
+        for (int w = 0; w < sg.nwarps; ++w) {
+            st_items.push_back(WorkItem{i, w});
+            const int sy = w / sg.strips_x;
+            st_rows.push_back(std::min(sg.seg_h, ny - sy * sg.seg_h));
+        }
+    }
+    // largest items first (the explicit kernels take items from a counter)
+    std::vector<int> order(st_items.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return st_rows[a] > st_rows[c]; });
+    std::vector<WorkItem> items;
+    items.reserve(st_items.size());
+    for (int k : order) items.push_back(st_items[k]);
+    // solver items, chunk by chunk
+    b->chunk_item0.assign(b->nchunks, 0);
+    b->chunk_nitems.assign(b->nchunks, 0);
+    int max_chunk_items = 0;
+    for (int c = 0; c < b->nchunks; ++c) {
+        const int i0 = c * CGB_MAX_INST, i1 = std::min(b->count, i0 + CGB_MAX_INST);
+        b->chunk_item0[c] = (int)items.size();
+        const size_t before = items.size();
+        if (t.cg_order == 0) {
+            for (int i = i0; i < i1; ++i)
+                for (int w = 0; w < cg_nw[i]; ++w) items.push_back(WorkItem{i, w});
+        } else {
+            int most = 0;
+            for (int i = i0; i < i1; ++i) most = std::max(most, cg_nw[i]);
+            for (int w = 0; w < most; ++w)
+                for (int i = i0; i < i1; ++i)
+                    if (w < cg_nw[i]) items.push_back(WorkItem{i, w});
+        }
+        b->chunk_nitems[c] = (int)(items.size() - before);
+        max_chunk_items = std::max(max_chunk_items, b->chunk_nitems[c]);
+    }
+    b->n_stage_items = (int)st_items.size();
+    b->n_cg_items = (int)(items.size() - st_items.size());
+    if (items.size() > b->items_cap) {
+        cudaFree(b->d_items);
+        b->d_items = nullptr;
+        b->items_cap = 0;
+        MHD_TRY(cudaMalloc(&b->d_items, items.size() * sizeof(WorkItem)));
+        b->items_cap = items.size();
+    }
+    MHD_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(WorkItem),
+                       cudaMemcpyHostToDevice));
+    for (int p = 0; p < 2; ++p)
+        MHD_TRY(cudaMemcpy(b->d_insts[p], b->h_insts[p].data(), b->count * sizeof(BatchInst),
+                           cudaMemcpyHostToDevice));
+    b->stage_grid[0] = grid_for(b->stage_occ[0], b->num_sms, b->n_stage_items, SW_WARPS);
+    b->stage_grid[1] = grid_for(b->stage_occ[1], b->num_sms, b->n_stage_items, SW_WARPS);
+    b->fin_grid = grid_for(b->fin_occ, b->num_sms, b->n_stage_items, FS_WARPS);
+    b->cg_grid = grid_for(b->cg_occ, b->num_sms, max_chunk_items, CGS_NT / 32);
+    b->tuning.stage_rows = t.stage_rows;
+    b->tuning.cg_rows = t.cg_rows;
+    b->tuning.cg_order = t.cg_order;
+    return MHD_OK;
+}
+
+mhd_status launch_cg_chunks(mhd_batch* b, const BatchInst* insts, int solve, bool record) {
+    for (int c = 0; c < b->nchunks; ++c) {
+        CgBatchArgs a{};
+        a.insts = insts;
+        a.inst0 = c * CGB_MAX_INST;
+        a.ninst = std::min(CGB_MAX_INST, b->count - a.inst0);
+        a.items = b->d_items + b->chunk_item0[c];
+        a.nitems = b->chunk_nitems[c];
+        a.partials = b->partials;
+        a.sync = b->syncs + 2 * c + solve;
+        a.solve_index = solve;
+        a.rec_stride = b->rec_cap;
+        a.prods_rec = record ? b->rec_prods : nullptr;
+        a.timeout_s = b->timeout_s;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(b->cg_grid);
+        cfg.blockDim = dim3(CGS_NT);
+        cfg.dynamicSmemBytes = kCgRingBytes;
+        cfg.stream = b->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_batch, a));
+    }
+    return MHD_OK;
+}
+
+// One batched step with the descriptors of the current parity. dt_in: device array of per-instance
+// dts or null (then dt_fixed for all; <= 0 selects the CFL step). run_mode: alpha rule of
+// instances without a fixed coefficient (1: from dt, 2: the driver's rule). ev: 6 events around
+// the kernels (stage 1, solve 0, stage 2, solve 1, finalize) or null.
+mhd_status enqueue_step(mhd_batch* b, const double* dt_in, double dt_fixed, int run_mode,
+                        double t_end, bool record, cudaEvent_t* ev) {
+    const BatchInst* I = b->d_insts[b->parity];
+    const int nthreads = std::max(std::max(b->count, 2 * b->nchunks), kQueues);
+    k_batch_coeffs<<<(nthreads + 127) / 128, 128, 0, b->stream>>>(
+        I, b->count, dt_in, dt_fixed, run_mode, t_end, b->g, b->d, record ? b->rec_dts : nullptr,
+        b->rec_cap, b->queues, kQueues, b->syncs, 2 * b->nchunks);
+    MHD_TRY(cudaGetLastError());
+    if (ev) MHD_TRY(cudaEventRecord(ev[0], b->stream));
+    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, 0, b->stream>>>(I, b->d_items,
+                                                                        b->n_stage_items, b->queues);
+    MHD_TRY(cudaGetLastError());
+    if (ev) MHD_TRY(cudaEventRecord(ev[1], b->stream));
+    mhd_status s = launch_cg_chunks(b, I, 0, record);
+    if (s != MHD_OK) return s;
+    if (ev) MHD_TRY(cudaEventRecord(ev[2], b->stream));
+    k_stage_batch<2><<<b->stage_grid[1], 32 * SW_WARPS, 0, b->stream>>>(
+        I, b->d_items, b->n_stage_items, b->queues + 1);
+    MHD_TRY(cudaGetLastError());
+    if (ev) MHD_TRY(cudaEventRecord(ev[3], b->stream));
+    s = launch_cg_chunks(b, I, 1, record);
+    if (s != MHD_OK) return s;
+    if (ev) MHD_TRY(cudaEventRecord(ev[4], b->stream));
+    k_finalize_batch<<<b->fin_grid, 32 * FS_WARPS, 0, b->stream>>>(I, b->d_items, b->n_stage_items,
+                                                                   b->queues + 2);
+    MHD_TRY(cudaGetLastError());
+    if (ev) MHD_TRY(cudaEventRecord(ev[5], b->stream));
+    b->parity ^= 1;
+    return MHD_OK;
+}
+
+mhd_status refresh_cfl(mhd_batch* b, int i) {
+    const BatchInst& I = b->h_insts[b->parity][i];
+    MHD_TRY(cudaMemsetAsync(&b->status[i].smax_bits, 0, sizeof(unsigned long long), b->stream));
+    const int blocks = std::max(1, std::min((int)((b->ncell[i] + 255) / 256), b->num_sms * 8));
+    CPlanes u;
+    for (int k = 0; k < 6; ++k) u.f[k] = I.S[k];
+    k_cfl_scan<<<blocks, 256, 0, b->stream>>>(I.D, u, b->status + i);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status read_status(mhd_batch* b) {
+    MHD_TRY(cudaMemcpyAsync(b->host_status, b->status, b->count * sizeof(DeviceStatus),
+                            cudaMemcpyDeviceToHost, b->stream));
+    MHD_TRY(cudaStreamSynchronize(b->stream));
+    return MHD_OK;
+}
+
+mhd_status status_of(unsigned flags) {
+    if (flags & kStatusTimeout) return MHD_ERR_TIMEOUT;
+    if (flags & kStatusNonFinite) return MHD_ERR_NONFINITE;
+    if (flags & kStatusCgNotConverged) return MHD_ERR_CG_NOT_CONVERGED;
+    return MHD_OK;
+}
+
+int severity(mhd_status s) {
+    switch (s) {
+        case MHD_ERR_TIMEOUT: return 3;
+        case MHD_ERR_NONFINITE: return 2;
+        case MHD_ERR_CG_NOT_CONVERGED: return 1;
+        default: return 0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, mhd_batch** out) {
+    if (!params || !out || count < 1) return MHD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    for (int i = 0; i < count; ++i) {
+        const mhd_params& p = params[i];
+        if (p.nx < 2 || p.ny < 2 || !(p.dx > 0) || !(p.dy > 0) || !(p.eta >= 0) ||
+            (p.ct_mode != 0 && p.ct_mode != 1) || (long long)p.nx * p.ny > (1LL << 31))
+            return MHD_ERR_INVALID_ARGUMENT;
+    }
+    if (!mhd_device_available()) return MHD_ERR_NO_DEVICE;
+    mhd_batch* b = new (std::nothrow) mhd_batch();
+    if (!b) return MHD_ERR_OUT_OF_MEMORY;
+    auto fail = [&](mhd_status s) {
+        mhd_batch_destroy(b);
+        return s;
+    };
+    b->count = count;
+    b->prm.assign(params, params + count);
+    b->ncell.resize(count);
+    b->have_state.assign(count, 0);
+    b->g = (2.0 - sqrt(2.0)) / 2.0;     // solvers.hpp:41
+    b->d = 1.0 - (1.0 / (2.0 * b->g));  // solvers.hpp:42
+    b->timeout_s = 0.0;
+    for (int i = 0; i < count; ++i) {
+        mhd_params& p = b->prm[i];
+        if (!(p.courant > 0)) p.courant = 0.5;
+        if (!(p.safety > 0)) p.safety = 0.9;
+        if (!(p.cg_timeout_s > 0)) p.cg_timeout_s = 30.0;
+        b->timeout_s = std::max(b->timeout_s, p.cg_timeout_s);
+        b->ncell[i] = (size_t)p.nx * (size_t)p.ny;
+        b->total_cells += b->ncell[i];
+    }
+    b->nchunks = (count + CGB_MAX_INST - 1) / CGB_MAX_INST;
+    if (cudaGetDevice(&b->device) != cudaSuccess) return fail(MHD_ERR_NO_DEVICE);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, b->device) != cudaSuccess) return fail(MHD_ERR_NO_DEVICE);
+    b->num_sms = prop.multiProcessorCount;
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(MHD_ERR_CUDA);
+        b->own_stream = true;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->stage_occ[0], k_stage_batch<1>,
+                                                      32 * SW_WARPS, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->stage_occ[1], k_stage_batch<2>,
+                                                      32 * SW_WARPS, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->fin_occ, k_finalize_batch, 32 * FS_WARPS,
+                                                      0) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cg_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCgRingBytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->cg_occ, k_cg_batch, CGS_NT, kCgRingBytes) !=
+            cudaSuccess ||
+        b->stage_occ[0] < 1 || b->stage_occ[1] < 1 || b->fin_occ < 1 || b->cg_occ < 1) {
+        cudaGetLastError();
+        return fail(MHD_ERR_CUDA);
+    }
+    b->cg_occ = std::min(b->cg_occ, std::max(1, mhd_host::env_int("MHD_B200_CG_BLOCKS_PER_SM", 1)));
+    const size_t max_cg_grid = (size_t)b->cg_occ * b->num_sms;
+    size_t max_cells = 0;
+    for (size_t n : b->ncell) max_cells = std::max(max_cells, n);
+    b->divb_blocks = std::max(1, std::min((int)((max_cells + 255) / 256), b->num_sms * 4));
+    if (cudaMalloc(&b->pool, (size_t)kBatchPlanes * b->total_cells * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&b->coeffs, count * sizeof(StepCoeffs)) != cudaSuccess ||
+        cudaMalloc(&b->status, count * sizeof(DeviceStatus)) != cudaSuccess ||
+        cudaMalloc(&b->d_insts[0], count * sizeof(BatchInst)) != cudaSuccess ||
+        cudaMalloc(&b->d_insts[1], count * sizeof(BatchInst)) != cudaSuccess ||
+        cudaMalloc(&b->partials, 2 * (size_t)CGB_MAX_INST * max_cg_grid * 4 * sizeof(double)) !=
+            cudaSuccess ||
+        cudaMalloc(&b->syncs, 2 * (size_t)b->nchunks * sizeof(CgSync)) != cudaSuccess ||
+        cudaMalloc(&b->queues, kQueues * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->dt_dev, count * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&b->divb_partial, 2 * (size_t)b->divb_blocks * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&b->divb_out, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&b->host_status, count * sizeof(DeviceStatus)) != cudaSuccess ||
+        cudaMallocHost(&b->host_small, 8 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MHD_ERR_OUT_OF_MEMORY);
+    }
+    // descriptors
+    for (int p = 0; p < 2; ++p) b->h_insts[p].assign(count, BatchInst{});
+    double* q = b->pool;
+    for (int i = 0; i < count; ++i) {
+        const mhd_params& p = b->prm[i];
+        const size_t n = b->ncell[i];
+        BatchInst I{};
+        I.D.nx = p.nx;
+        I.D.ny = p.ny;
+        I.D.dx = p.dx;
+        I.D.dy = p.dy;
+        I.D.eta = p.eta;
+        I.D.ct_mode = p.ct_mode;
+        I.C = b->coeffs + i;
+        I.st = b->status + i;
+        for (int k = 0; k < 6; ++k) I.S[k] = q + (size_t)k * n;
+        for (int k = 0; k < 6; ++k) I.T[k] = q + (size_t)(6 + k) * n;
+        for (int k = 0; k < 6; ++k) I.A[k] = q + (size_t)(12 + k) * n;
+        I.x = q + 18 * n;
+        I.r[0] = q + 19 * n;
+        I.r[1] = q + 20 * n;
+        I.p[0] = q + 21 * n;
+        I.p[1] = q + 22 * n;
+        I.max_iters = p.cg_max_iters > 0 ? p.cg_max_iters : 2LL * (long long)n;
+        I.tol = p.cg_tol > 0 ? p.cg_tol : 2.220446049250313e-16;
+        I.alpha = 0.0;
+        I.alpha_fixed = 0;
+        I.hmin = std::min(p.dx, p.dy);
+        I.courant = p.courant;
+        I.safety = p.safety;
+        b->h_insts[0][i] = I;
+        for (int k = 0; k < 4; ++k) std::swap(I.S[k], I.A[k]);  // odd steps
+        b->h_insts[1][i] = I;
+        q += (size_t)kBatchPlanes * n;
+    }
+    if (cudaMemsetAsync(b->status, 0, count * sizeof(DeviceStatus), b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->coeffs, 0, count * sizeof(StepCoeffs), b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->pool, 0, (size_t)kBatchPlanes * b->total_cells * sizeof(double),
+                        b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->syncs, 0, 2 * (size_t)b->nchunks * sizeof(CgSync), b->stream) !=
+            cudaSuccess)
+        return fail(MHD_ERR_CUDA);
+    mhd_batch_tuning t{};
+    t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", 32);
+    t.cg_rows = mhd_host::env_int("MHD_B200_BATCH_CG_ROWS", 32);
+    t.cg_order = mhd_host::env_int("MHD_B200_BATCH_CG_ORDER", 0);
+    const mhd_status s = apply_tuning(b, t);
+    if (s != MHD_OK) return fail(s);
+    *out = b;
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_destroy(mhd_batch* b) {
+    if (!b) return MHD_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaFree(b->pool);
+    cudaFree(b->coeffs);
+    cudaFree(b->status);
+    cudaFree(b->d_insts[0]);
+    cudaFree(b->d_insts[1]);
+    cudaFree(b->d_items);
+    cudaFree(b->partials);
+    cudaFree(b->syncs);
+    cudaFree(b->queues);
+    cudaFree(b->dt_dev);
+    cudaFree(b->divb_partial);
+    cudaFree(b->divb_out);
+    cudaFree(b->rec_dts);
+    cudaFree(b->rec_prods);
+    if (b->host_status) cudaFreeHost(b->host_status);
+    if (b->host_small) cudaFreeHost(b->host_small);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    cudaGetLastError();
+    delete b;
+    return MHD_OK;
+}
+
+int mhd_batch_count(mhd_batch* b) { return b ? b->count : 0; }
+
+void* mhd_batch_stream(mhd_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int mhd_batch_launches_per_step(mhd_batch* b) { return b ? 4 + 2 * b->nchunks : 0; }
+
+static mhd_status batch_copy_in(mhd_batch* b, int index, const double* const f[6],
+                                cudaMemcpyKind kind) {
+    mhd_status s = check_index(b, index);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k)
+        if (!f[k]) return MHD_ERR_INVALID_ARGUMENT;
+    const BatchInst& I = b->h_insts[b->parity][index];
+    for (int k = 0; k < 6; ++k)
+        MHD_TRY(cudaMemcpyAsync(I.S[k], f[k], b->ncell[index] * sizeof(double), kind, b->stream));
+    b->have_state[index] = 1;
+    return refresh_cfl(b, index);
+}
+
+static mhd_status batch_copy_out(mhd_batch* b, int index, double* const f[6], cudaMemcpyKind kind) {
+    mhd_status s = check_index(b, index);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    if (!b->have_state[index]) return MHD_ERR_NO_STATE;
+    const BatchInst& I = b->h_insts[b->parity][index];
+    for (int k = 0; k < 6; ++k) {
+        if (!f[k]) continue;
+        MHD_TRY(cudaMemcpyAsync(f[k], I.S[k], b->ncell[index] * sizeof(double), kind, b->stream));
+    }
+    if (kind == cudaMemcpyDeviceToHost) MHD_TRY(cudaStreamSynchronize(b->stream));
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_set_state(mhd_batch* b, int index, const double* const f[6]) {
+    return batch_copy_in(b, index, f, cudaMemcpyHostToDevice);
+}
+mhd_status mhd_batch_set_state_device(mhd_batch* b, int index, const double* const f[6]) {
+    return batch_copy_in(b, index, f, cudaMemcpyDeviceToDevice);
+}
+mhd_status mhd_batch_get_state(mhd_batch* b, int index, double* const f[6]) {
+    return batch_copy_out(b, index, f, cudaMemcpyDeviceToHost);
+}
+mhd_status mhd_batch_get_state_device(mhd_batch* b, int index, double* const f[6]) {
+    return batch_copy_out(b, index, f, cudaMemcpyDeviceToDevice);
+}
+
+mhd_status mhd_batch_set_implicit_coefficient(mhd_batch* b, int index, double alpha) {
+    mhd_status s = check_index(b, index);
+    if (s != MHD_OK) return s;
+    if (!(alpha >= 0) || !std::isfinite(alpha)) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaStreamSynchronize(b->stream));  // in-flight steps read the descriptors
+    for (int p = 0; p < 2; ++p) {
+        b->h_insts[p][index].alpha = alpha;
+        b->h_insts[p][index].alpha_fixed = 1;
+        MHD_TRY(cudaMemcpy(b->d_insts[p] + index, &b->h_insts[p][index], sizeof(BatchInst),
+                           cudaMemcpyHostToDevice));
+    }
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_step(mhd_batch* b, const double* dts) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if (!all_states_set(b)) return MHD_ERR_NO_STATE;
+    if (dts) {
+        for (int i = 0; i < b->count; ++i)
+            if (!std::isfinite(dts[i])) return MHD_ERR_INVALID_ARGUMENT;
+        // pageable source: the call returns once the values are staged, so dts may be reused
+        MHD_TRY(cudaMemcpyAsync(b->dt_dev, dts, b->count * sizeof(double), cudaMemcpyHostToDevice,
+                                b->stream));
+    }
+    return enqueue_step(b, dts ? b->dt_dev : nullptr, 0.0, 1, 0.0, false, nullptr);
+}
+
+mhd_status mhd_batch_run(mhd_batch* b, int nsteps, double dt_fixed, double t_end, double* dts_out,
+                         long long* prods_out) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if (!all_states_set(b)) return MHD_ERR_NO_STATE;
+    if (nsteps < 0 || !std::isfinite(dt_fixed) || !std::isfinite(t_end)) return MHD_ERR_INVALID_ARGUMENT;
+    if (nsteps == 0) return MHD_OK;
+    if (nsteps > b->rec_cap) {
+        MHD_TRY(cudaStreamSynchronize(b->stream));
+        cudaFree(b->rec_dts);
+        cudaFree(b->rec_prods);
+        b->rec_dts = nullptr;
+        b->rec_prods = nullptr;
+        b->rec_cap = 0;
+        MHD_TRY(cudaMalloc(&b->rec_dts, (size_t)b->count * nsteps * sizeof(double)));
+        MHD_TRY(cudaMalloc(&b->rec_prods, (size_t)b->count * nsteps * 2 * sizeof(long long)));
+        b->rec_cap = nsteps;
+    }
+    k_batch_driver_reset<<<(b->count + 127) / 128, 128, 0, b->stream>>>(b->d_insts[b->parity],
+                                                                         b->count);
+    MHD_TRY(cudaGetLastError());
+    auto one_step = [&]() { return enqueue_step(b, nullptr, dt_fixed, 2, t_end, true, nullptr); };
+    // Two consecutive steps (even and odd descriptors) form one CUDA graph, replayed nsteps/2 times.
+    int done = 0;
+    if (nsteps >= 4 && mhd_host::env_int("MHD_B200_NO_GRAPH", 0) == 0) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const int parity0 = b->parity;
+        bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            const mhd_status r1 = one_step();
+            const mhd_status r2 = (r1 == MHD_OK) ? one_step() : r1;
+            ok = cudaStreamEndCapture(b->stream, &graph) == cudaSuccess && r1 == MHD_OK && r2 == MHD_OK;
+            b->parity = parity0;  // the captured steps did not run
+        }
+        if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (ok) {
+            for (; done + 2 <= nsteps; done += 2) {
+                if (cudaGraphLaunch(exec, b->stream) != cudaSuccess) {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (!ok && done > 0) return MHD_ERR_CUDA;
+    }
+    for (; done < nsteps; ++done) {
+        s = one_step();
+        if (s != MHD_OK) return s;
+    }
+    if (dts_out)
+        MHD_TRY(cudaMemcpy2DAsync(dts_out, (size_t)nsteps * sizeof(double), b->rec_dts,
+                                  (size_t)b->rec_cap * sizeof(double), (size_t)nsteps * sizeof(double),
+                                  b->count, cudaMemcpyDeviceToHost, b->stream));
+    if (prods_out)
+        MHD_TRY(cudaMemcpy2DAsync(prods_out, (size_t)nsteps * 2 * sizeof(long long), b->rec_prods,
+                                  (size_t)b->rec_cap * 2 * sizeof(long long),
+                                  (size_t)nsteps * 2 * sizeof(long long), b->count,
+                                  cudaMemcpyDeviceToHost, b->stream));
+    if (dts_out || prods_out) MHD_TRY(cudaStreamSynchronize(b->stream));
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_set_tuning(mhd_batch* b, const mhd_batch_tuning* t) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if (!t) return MHD_ERR_INVALID_ARGUMENT;
+    return apply_tuning(b, *t);
+}
+
+mhd_status mhd_batch_get_tuning(mhd_batch* b, mhd_batch_tuning* t) {
+    if (!b || !t) return MHD_ERR_INVALID_ARGUMENT;
+    *t = b->tuning;
+    return MHD_OK;
+}
+
+// Autotuner: one CFL step of the current states per candidate, timed per kernel with events;
+// the explicit-stage row height and the solver's (row height, dealing order) are chosen
+// independently (they set disjoint kernels' decompositions). States, device statuses, step
+// coefficients and the descriptor parity are restored after every trial.
+mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if (!all_states_set(b)) return MHD_ERR_NO_STATE;
+    MHD_TRY(cudaStreamSynchronize(b->stream));
+    const mhd_batch_tuning before = b->tuning;
+    double* backup = nullptr;
+    StepCoeffs* coeffs_bk = nullptr;
+    DeviceStatus* status_bk = nullptr;
+    cudaEvent_t ev[6] = {};
+    struct Cleanup {
+        double*& backup;
+        StepCoeffs*& c;
+        DeviceStatus*& st;
+        cudaEvent_t* ev;
+        ~Cleanup() {
+            cudaFree(backup);
+            cudaFree(c);
+            cudaFree(st);
+            for (int k = 0; k < 6; ++k)
+                if (ev[k]) cudaEventDestroy(ev[k]);
+        }
+    } cleanup{backup, coeffs_bk, status_bk, ev};
+    MHD_TRY(cudaMalloc(&backup, 6 * b->total_cells * sizeof(double)));
+    MHD_TRY(cudaMalloc(&coeffs_bk, b->count * sizeof(StepCoeffs)));
+    MHD_TRY(cudaMalloc(&status_bk, b->count * sizeof(DeviceStatus)));
+    for (int k = 0; k < 6; ++k) MHD_TRY(cudaEventCreate(&ev[k]));
+    const int parity0 = b->parity;
+    auto planes_copy = [&](bool save) -> mhd_status {
+        size_t off = 0;
+        for (int i = 0; i < b->count; ++i) {
+            const BatchInst& I = b->h_insts[parity0][i];
+            for (int k = 0; k < 6; ++k) {
+                double* bk = backup + off + (size_t)k * b->ncell[i];
+                MHD_TRY(cudaMemcpyAsync(save ? bk : I.S[k], save ? I.S[k] : bk,
+                                        b->ncell[i] * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        b->stream));
+            }
+            off += 6 * b->ncell[i];
+        }
+        MHD_TRY(cudaMemcpyAsync(save ? coeffs_bk : b->coeffs, save ? b->coeffs : coeffs_bk,
+                                b->count * sizeof(StepCoeffs), cudaMemcpyDeviceToDevice, b->stream));
+        MHD_TRY(cudaMemcpyAsync(save ? status_bk : b->status, save ? b->status : status_bk,
+                                b->count * sizeof(DeviceStatus), cudaMemcpyDeviceToDevice, b->stream));
+        b->parity = parity0;
+        return MHD_OK;
+    };
+    if ((s = planes_copy(true)) != MHD_OK) return s;
+    constexpr int nst = sizeof(kStageRowsCand) / sizeof(int);
+    constexpr int ncg = sizeof(kCgRowsCand) / sizeof(int);
+    double best_stage = 1e300, best_cg = 1e300;
+    int best_stage_rows = before.stage_rows, best_cg_rows = before.cg_rows, best_order = before.cg_order;
+    // trial -1 warms the kernels up; trials 0 .. 2*ncg-1 cover every solver candidate and every
+    // stage candidate (twice, the better time counts)
+    for (int trial = -1; trial < 2 * ncg; ++trial) {
+        mhd_batch_tuning t{};
+        const int tk = std::max(trial, 0);
+        t.stage_rows = kStageRowsCand[tk % nst];
+        t.cg_rows = kCgRowsCand[tk % ncg];
+        t.cg_order = tk / ncg;
+        if ((s = apply_tuning(b, t)) != MHD_OK) return s;
+        if ((s = enqueue_step(b, nullptr, 0.0, 1, 0.0, false, ev)) != MHD_OK) return s;
+        MHD_TRY(cudaStreamSynchronize(b->stream));
+        float ms[5];
+        for (int k = 0; k < 5; ++k) MHD_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+        if ((s = planes_copy(false)) != MHD_OK) return s;
+        if (trial < 0) continue;
+        const double stage_ms = (double)ms[0] + ms[2] + ms[4];
+        const double cg_ms = (double)ms[1] + ms[3];
+        if (stage_ms < best_stage) {
+            best_stage = stage_ms;
+            best_stage_rows = t.stage_rows;
+        }
+        if (cg_ms < best_cg) {
+            best_cg = cg_ms;
+            best_cg_rows = t.cg_rows;
+            best_order = t.cg_order;
+        }
+    }
+    mhd_batch_tuning chosen{};
+    chosen.stage_rows = best_stage_rows;
+    chosen.cg_rows = best_cg_rows;
+    chosen.cg_order = best_order;
+    if ((s = apply_tuning(b, chosen)) != MHD_OK) return s;
+    b->tuning.stage_ms = best_stage;
+    b->tuning.cg_ms = best_cg;
+    MHD_TRY(cudaStreamSynchronize(b->stream));
+    if (out) *out = b->tuning;
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_synchronize(mhd_batch* b, mhd_status* per_instance) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if ((s = read_status(b)) != MHD_OK) return s;
+    mhd_status worst = MHD_OK;
+    bool any = false;
+    for (int i = 0; i < b->count; ++i) {
+        const mhd_status si = status_of(b->host_status[i].flags);
+        if (per_instance) per_instance[i] = si;
+        if (severity(si) > severity(worst)) worst = si;
+        any |= b->host_status[i].flags != 0;
+    }
+    if (any) {
+        for (int i = 0; i < b->count; ++i)
+            if (b->host_status[i].flags)
+                MHD_TRY(cudaMemsetAsync(&b->status[i].flags, 0, sizeof(unsigned int), b->stream));
+        MHD_TRY(cudaStreamSynchronize(b->stream));
+    }
+    return worst;
+}
+
+mhd_status mhd_batch_last_cg_products(mhd_batch* b, long long* out) {
+    mhd_status s = check_batch(b);
+    if (s != MHD_OK) return s;
+    if (!out) return MHD_ERR_INVALID_ARGUMENT;
+    if ((s = read_status(b)) != MHD_OK) return s;
+    for (int i = 0; i < b->count; ++i) {
+        out[2 * i] = b->host_status[i].cg_products[0];
+        out[2 * i + 1] = b->host_status[i].cg_products[1];
+    }
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_cfl_dt(mhd_batch* b, int index, double* dt) {
+    mhd_status s = check_index(b, index);
+    if (s != MHD_OK) return s;
+    if (!dt) return MHD_ERR_INVALID_ARGUMENT;
+    if (!b->have_state[index]) return MHD_ERR_NO_STATE;
+    MHD_TRY(cudaMemcpyAsync(b->host_small, &b->status[index].smax_bits, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, b->stream));
+    MHD_TRY(cudaStreamSynchronize(b->stream));
+    double smaxv;
+    memcpy(&smaxv, b->host_small, sizeof(double));
+    const mhd_params& p = b->prm[index];
+    const double h = std::min(p.dx, p.dy);  // diagnostics.hpp:52-86
+    double dt_res = INFINITY;
+    if (p.eta != 0.0) dt_res = h * h / (4.0 * p.eta);
+    if (!(smaxv > 1e-8)) smaxv = std::max(smaxv, 1e-8);
+    *dt = std::min(p.courant * h / smaxv, dt_res) * p.safety;
+    return MHD_OK;
+}
+
+mhd_status mhd_batch_divb(mhd_batch* b, int index, double* rms, double* maxabs) {
+    mhd_status s = check_index(b, index);
+    if (s != MHD_OK) return s;
+    if (!b->have_state[index]) return MHD_ERR_NO_STATE;
+    const BatchInst& I = b->h_insts[b->parity][index];
+    const int blocks = std::max(1, std::min((int)((b->ncell[index] + 255) / 256), b->divb_blocks));
+    k_divb_partial<<<blocks, 256, 0, b->stream>>>(I.D, I.S[4], I.S[5], b->divb_partial);
+    MHD_TRY(cudaGetLastError());
+    k_divb_final<<<1, 32, 0, b->stream>>>(b->divb_partial, blocks, (long long)b->ncell[index],
+                                          b->divb_out);
+    MHD_TRY(cudaGetLastError());
+    MHD_TRY(cudaMemcpyAsync(b->host_small, b->divb_out, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                            b->stream));
+    MHD_TRY(cudaStreamSynchronize(b->stream));
+    if (rms) *rms = b->host_small[0];
+    if (maxabs) *maxabs = b->host_small[1];
+    return MHD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,398 @@
+// Batched IMEX step: many independent periodic simulations of uneven sizes advanced together,
+// one persistent fused launch per stage of the step (coefficients, stage 1, implicit solve,
+// stage 2, implicit solve, finalize). Every instance keeps its own dt (CFL or fixed), its own
+// matrix coefficient and its own convergence, exactly as if it were stepped alone
+// (integrator_main.cpp:76-112 per instance).
+//
+// Work is described by flat lists of warp work items (instance, item), where item indexes the
+// instance's strip/segment decomposition: 28-column strips for the explicit stages and the
+// finalize (SweepGeom), 30-column strips for the solver. The explicit kernels are persistent and
+// pull items from a global counter (largest items first). The solver kernel deals its items to
+// warps in a fixed order, because its sums must be reduced in a fixed order.
+//
+// The descriptor array exists twice, for even and odd steps: the finalize leaves U^{n+1}'s hydro
+// planes in the accumulator, so the state and accumulator hydro pointers trade places every step.
+#pragma once
+
+#include "mhd_cg_sweep.cuh"
+#include "mhd_finalize_sweep.cuh"
+#include "mhd_sweep.cuh"
+
+namespace mhd {
+
+struct BatchInst {
+    Domain D;
+    StepCoeffs* C;
+    DeviceStatus* st;
+    double* S[6];
+    double* T[6];
+    double* A[6];
+    double* x;
+    double* r[2];
+    double* p[2];
+    SweepGeom sg;  // explicit stages and finalize (SW_OUT == FS_OUT columns per strip)
+    int cg_strips_x, cg_seg_h;
+    long long max_iters;
+    double tol;
+    double alpha;  // fixed matrix coefficient when alpha_fixed
+    int alpha_fixed;
+    int pad;
+    double hmin, courant, safety;
+};
+
+struct WorkItem {
+    int inst;
+    int w;
+};
+
+static_assert(SW_OUT == FS_OUT, "stages and finalize share one work-item list");
+
+// Step coefficients of every instance (one thread each), then the per-step resets: the max
+// signal speed (recomputed by the finalize), the explicit kernels' work counters and the
+// solver's barrier counters.
+static __global__ void k_batch_coeffs(const BatchInst* __restrict__ insts, int n,
+                                      const double* __restrict__ dt_in, double dt_fixed,
+                                      int run_mode, double t_end, double g, double d,
+                                      double* dts_rec, int rec_stride, int* queues, int nqueues,
+                                      CgSync* syncs, int nsync) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nqueues) queues[i] = 0;
+    if (i < nsync) {
+        syncs[i].count = 0ULL;
+        syncs[i].error = 0u;
+    }
+    if (i >= n) return;
+    const BatchInst& I = insts[i];
+    const double dt = dt_in ? dt_in[i] : dt_fixed;
+    const int mode = I.alpha_fixed ? 0 : run_mode;
+    step_coeffs_one(I.C, I.st, dt, I.alpha, mode, I.D.eta, I.hmin, I.courant, I.safety, g, d,
+                    t_end, dts_rec ? dts_rec + (size_t)i * rec_stride : nullptr);
+    I.st->smax_bits = 0ULL;
+}
+
+static __global__ void k_batch_driver_reset(const BatchInst* __restrict__ insts, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    StepCoeffs* C = insts[i].C;
+    C->t = 0.0;
+    C->prev_dt = 0.0;
+    C->step = 0;
+    C->cur = 0;
+    C->first = 1;
+}
+
+// Next work item of the warp from a global counter (lane 0 takes it, all lanes get it).
+__device__ __forceinline__ int batch_next_item(int* queue) {
+    int it = 0;
+    if ((threadIdx.x & 31) == 0) it = atomicAdd(queue, 1);
+    return __shfl_sync(0xffffffffu, it, 0);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
+k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ items, int nitems,
+              int* queue) {
+    for (;;) {
+        const int it = batch_next_item(queue);
+        if (it >= nitems) break;
+        const WorkItem e = items[it];
+        const BatchInst& I = insts[e.inst];
+        CPlanes in;
+        Planes oa, ob;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            in.f[q] = (MODE == 1) ? I.S[q] : I.T[q];
+            oa.f[q] = I.T[q];
+            ob.f[q] = I.A[q];
+        }
+        const Domain D = I.D;
+        const SweepGeom G = I.sg;
+        stage_sweep_warp<MODE>(D, I.C, in, (MODE == 1) ? nullptr : I.x, oa, ob, G, e.w);
+    }
+}
+
+static __global__ void __launch_bounds__(32 * FS_WARPS)
+k_finalize_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ items, int nitems,
+                 int* queue) {
+    for (;;) {
+        const int it = batch_next_item(queue);
+        if (it >= nitems) break;
+        const WorkItem e = items[it];
+        const BatchInst& I = insts[e.inst];
+        Planes acc;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc.f[q] = I.A[q];
+        const Domain D = I.D;
+        const SweepGeom G = I.sg;
+        finalize_sweep_warp(D, I.C, acc, I.x, I.S[4], I.S[5], I.st, G, e.w);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched implicit solve: the CGs of up to CGB_MAX_INST instances in one persistent cooperative
+// kernel, running their phases in lockstep (solvers.hpp:404-489 per instance, Eigen's
+// ConjugateGradient defaults as in k_cg_sweep).
+//
+// The items of all instances (instance-major) are dealt to the grid's warps in a fixed
+// round-robin order, so each instance is spread over all SMs and stays spread while the others
+// converge. In a phase every warp sums its partials per instance (item order), each block sums
+// its warps per instance (warp order) and publishes one partial per (instance, block); after the
+// grid barrier every block reduces each instance's block partials in the same fixed order, so all
+// blocks hold identical scalars and take identical decisions. Instances that converged (or whose
+// right-hand side vanished) skip their items; the loop ends when no instance is active.
+
+constexpr int CGB_MAX_INST = 64;
+
+enum CgInstStatus : int { kCgActive = 0, kCgConverged = 1, kCgZero = 2, kCgBreakdown = 3, kCgCapped = 4 };
+
+struct CgBInst {
+    double cx, cy, diag, invdiag;  // matrix of this solve
+    double alpha, beta;            // CG step scalars
+    double bb, absNew, thr, rr;
+    long long products;
+    int status;
+    int pad;
+};
+
+struct CgBatchArgs {
+    const BatchInst* insts;  // descriptors of this step's parity
+    int inst0, ninst;        // instances [inst0, inst0 + ninst) of this launch
+    const WorkItem* items;   // their solver items, instance-major
+    int nitems;
+    double* partials;        // [2][CGB_MAX_INST][gridDim.x][4]
+    CgSync* sync;
+    int solve_index;         // 0: B* = U1*_B (T planes), 1: B* = U2*_B (A planes)
+    int rec_stride;
+    long long* prods_rec;    // [instance][rec_stride][2] products record, or null
+    double timeout_s;
+};
+
+__device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const BatchInst& I) {
+    CgSweepArgs g{};
+    g.D = I.D;
+    g.C = I.C;
+    g.bxf = (a.solve_index == 0) ? I.T[4] : I.A[4];
+    g.byf = (a.solve_index == 0) ? I.T[5] : I.A[5];
+    g.x = I.x;
+    g.r[0] = I.r[0];
+    g.r[1] = I.r[1];
+    g.p[0] = I.p[0];
+    g.p[1] = I.p[1];
+    g.strips_x = I.cg_strips_x;
+    g.seg_h = I.cg_seg_h;
+    return g;
+}
+
+// One sweep phase over this warp's items. PH as in cg_sweep_segment; NV sums per instance.
+// Ends with the block's partials of every instance published in part_out.
+template <int PH, int NV>
+__device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh,
+                                          double (*wsum)[CGB_MAX_INST][3], double* ring, int k,
+                                          int dir, double* part_out) {
+    constexpr int NW = CGS_NT / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int li = lane; li < a.ninst; li += 32)
+#pragma unroll
+        for (int c = 0; c < NV; ++c) wsum[wid][li][c] = 0.0;
+    __syncwarp();
+    const bool odd = (k & 1) != 0;
+    for (int it = blockIdx.x * NW + wid; it < a.nitems; it += gridDim.x * NW) {
+        const WorkItem e = a.items[it];
+        const int li = e.inst - a.inst0;
+        if (PH != 0 && sh[li].status != kCgActive) continue;
+        const BatchInst& I = a.insts[e.inst];
+        const CgSweepArgs g = cgb_args(a, I);
+        CgScal s;
+        s.cx = sh[li].cx;
+        s.cy = sh[li].cy;
+        s.diag = sh[li].diag;
+        s.invdiag = sh[li].invdiag;
+        s.alpha = sh[li].alpha;
+        s.beta = sh[li].beta;
+        double acc[3] = {0.0, 0.0, 0.0};
+        if constexpr (PH == 0) {
+            cg_sweep_segment<0>(g, s, e.w, dir, nullptr, nullptr, g.r[0], nullptr, ring, acc);
+        } else {
+            const double* rk = odd ? g.r[1] : g.r[0];
+            double* rk1 = odd ? g.r[0] : g.r[1];
+            const double* pkm1 = odd ? g.p[0] : g.p[1];
+            double* pk = odd ? g.p[1] : g.p[0];
+            cg_sweep_segment<PH>(g, s, e.w, dir, rk, pkm1, rk1, pk, ring, acc);
+        }
+#pragma unroll
+        for (int c = 0; c < NV; ++c)
+            for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) wsum[wid][li][c] += acc[c];
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < a.ninst * NV; q += CGS_NT) {
+        const int li = q / NV, c = q - li * NV;
+        double v = 0.0;
+        for (int w2 = 0; w2 < NW; ++w2) v += wsum[w2][li][c];
+        part_out[((size_t)li * gridDim.x + blockIdx.x) * 4 + c] = v;
+    }
+}
+
+// Sum of instance li's block partials (all blocks, fixed order); identical in every lane.
+template <int NV>
+__device__ __forceinline__ void cgb_span_sum(const double* part, int li, double (&v)[NV]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) v[c] = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+        const double* p = part + ((size_t)li * gridDim.x + b) * 4;
+#pragma unroll
+        for (int c = 0; c < NV; ++c) v[c] += __ldcg(&p[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < NV; ++c)
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+}
+
+static __global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
+k_cg_batch(CgBatchArgs a) {
+    constexpr int NW = CGS_NT / 32;
+    __shared__ CgBInst sh[CGB_MAX_INST];
+    __shared__ double wsum[NW][CGB_MAX_INST][3];
+    __shared__ int sflag;
+#if defined(__CUDA_ARCH__)
+    extern __shared__ __align__(16) double cg_ring_mem[];
+#else
+    static double cg_ring_mem[(CGS_NT / 32) * CG_RING * CG_SLOT];
+#endif
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double* const ring = cg_ring_mem + (size_t)wid * CG_RING * CG_SLOT;
+    unsigned long long target = 0;
+    const unsigned long long deadline = global_timer_ns() + (unsigned long long)(a.timeout_s * 1e9);
+    double* const part0 = a.partials;
+    double* const part1 = a.partials + (size_t)CGB_MAX_INST * gridDim.x * 4;
+    auto part = [&](int ph) { return (ph & 1) ? part1 : part0; };
+    int phase = 0;
+    int dir = 1;
+    auto barrier_or_quit = [&]() -> bool {
+        if (grid_barrier(a.sync, target, deadline, &sflag)) return true;
+        if (tid == 0 && blockIdx.x == 0)
+            for (int li = 0; li < a.ninst; ++li)
+                atomicOr(&a.insts[a.inst0 + li].st->flags, (unsigned)kStatusTimeout);
+        return false;
+    };
+
+    // matrix of each instance's solve (the coefficient was set by this step's coefficients)
+    for (int li = tid; li < a.ninst; li += CGS_NT) {
+        const BatchInst& I = a.insts[a.inst0 + li];
+        const double am = I.C->alpha;
+        CgBInst& S = sh[li];
+        S.cx = am / (I.D.dx * I.D.dx);
+        S.cy = am / (I.D.dy * I.D.dy);
+        S.diag = 1 + 2 * (S.cx + S.cy);
+        S.invdiag = (S.diag == 0.0) ? 1.0 : 1.0 / S.diag;
+        S.alpha = 0.0;
+        S.beta = 0.0;
+        S.products = 0;
+        S.rr = 0.0;
+        S.status = kCgActive;
+    }
+    __syncthreads();
+
+    // ---- phase A0: r0 = b, p0 = b/d, |b|^2, r.z, p.Ap
+    cgb_phase<0, 3>(a, sh, wsum, ring, 0, dir, part(phase));
+    if (!barrier_or_quit()) return;
+    for (int li = wid; li < a.ninst; li += NW) {
+        double v[3];
+        cgb_span_sum<3>(part(phase), li, v);
+        if (lane == 0) {
+            CgBInst& S = sh[li];
+            const BatchInst& I = a.insts[a.inst0 + li];
+            S.bb = v[0];
+            S.absNew = v[1];
+            S.thr = smax(I.tol * I.tol * S.bb, 2.2250738585072014e-308);
+            if (!isfinite(S.bb)) S.status = kCgBreakdown;
+            else if (S.bb == 0.0 || S.bb < S.thr) S.status = kCgZero;
+            else if (I.max_iters <= 0) S.status = kCgCapped;
+            S.alpha = (S.status == kCgActive) ? S.absNew / v[2] : 0.0;
+        }
+    }
+    ++phase;
+    dir = -dir;
+    __syncthreads();
+
+    for (int k = 0;; ++k) {
+        if (k > 0) {
+            // ---- phase A_k: p_k, q = A p_k, p.q
+            cgb_phase<1, 1>(a, sh, wsum, ring, k, dir, part(phase));
+            if (!barrier_or_quit()) return;
+            for (int li = wid; li < a.ninst; li += NW) {
+                if (sh[li].status != kCgActive) continue;
+                double v[1];
+                cgb_span_sum<1>(part(phase), li, v);
+                if (lane == 0) sh[li].alpha = sh[li].absNew / v[0];
+            }
+            ++phase;
+            dir = -dir;
+            __syncthreads();
+        }
+        // ---- phase B_k: x, r_{k+1}, p_k; r.r, r.z
+        if (k == 0) cgb_phase<2, 2>(a, sh, wsum, ring, k, dir, part(phase));
+        else cgb_phase<3, 2>(a, sh, wsum, ring, k, dir, part(phase));
+        if (!barrier_or_quit()) return;
+        int active = 0;
+        for (int li = wid; li < a.ninst; li += NW) {
+            if (sh[li].status != kCgActive) continue;
+            double v[2];
+            cgb_span_sum<2>(part(phase), li, v);
+            if (lane == 0) {
+                CgBInst& S = sh[li];
+                S.products += 1;
+                S.rr = v[0];
+                if (!isfinite(v[0]) || !isfinite(S.alpha)) S.status = kCgBreakdown;
+                else if (v[0] < S.thr) S.status = kCgConverged;
+                else if (S.products >= a.insts[a.inst0 + li].max_iters) S.status = kCgCapped;
+                else {
+                    const double absOld = S.absNew;
+                    S.absNew = v[1];
+                    S.beta = S.absNew / absOld;
+                    active = 1;
+                }
+            }
+        }
+        ++phase;
+        dir = -dir;
+        if (!__syncthreads_or(active)) break;
+    }
+
+    // x = 0 for a vanished right-hand side (Eigen returns the zero vector) and on breakdown
+    for (int it = blockIdx.x * NW + wid; it < a.nitems; it += gridDim.x * NW) {
+        const WorkItem e = a.items[it];
+        const int s0 = sh[e.inst - a.inst0].status;
+        if (s0 != kCgZero && s0 != kCgBreakdown) continue;
+        const BatchInst& I = a.insts[e.inst];
+        const int nx = I.D.nx, ny = I.D.ny;
+        const int sx = e.w % I.cg_strips_x, sy = e.w / I.cg_strips_x;
+        const int i = sx * CG_W - 1 + lane;
+        const int r0 = sy * I.cg_seg_h, r1 = min(r0 + I.cg_seg_h, ny);
+        if (lane >= 1 && lane <= CG_W && i < nx)
+            for (int j = r0; j < r1; ++j) I.x[(size_t)j * nx + i] = 0.0;
+    }
+    if (blockIdx.x == 0) {
+        for (int li = tid; li < a.ninst; li += CGS_NT) {
+            const BatchInst& I = a.insts[a.inst0 + li];
+            const CgBInst& S = sh[li];
+            I.st->cg_products[a.solve_index] = S.products;
+            I.st->cg_products_total += S.products;
+            I.st->cg_last_rr[a.solve_index] = (S.bb > 0.0) ? S.rr / S.bb : 0.0;
+            if (a.prods_rec)
+                a.prods_rec[((size_t)(a.inst0 + li) * a.rec_stride + I.C->cur) * 2 + a.solve_index] =
+                    S.products;
+            if (S.status == kCgBreakdown)
+                atomicOr(&I.st->flags, (unsigned)(kStatusCgBreakdown | kStatusNonFinite));
+            else if (S.status == kCgCapped)
+                atomicOr(&I.st->flags, (unsigned)kStatusCgNotConverged);
+        }
+    }
+}
+
+}  // namespace mhd

@@ -20,6 +20,7 @@
 
 #include "../../include/mhd_b200.h"
 #include "mhd_cg_sweep.cuh"
+#include "mhd_host_util.h"
 #include "mhd_kernels.cuh"
 #include "mhd_finalize_sweep.cuh"
 #include "mhd_sweep.cuh"
@@ -81,29 +82,8 @@ struct mhd_context {
 
 namespace {
 
-mhd_status cuda_status(cudaError_t e) {
-    if (e == cudaSuccess) return MHD_OK;
-    if (e == cudaErrorMemoryAllocation) return MHD_ERR_OUT_OF_MEMORY;
-    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ||
-        e == cudaErrorNoKernelImageForDevice)
-        return MHD_ERR_NO_DEVICE;
-    return MHD_ERR_CUDA;
-}
-
-#define MHD_TRY(expr)                                   \
-    do {                                                \
-        cudaError_t _e = (expr);                        \
-        if (_e != cudaSuccess) {                        \
-            if (getenv("MHD_B200_VERBOSE"))             \
-                fprintf(stderr, "mhd_b200: %s: %s\n", #expr, cudaGetErrorString(_e)); \
-            return cuda_status(_e);                     \
-        }                                               \
-    } while (0)
-
-int env_int(const char* name, int def) {
-    const char* v = getenv(name);
-    return v ? atoi(v) : def;
-}
+using mhd_host::cuda_status;
+using mhd_host::env_int;
 
 // Request for k_step_coeffs, mirroring the decisions of the reference driver.
 mhd_status launch_coeffs(mhd_context* c, double dt, int alpha_mode, double t_end, double* dts_out) {

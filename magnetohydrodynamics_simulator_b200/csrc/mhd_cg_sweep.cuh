@@ -246,7 +246,7 @@ __device__ __forceinline__ void publish(double (&acc)[3], double* slot, double* 
     }
 }
 
-__global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
+static __global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
 k_cg_sweep(CgSweepArgs a) {
     __shared__ double red[CGS_NT / 32 * 4];
     __shared__ double scal[8];

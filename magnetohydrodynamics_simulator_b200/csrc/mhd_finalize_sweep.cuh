@@ -18,13 +18,13 @@ constexpr int FS_OUT = 28;
 constexpr int FS_WARPS = 8;
 constexpr int FS_PRE = 3;  // rows swept before the first output row
 
-__global__ void __launch_bounds__(32 * FS_WARPS)
-k_finalize_sweep(Domain D, const StepCoeffs* __restrict__ C, Planes acc,
-                 const double* __restrict__ xsolve, double* __restrict__ bx_out,
-                 double* __restrict__ by_out, DeviceStatus* st, SweepGeom G) {
+// The sweep of one warp over work item w of one grid.
+__device__ __forceinline__ void finalize_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
+                                                    const Planes& acc, const double* __restrict__ xsolve,
+                                                    double* __restrict__ bx_out,
+                                                    double* __restrict__ by_out, DeviceStatus* st,
+                                                    const SweepGeom& G, int w) {
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * FS_WARPS + (threadIdx.x >> 5);
-    if (w >= G.nwarps) return;
     const int nx = D.nx, ny = D.ny;
     const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int c0 = sx * FS_OUT;
@@ -110,6 +110,15 @@ k_finalize_sweep(Domain D, const StepCoeffs* __restrict__ C, Planes acc,
         atomicMax(&st->smax_bits, (unsigned long long)__double_as_longlong(vmax));
         if (any_bad) atomicOr(&st->flags, (unsigned)kStatusNonFinite);
     }
+}
+
+static __global__ void __launch_bounds__(32 * FS_WARPS)
+k_finalize_sweep(Domain D, const StepCoeffs* __restrict__ C, Planes acc,
+                 const double* __restrict__ xsolve, double* __restrict__ bx_out,
+                 double* __restrict__ by_out, DeviceStatus* st, SweepGeom G) {
+    const int w = blockIdx.x * FS_WARPS + (threadIdx.x >> 5);
+    if (w >= G.nwarps) return;
+    finalize_sweep_warp(D, C, acc, xsolve, bx_out, by_out, st, G, w);
 }
 
 }  // namespace mhd

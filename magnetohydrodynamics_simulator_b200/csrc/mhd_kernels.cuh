@@ -214,7 +214,7 @@ __device__ __forceinline__ void reduce_partials(const double* part, int nblocks,
 // eta > 0 and dt moved by more than 1e-10 relative to the previous step (integrator_main.cpp:55-60,
 // 87-95). t_end > 0 clips dt so the time does not pass it (integrator_main.cpp:83).
 
-__global__ void k_driver_reset(StepCoeffs* C) {
+static __global__ void k_driver_reset(StepCoeffs* C) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     C->t = 0.0;
     C->prev_dt = 0.0;
@@ -223,10 +223,10 @@ __global__ void k_driver_reset(StepCoeffs* C) {
     C->first = 1;
 }
 
-__global__ void k_step_coeffs(StepCoeffs* C, const DeviceStatus* st, double dt, double alpha,
-                              int alpha_mode, double eta, double hmin, double courant,
-                              double safety, double g, double d, double t_end, double* dts_out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void step_coeffs_one(StepCoeffs* C, const DeviceStatus* st, double dt,
+                                                double alpha, int alpha_mode, double eta,
+                                                double hmin, double courant, double safety,
+                                                double g, double d, double t_end, double* dts_out) {
     if (dt <= 0.0) {
         const double smaxv = smax(__longlong_as_double((long long)st->smax_bits), 1e-8);
         double dt_res = __longlong_as_double(0x7ff0000000000000LL);  // +inf
@@ -258,6 +258,13 @@ __global__ void k_step_coeffs(StepCoeffs* C, const DeviceStatus* st, double dt, 
     C->t += dt;
 }
 
+static __global__ void k_step_coeffs(StepCoeffs* C, const DeviceStatus* st, double dt, double alpha,
+                              int alpha_mode, double eta, double hmin, double courant,
+                              double safety, double g, double d, double t_end, double* dts_out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    step_coeffs_one(C, st, dt, alpha, alpha_mode, eta, hmin, courant, safety, g, d, t_end, dts_out);
+}
+
 // ------------------------------------------------------------------------------------------
 // Finalize: B2 = U2*_B + dt*g*rate(E2); g3 = explicit resistive rate of B2;
 // B^{n+1} = U2*_B + dt*g*g3 (solvers.hpp:571-608); density floor of the new state in place
@@ -279,7 +286,7 @@ struct FinalSmem {
     double red[32];
 };
 
-__global__ void __launch_bounds__(FN_NT)
+static __global__ void __launch_bounds__(FN_NT)
 k_finalize(Domain D, const StepCoeffs* __restrict__ C, Planes acc, const double* __restrict__ xsolve,
            double* __restrict__ bx_out, double* __restrict__ by_out, DeviceStatus* st, int tiles_x) {
     __shared__ FinalSmem s;
@@ -367,7 +374,7 @@ k_finalize(Domain D, const StepCoeffs* __restrict__ C, Planes acc, const double*
 // ------------------------------------------------------------------------------------------
 // CFL speed of a state that did not come out of a step (diagnostics.hpp:44-88 scan only).
 
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_cfl_scan(Domain D, CPlanes u, DeviceStatus* st) {
     __shared__ double red[32];
     const int nx = D.nx, ny = D.ny;
@@ -390,7 +397,7 @@ k_cfl_scan(Domain D, CPlanes u, DeviceStatus* st) {
 // Diagnostics
 
 // diagnostics.hpp:15-42: per-block sum of div^2 and max |div| over physical cells.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_divb_partial(Domain D, const double* __restrict__ bxf, const double* __restrict__ byf,
                double* partial) {
     __shared__ double red[64];
@@ -415,7 +422,7 @@ k_divb_partial(Domain D, const double* __restrict__ bxf, const double* __restric
     }
 }
 
-__global__ void k_divb_final(const double* partial, int nblocks, long long ncells, double* out) {
+static __global__ void k_divb_final(const double* partial, int nblocks, long long ncells, double* out) {
     if (threadIdx.x != 0) return;
     double s2 = 0.0, mx = 0.0;
     for (int b = 0; b < nblocks; ++b) {
@@ -427,7 +434,7 @@ __global__ void k_divb_final(const double* partial, int nblocks, long long ncell
 }
 
 // Primitives of the current state (Grid::computeCellB + computePrimitives), dense layout.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_primitives(Domain D, CPlanes u, double* rho_f, double* vx, double* vy, double* p, double* bxc,
              double* byc) {
     const int nx = D.nx, ny = D.ny;
@@ -451,7 +458,7 @@ k_primitives(Domain D, CPlanes u, double* rho_f, double* vx, double* vy, double*
 // Rate of the face field from a corner field E (solvers.hpp:472-488): bx' = -(E(i,j+1) - E(i,j))/dy,
 // by' = (E(i+1,j) - E(i,j))/dx. With E == nullptr the corner field is eta*J_z(bxf, byf) itself
 // (the explicit resistive term, solvers.hpp:450-463 and :470).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_corner_rates(Domain D, const double* __restrict__ E, const double* __restrict__ bxf,
                const double* __restrict__ byf, double* __restrict__ bx_rate,
                double* __restrict__ by_rate) {
@@ -473,12 +480,12 @@ k_corner_rates(Domain D, const double* __restrict__ E, const double* __restrict_
     }
 }
 
-__global__ void k_set_alpha(StepCoeffs* C, double alpha) {
+static __global__ void k_set_alpha(StepCoeffs* C, double alpha) {
     if (threadIdx.x == 0 && blockIdx.x == 0) C->alpha = alpha;
 }
 
 // Dense periodic plane -> padded plane with ng periodic ghost layers (Grid.hpp:143-161).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_pad_plane(const double* __restrict__ src, double* __restrict__ dst, int nx, int ny, int ng) {
     const int W = nx + 2 * ng;
     const size_t n = (size_t)W * (ny + 2 * ng);

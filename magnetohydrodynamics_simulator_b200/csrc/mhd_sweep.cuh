@@ -40,13 +40,13 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 #define MHD_SWEEP_MIN_BLOCKS_2 2
 #endif
 
+// The sweep of one warp over work item w (strip w % strips_x, segment w / strips_x) of one grid.
 template <int MODE>
-__global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
-k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
-              const double* __restrict__ xsolve, Planes outA, Planes outB, SweepGeom G) {
+__device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
+                                                 const CPlanes& in, const double* __restrict__ xsolve,
+                                                 const Planes& outA, const Planes& outB,
+                                                 const SweepGeom& G, int w) {
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
-    if (w >= G.nwarps) return;
     const int nx = D.nx, ny = D.ny;
     const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int c0 = sx * SW_OUT;
@@ -304,6 +304,15 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
             accB[1] = nB[1];
         }
     }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
+k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
+              const double* __restrict__ xsolve, Planes outA, Planes outB, SweepGeom G) {
+    const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
+    if (w >= G.nwarps) return;
+    stage_sweep_warp<MODE>(D, C, in, xsolve, outA, outB, G, w);
 }
 
 }  // namespace mhd

@@ -76,3 +76,33 @@ def test_invalid_parameters_rejected(lib):
     assert lib.mhd_create(ctypes.byref(p), None, ctypes.byref(h)) == 1  # dx <= 0
     lib.mhd_default_params(ctypes.byref(p), 16, 16, 0.1, 0.1, -1.0)
     assert lib.mhd_create(ctypes.byref(p), None, ctypes.byref(h)) == 1  # eta < 0
+
+
+def test_batch_invalid_parameters_rejected(lib):
+    from magnetohydrodynamics_simulator_b200 import capi
+
+    lib = capi.load_library()
+    arr = (capi.Params * 3)()
+    for k in range(3):
+        lib.mhd_default_params(ctypes.byref(arr[k]), 16 + k, 16, 0.1, 0.1, 1e-3)
+    h = ctypes.c_void_p()
+    assert lib.mhd_batch_create(arr, 0, None, ctypes.byref(h)) == 1  # empty batch
+    arr[1].nx = 1
+    assert lib.mhd_batch_create(arr, 3, None, ctypes.byref(h)) == 1  # one bad instance
+    arr[1].nx = 17
+    arr[2].ct_mode = 5
+    assert lib.mhd_batch_create(arr, 3, None, ctypes.byref(h)) == 1
+    assert lib.mhd_batch_step(None, None) == 1
+    assert lib.mhd_batch_count(None) == 0
+
+
+def test_batch_without_device_is_reported_not_faked():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from magnetohydrodynamics_simulator_b200 import Batch, MHDError
+
+    with pytest.raises(MHDError) as e:
+        Batch([dict(nx=16, ny=16, dx=0.1, dy=0.1, eta=1e-3)])
+    assert e.value.status == 6
