@@ -11,6 +11,11 @@ Lines printed (rank 0, one JSON line):
                       cpu_baseline = the reference's own IMEX step (compiled here) on 1 host core.
   --impl reference    the reference's CPU implementation (oracle/_ref, compiled from the
                       reference's headers) on the same workload, a bounded sample per step.
+The default line also carries "batched": 64 independent periodic runs of seeded sizes from
+{256, 384, 512, 768, 1024}^2 (random smooth states, eta log-uniform in [1e-4, 1e-2], CFL dt per
+instance), stepped as one batch (one launch per stage, CUDA graph, autotuned decomposition) and,
+for comparison, as the plain per-instance loop (one context per instance, each run in turn on one
+stream), both timed with CUDA events.
 Multi-GPU: replicas only (independent simulations per rank, no collective on the data path).
 """
 from __future__ import annotations
@@ -321,6 +326,9 @@ def run_gpu_arm(args):
                              f"on the same {n}x{n} Orszag-Tang state; reference headers compiled "
                              f"-O3 -ffast-math, single thread, {r[1]:.1f} s"}
     clk = clocks.summary()
+    batched = None
+    if not args.no_batch:
+        batched = measure_batched(torch, m, args.batch_steps)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -335,6 +343,7 @@ def run_gpu_arm(args):
         "clocks": clk,
         "gpu_launches": args.steps * ctx.launches_per_step,
         "status": [status, status2],
+        "batched": batched,
     }
     ctx.close()
     if dist is not None:
@@ -343,6 +352,71 @@ def run_gpu_arm(args):
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+BATCH_WORKLOAD = "mixed64_sizes256-1024_seed2024_eta1e-4..1e-2_cfl0.5"
+
+
+def measure_batched(torch, m, steps):
+    """Batched stepping of the mixed-size batch vs the plain per-instance loop (same inputs,
+    same steps, CFL dt per instance). Returns the "batched" object of the JSON line."""
+    specs = m.problems.mixed_batch(64)
+    insts, ics = [], []
+    for n_i, eta_i, seed_i in specs:
+        fields, dx_i = m.problems.random_instance(n_i, seed_i)
+        insts.append(dict(nx=n_i, ny=n_i, dx=dx_i, dy=dx_i, eta=eta_i))
+        ics.append(fields)
+    zones = float(sum(s["nx"] * s["ny"] for s in insts))
+
+    b = m.Batch(insts)
+    for i, f in enumerate(ics):
+        b.set_state(i, f)
+    tuning = b.autotune()
+    bstream = torch.cuda.ExternalStream(b.stream)
+    b.run(4, record=False)  # warm-up (graph capture path included)
+    for i, f in enumerate(ics):
+        b.set_state(i, f)
+    b.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(bstream)
+    b.run(steps, record=False)
+    e1.record(bstream)
+    e1.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    worst, _ = b.synchronize_status()
+    launches = b.launches_per_step
+    b.close()
+
+    # plain loop: one context per instance on one shared stream, each advanced `steps` steps in turn
+    shared = torch.cuda.Stream()
+    ctxs = []
+    for s, f in zip(insts, ics):
+        c = m.Context(s["nx"], s["ny"], s["dx"], s["dy"], s["eta"], stream=shared.cuda_stream)
+        c.set_state(f)
+        c.run(4, record=False)  # warm-up
+        c.set_state(f)
+        ctxs.append(c)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(shared)
+    for c in ctxs:
+        c.run(steps, record=False)
+    p1.record(shared)
+    p1.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    for c in ctxs:
+        c.close()
+    return {
+        "workload": BATCH_WORKLOAD, "instances": len(insts), "steps": steps,
+        "zones_per_step": int(zones), "value": zones * steps / (batch_ms * 1e-3), "unit": UNIT,
+        "ms_per_step": batch_ms / steps, "launches_per_step": launches,
+        "tuning": {k: tuning[k] for k in ("stage_rows", "cg_rows", "cg_order")},
+        "plain_loop": {"value": zones * steps / (plain_ms * 1e-3), "unit": UNIT,
+                       "ms_per_step": plain_ms / steps,
+                       "how": "one context per instance on one stream, run(steps) in turn"},
+        "speedup_vs_plain_loop": plain_ms / batch_ms, "status": worst,
+    }
 
 
 def main():
@@ -354,6 +428,8 @@ def main():
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
