@@ -15,7 +15,12 @@ The default line also carries "batched": 64 independent periodic runs of seeded 
 {256, 384, 512, 768, 1024}^2 (random smooth states, eta log-uniform in [1e-4, 1e-2], CFL dt per
 instance), stepped as one batch (one launch per stage, CUDA graph, autotuned decomposition) and,
 for comparison, as the plain per-instance loop (one context per instance, each run in turn on one
-stream), both timed with CUDA events.
+stream), both timed with CUDA events; and "adjoint": the differentiable form on a 1024^2 smooth
+state (4 random Fourier modes, velocity amplitude 0.05, Az amplitude 0.1, rho = p = 1), eta = 5e-3,
+100 fixed steps of dt = 1e-3, checkpoint every 10 steps, loss = 1/2 |rho(T) - rho_target|^2 with the
+target from the forward solver at eta = 4e-3: forward and backward device times per step (the
+backward includes the recomputation of every segment) and a central-difference check of dL/deta
+and of the directional derivative along a smooth perturbation of Az.
 Multi-GPU: replicas only (independent simulations per rank, no collective on the data path).
 """
 from __future__ import annotations
@@ -329,6 +334,9 @@ def run_gpu_arm(args):
     batched = None
     if not args.no_batch:
         batched = measure_batched(torch, m, args.batch_steps)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = measure_adjoint(torch, m)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -344,6 +352,7 @@ def run_gpu_arm(args):
         "gpu_launches": args.steps * ctx.launches_per_step,
         "status": [status, status2],
         "batched": batched,
+        "adjoint": adjoint,
     }
     ctx.close()
     if dist is not None:
@@ -419,6 +428,106 @@ def measure_batched(torch, m, steps):
     }
 
 
+ADJ_WORKLOAD = "adjoint_1024x1024_4modes_v0.05_az0.1_eta5e-3_dt1e-3_100steps_ckpt10"
+
+
+def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
+    """Forward / backward device time of the differentiable trajectory and a gradient check."""
+    from magnetohydrodynamics_simulator_b200.autograd import state_from_potential, trajectory
+
+    dev = "cuda"
+    dx = 2 * np.pi / n
+    rng = np.random.default_rng(5)
+    x = np.arange(n) * dx
+    X, Y = np.meshgrid(x, x)
+
+    def modes(amp, shift):
+        f = np.zeros((n, n))
+        for _ in range(4):
+            kx, ky = rng.integers(-4, 5, size=2)
+            f += amp * rng.uniform(0.5, 1.0) * np.sin(kx * (X + shift) + ky * (Y + shift) + rng.uniform(0, 2 * np.pi))
+        return torch.tensor(f, device=dev)
+
+    vx, vy = modes(0.05, dx / 2), modes(0.05, dx / 2)
+    az0, daz = modes(0.1, 0.0), modes(0.1, 0.0)
+    one = torch.ones(n, n, dtype=torch.float64, device=dev)
+    adj = m.Adjoint(n, n, dx, dx, eta, dt, nsteps, checkpoint_every=every)
+    astream = torch.cuda.ExternalStream(adj.stream)
+
+    def u0_of(az):
+        return state_from_potential(az, one, vx, vy, one, dx, dx).contiguous()
+
+    def loss(az, eta_v, target):
+        uT = trajectory(u0_of(az), torch.tensor(eta_v, dtype=torch.float64, device=dev), adj)
+        return 0.5 * ((uT[0] - target) ** 2).sum()
+
+    with torch.no_grad():
+        target = trajectory(u0_of(az0), torch.tensor(0.8 * eta, dtype=torch.float64, device=dev), adj)[0].clone()
+    # warm-up forward + backward
+    az = az0.clone().requires_grad_(True)
+    loss(az, eta, target).backward()
+    # timed: device time of the library calls, events on the library's stream
+    u0 = u0_of(az0)
+    uT = torch.empty_like(u0)
+    gT = torch.randn_like(u0)
+    g0 = torch.empty_like(u0)
+    ptr = lambda t: [t[k].data_ptr() for k in range(6)]  # noqa: E731
+    adj.set_eta(eta)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(astream)
+    adj.forward(ptr(u0), ptr(uT))
+    ev[1].record(astream)
+    adj.backward(ptr(gT), ptr(g0))
+    ev[2].record(astream)
+    ev[2].synchronize()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    # gradients through torch.autograd vs central differences of the forward solver, taken on the
+    # final state (difference of two trajectories, contracted afterwards)
+    az = az0.clone().requires_grad_(True)
+    eta_t = torch.tensor(eta, dtype=torch.float64, device=dev, requires_grad=True)
+    uTg = trajectory(u0_of(az), eta_t, adj)
+    L0 = 0.5 * ((uTg[0] - target) ** 2).sum()
+    L0.backward()
+    g_eta, g_dir_loss = float(eta_t.grad), float((az.grad * daz).sum())
+    w = torch.randn(target.shape, generator=torch.Generator(device=dev).manual_seed(3),
+                    dtype=torch.float64, device=dev)
+    az = az0.clone().requires_grad_(True)
+    e0 = torch.tensor(eta, dtype=torch.float64, device=dev)
+    (trajectory(u0_of(az), e0, adj)[0] * w).sum().backward()
+    g_dir = float((az.grad * daz).sum())
+    with torch.no_grad():
+        h = 1e-3 * eta
+        rp, rm = trajectory(u0_of(az0), e0 + h, adj)[0], trajectory(u0_of(az0), e0 - h, adj)[0]
+        fd_eta = float((((rp - rm) / (2 * h)) * ((rp + rm) / 2 - target)).sum())
+        s_ = 3e-7
+        rp = trajectory(u0_of(az0 + s_ * daz), e0, adj)[0]
+        rm = trajectory(u0_of(az0 - s_ * daz), e0, adj)[0]
+        fd_dir = float((((rp - rm) / (2 * s_)) * w).sum())
+        fd_dir_loss = float((((rp - rm) / (2 * s_)) * ((rp + rm) / 2 - target)).sum())
+    f_launch, a_launch = adj.launch_counts()
+    adj.close()
+    return {
+        "workload": ADJ_WORKLOAD, "grid": [n, n], "steps": nsteps, "checkpoint_every": every,
+        "forward_ms_per_step": fwd_ms / nsteps, "backward_ms_per_step": bwd_ms / nsteps,
+        "adjoint_over_forward": bwd_ms / fwd_ms,
+        "adjoint_over_forward_excluding_recompute": (bwd_ms - fwd_ms) / fwd_ms,
+        "launches_per_step": {"forward": f_launch, "adjoint": a_launch, "recompute": f_launch},
+        "gradient_check": {
+            "method": "central differences of the final state (two trajectories), contracted after",
+            "d_eta": {"loss": "1/2|rho(T) - rho_target|^2", "adjoint": g_eta,
+                      "central_difference": fd_eta, "step": 1e-3 * eta,
+                      "rel_err": abs(g_eta - fd_eta) / abs(fd_eta)},
+            "d_az_direction": {"loss": "<w, rho(T)>, w ~ N(0,1)", "adjoint": g_dir,
+                               "central_difference": fd_dir, "step": 3e-7,
+                               "rel_err": abs(g_dir - fd_dir) / abs(fd_dir)},
+            "d_az_direction_density_loss": {"loss": "1/2|rho(T) - rho_target|^2", "adjoint": g_dir_loss,
+                                            "central_difference": fd_dir_loss, "step": 3e-7,
+                                            "rel_err": abs(g_dir_loss - fd_dir_loss) / abs(fd_dir_loss)},
+        },
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,6 +539,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -223,6 +223,43 @@ void* mhd_batch_stream(mhd_batch* b);
 /* Kernel launches one mhd_batch_step enqueues. */
 int mhd_batch_launches_per_step(mhd_batch* b);
 
+/* ---------------------------------------------------------------------------------------------
+ * Differentiation (no counterpart in the reference): the discrete adjoint of a fixed-dt
+ * trajectory of IMEX steps (solvers.hpp:491-613 with the driver's matrix alpha = dt*eta*g),
+ * computed by hand-written adjoint kernels of the reconstruction, HLL flux, CT and stage update
+ * and by the (self-adjoint) implicit solve. The forward pass keeps every checkpoint_every-th
+ * state; the backward pass recomputes each segment of steps from its checkpoint and runs the
+ * adjoint steps backwards through it. All state arguments are device pointers to dense nx*ny
+ * planes in the order rho, mx, my, E, bxf, byf. Density and pressure floors are differentiated as
+ * clamps (zero derivative where active); minmod, HLL and CT branches as selections. */
+typedef struct mhd_adjoint mhd_adjoint;
+
+/* p: the grid (nx, ny, dx, dy, eta, ct_mode, cg_tol, cg_max_iters, cg_timeout_s are used);
+ * dt > 0 the fixed step; nsteps >= 1; checkpoint_every >= 1. */
+mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkpoint_every,
+                          void* stream, mhd_adjoint** out);
+mhd_status mhd_adj_destroy(mhd_adjoint* a);
+/* Resistivity of the following passes (the matrix coefficient follows: alpha = dt*eta*g). */
+mhd_status mhd_adj_set_eta(mhd_adjoint* a, double eta);
+/* nsteps steps from u0; the final state is written to uT. Keeps the checkpoints. */
+mhd_status mhd_adj_forward(mhd_adjoint* a, const double* const u0[6], double* const uT[6]);
+/* Given dL/duT (device), write dL/du0 (device) and dL/deta (host, may be NULL) of the trajectory
+ * of the last mhd_adj_forward. Synchronous. */
+mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6],
+                            double* const grad_u0[6], double* grad_eta);
+/* One step's vector-Jacobian product at state u: lam = (dU^{n+1}/dU^n)^T lam_next, and
+ * *grad_eta (host, may be NULL) = lam_next . dU^{n+1}/deta. Synchronous. */
+mhd_status mhd_adj_step_vjp(mhd_adjoint* a, const double* const u[6],
+                            const double* const lam_next[6], double* const lam[6],
+                            double* grad_eta);
+/* Vector-Jacobian product of the explicit rate (solvers.hpp:393-402) at u: out = F'(u)^T w. */
+mhd_status mhd_adj_rate_vjp(mhd_adjoint* a, const double* const u[6], const double* const w[6],
+                            double* const out[6]);
+/* Kernel launches of one forward step and of one adjoint step (for launch accounting). */
+mhd_status mhd_adj_launch_counts(mhd_adjoint* a, int* forward_step, int* adjoint_step);
+/* The stream the adjoint object enqueues on (a cudaStream_t). */
+void* mhd_adj_stream(mhd_adjoint* a);
+
 const char* mhd_status_string(mhd_status s);
 
 /* 1 when a device this library was built for is present, else 0. */

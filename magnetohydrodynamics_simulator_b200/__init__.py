@@ -5,6 +5,8 @@ The product is the shared library ``libmhd_b200.so`` (CUDA kernels + the C ABI o
 
 * :class:`Context` -- one device-resident simulation (set_state / step / run / cfl_dt / divb);
 * :class:`Batch` -- many independent simulations of uneven sizes stepped together;
+* :class:`Adjoint` -- a differentiable fixed-dt trajectory (hand-written adjoint kernels); its
+  torch.autograd binding is :mod:`magnetohydrodynamics_simulator_b200.autograd`;
 * :mod:`problems` -- the benchmark initial conditions.
 """
 from .capi import (  # noqa: F401
@@ -13,6 +15,7 @@ from .capi import (  # noqa: F401
     FIELDS,
     LAYOUT_DENSE,
     LAYOUT_PADDED,
+    Adjoint,
     Batch,
     Context,
     MHDError,
@@ -23,6 +26,7 @@ from .capi import (  # noqa: F401
 from . import problems  # noqa: F401
 
 __all__ = [
+    "Adjoint",
     "Batch",
     "Context",
     "MHDError",

@@ -135,6 +135,17 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_batch_launches_per_step.argtypes = [vp]
     lib.mhd_resistive_rate_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_double,
                                                vp, vp, vp, vp, llp, vp]
+    lib.mhd_adj_create.argtypes = [ctypes.POINTER(Params), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                   vp, ctypes.POINTER(vp)]
+    lib.mhd_adj_destroy.argtypes = [vp]
+    lib.mhd_adj_set_eta.argtypes = [vp, ctypes.c_double]
+    lib.mhd_adj_forward.argtypes = [vp, P6, P6]
+    lib.mhd_adj_backward.argtypes = [vp, P6, P6, _dp]
+    lib.mhd_adj_step_vjp.argtypes = [vp, P6, P6, P6, _dp]
+    lib.mhd_adj_rate_vjp.argtypes = [vp, P6, P6, P6]
+    lib.mhd_adj_launch_counts.argtypes = [vp, ip, ip]
+    lib.mhd_adj_stream.argtypes = [vp]
+    lib.mhd_adj_stream.restype = vp
     _lib = lib
     return lib
 
@@ -431,6 +442,77 @@ class Batch:
     @property
     def launches_per_step(self) -> int:
         return int(self.lib.mhd_batch_launches_per_step(self.h))
+
+
+class Adjoint:
+    """Differentiable fixed-dt trajectory of `nsteps` IMEX steps of one grid (the mhd_adj_* ABI):
+    forward keeps every `checkpoint_every`-th state, backward recomputes each segment and runs the
+    hand-written adjoint steps. State arguments are lists of six device addresses (dense planes
+    rho, mx, my, E, bxf, byf). Calls are synchronous on the object's own stream."""
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, eta: float, dt: float, nsteps: int,
+                 checkpoint_every: int = 10, *, ct_mode: int = 0, cg_tol: float = 0.0,
+                 cg_max_iters: int = 0, cg_timeout_s: float = 30.0, stream: int | None = None):
+        self.lib = load_library()
+        self.nx, self.ny, self.dt, self.nsteps = int(nx), int(ny), float(dt), int(nsteps)
+        self.checkpoint_every = int(checkpoint_every)
+        p = Params()
+        _check(self.lib.mhd_default_params(ctypes.byref(p), nx, ny, dx, dy, eta), "mhd_default_params")
+        p.ct_mode = ct_mode
+        p.cg_tol = cg_tol
+        p.cg_max_iters = cg_max_iters
+        p.cg_timeout_s = cg_timeout_s
+        self.params = p
+        self.eta = float(eta)
+        h = ctypes.c_void_p()
+        _check(self.lib.mhd_adj_create(ctypes.byref(p), dt, nsteps, checkpoint_every,
+                                       ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)),
+               "mhd_adj_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_adj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_eta(self, eta: float):
+        _check(self.lib.mhd_adj_set_eta(self.h, float(eta)), "mhd_adj_set_eta")
+        self.eta = float(eta)
+
+    def forward(self, u0: Sequence[int], uT: Sequence[int]):
+        _check(self.lib.mhd_adj_forward(self.h, _device_ptrs(u0), _device_ptrs(uT)), "mhd_adj_forward")
+
+    def backward(self, grad_uT: Sequence[int], grad_u0: Sequence[int]) -> float:
+        g = ctypes.c_double()
+        _check(self.lib.mhd_adj_backward(self.h, _device_ptrs(grad_uT), _device_ptrs(grad_u0),
+                                         ctypes.byref(g)), "mhd_adj_backward")
+        return g.value
+
+    def step_vjp(self, u: Sequence[int], lam_next: Sequence[int], lam: Sequence[int]) -> float:
+        g = ctypes.c_double()
+        _check(self.lib.mhd_adj_step_vjp(self.h, _device_ptrs(u), _device_ptrs(lam_next),
+                                         _device_ptrs(lam), ctypes.byref(g)), "mhd_adj_step_vjp")
+        return g.value
+
+    def rate_vjp(self, u: Sequence[int], w: Sequence[int], out: Sequence[int]):
+        _check(self.lib.mhd_adj_rate_vjp(self.h, _device_ptrs(u), _device_ptrs(w), _device_ptrs(out)),
+               "mhd_adj_rate_vjp")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mhd_adj_stream(self.h) or 0
+
+    def launch_counts(self):
+        f, a = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.mhd_adj_launch_counts(self.h, ctypes.byref(f), ctypes.byref(a)),
+               "mhd_adj_launch_counts")
+        return int(f.value), int(a.value)
 
 
 def ars_gamma() -> float:
