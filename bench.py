@@ -19,8 +19,8 @@ stream), both timed with CUDA events; and "adjoint": the differentiable form on 
 state (4 random Fourier modes, velocity amplitude 0.05, Az amplitude 0.1, rho = p = 1), eta = 5e-3,
 100 fixed steps of dt = 1e-3, checkpoint every 10 steps, loss = 1/2 |rho(T) - rho_target|^2 with the
 target from the forward solver at eta = 4e-3: forward and backward device times per step (the
-backward includes the recomputation of every segment) and a central-difference check of dL/deta
-and of the directional derivative along a smooth perturbation of Az.
+backward recomputes each segment's explicit stages from its checkpoint) and central-difference
+checks of dL/deta and of the derivative along a smooth perturbation of Az.
 Multi-GPU: replicas only (independent simulations per rank, no collective on the data path).
 """
 from __future__ import annotations
@@ -511,8 +511,9 @@ def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
         "workload": ADJ_WORKLOAD, "grid": [n, n], "steps": nsteps, "checkpoint_every": every,
         "forward_ms_per_step": fwd_ms / nsteps, "backward_ms_per_step": bwd_ms / nsteps,
         "adjoint_over_forward": bwd_ms / fwd_ms,
-        "adjoint_over_forward_excluding_recompute": (bwd_ms - fwd_ms) / fwd_ms,
-        "launches_per_step": {"forward": f_launch, "adjoint": a_launch, "recompute": f_launch},
+        "backward_includes": "recomputation of each segment's explicit stages from its checkpoint "
+                             "(the implicit solutions of every step are kept by the forward pass)",
+        "launches_per_step": {"forward": f_launch, "backward": a_launch},
         "gradient_check": {
             "method": "central differences of the final state (two trajectories), contracted after",
             "d_eta": {"loss": "1/2|rho(T) - rho_target|^2", "adjoint": g_eta,

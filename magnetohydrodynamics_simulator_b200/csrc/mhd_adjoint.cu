@@ -3,11 +3,12 @@
 // Forward: the same kernels as a single context (stage 1, implicit solve, stage 2, implicit solve,
 // finalize) on a fixed dt, with every intermediate a step produces kept in a slot:
 //   T[6]   predictor U1* (stage 1)          A[6]  accumulator -> U2* (stage 2; its hydro planes
-//   x1, x2 corner fields of the two solves        become U^{n+1}'s after the finalize's floor)
-//   Bn[2]  B^{n+1} (finalize)
-// so U^{n+1} = (A[0..3], Bn). A plain forward pass alternates two slots and copies every
-// checkpoint_every-th state out; the backward pass recomputes a segment of steps into one slot per
-// step and then runs the adjoint steps backwards over it.
+//   Bn[2]  B^{n+1} (finalize)                     become U^{n+1}'s after the finalize's floor)
+// so U^{n+1} = (A[0..3], Bn). The corner fields x1, x2 of every step's two implicit solves are kept
+// for the whole trajectory (2 planes per step). A forward pass alternates two slots and copies every
+// checkpoint_every-th state out; the backward pass recomputes the explicit stages of a segment of
+// steps into one slot per step (the stored solutions stand in for the solves) and then runs the
+// adjoint steps backwards over it.
 //
 // Adjoint of one step (U^{n+1} = Phi(U^n); notation of mhd_adjoint.cuh, cg = dt*g, cd = dt*d,
 // c1md = dt*(1-d), c1mg = dt*(1-g), S the implicit rate, R the explicit resistive rate):
@@ -39,14 +40,12 @@ using namespace mhd;
 
 namespace {
 
-constexpr int kSlotPlanes = 16;     // T[6], A[6], x1, x2, Bn[2]
+constexpr int kSlotPlanes = 14;     // T[6], A[6], Bn[2]
 constexpr int kScratchPlanes = 59;  // adjoint-step and solver scratch (see AdjScratch)
 
 struct Slot {
     double* T[6];
     double* A[6];
-    double* x1;
-    double* x2;
     double* Bn[2];
 };
 
@@ -82,6 +81,7 @@ struct mhd_adjoint {
     double* pool = nullptr;
     std::vector<double*> ckpt;  // nseg * 6 planes
     std::vector<Slot> slots;
+    std::vector<double*> xs;  // 2 * nsteps planes: the corner fields x1, x2 of every step
     AdjScratch s{};
     StepCoeffs* coeffs = nullptr;
     DeviceStatus* status = nullptr;
@@ -170,22 +170,24 @@ mhd_status solve(mhd_adjoint* a, const double* bxf, const double* byf, double rh
     return MHD_OK;
 }
 
-// One forward step from U into slot sl (U^{n+1} = (sl.A[0..3], sl.Bn)).
-mhd_status forward_step(mhd_adjoint* a, const double* const U[6], const Slot& sl) {
+// One forward step from U into slot sl (U^{n+1} = (sl.A[0..3], sl.Bn)) with the corner fields of
+// the two solves in x1, x2: solved when do_solve, else taken as stored by an earlier pass (the
+// same inputs give bit-identical stage outputs, so the stored solutions are those of this step).
+mhd_status forward_step(mhd_adjoint* a, const double* const U[6], const Slot& sl, double* x1,
+                        double* x2, bool do_solve) {
     const Domain& D = a->dom;
     k_stage_sweep<1><<<a->st_blocks[0], 32 * SW_WARPS, 0, a->stream>>>(
         D, a->coeffs, cplanes6(U), nullptr, planes6(sl.T), planes6(sl.A), a->sg[0]);
     MHD_TRY(cudaGetLastError());
-    mhd_status s = solve(a, sl.T[4], sl.T[5], a->eta, sl.x1);
-    if (s != MHD_OK) return s;
+    mhd_status s;
+    if (do_solve && (s = solve(a, sl.T[4], sl.T[5], a->eta, x1)) != MHD_OK) return s;
     k_stage_sweep<2><<<a->st_blocks[1], 32 * SW_WARPS, 0, a->stream>>>(
-        D, a->coeffs, cplanes6(sl.T), sl.x1, planes6(sl.T), planes6(sl.A), a->sg[1]);
+        D, a->coeffs, cplanes6(sl.T), x1, planes6(sl.T), planes6(sl.A), a->sg[1]);
     MHD_TRY(cudaGetLastError());
-    s = solve(a, sl.A[4], sl.A[5], a->eta, sl.x2);
-    if (s != MHD_OK) return s;
+    if (do_solve && (s = solve(a, sl.A[4], sl.A[5], a->eta, x2)) != MHD_OK) return s;
     MHD_TRY(cudaMemsetAsync(&a->status->smax_bits, 0, sizeof(unsigned long long), a->stream));
     k_finalize_sweep<<<a->fn_blocks, 32 * FS_WARPS, 0, a->stream>>>(
-        D, a->coeffs, planes6(sl.A), sl.x2, sl.Bn[0], sl.Bn[1], a->status, a->fg);
+        D, a->coeffs, planes6(sl.A), x2, sl.Bn[0], sl.Bn[1], a->status, a->fg);
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
 }
@@ -257,9 +259,10 @@ mhd_status axpby(mhd_adjoint* a, int nplanes, double ca, const double* const* x,
     return MHD_OK;
 }
 
-// The adjoint of the step taken from U with intermediates in sl: s.lam holds lam' on entry and
-// lam on return; geta accumulates.
-mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl) {
+// The adjoint of the step taken from U with intermediates in sl, x1, x2: s.lam holds lam' on
+// entry and lam on return; geta accumulates.
+mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl, const double* x1,
+                        const double* x2) {
     const Domain& D = a->dom;
     AdjScratch& s = a->s;
     const double eta = a->eta;
@@ -270,7 +273,7 @@ mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl
     mhd_status r;
     // final combination: B^{n+1} = A_B + cg * eta * C Jz(B2)
     k_adj_jz<<<B, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
-    k_adj_jz<<<B, 256, 0, st>>>(D, sl.A[4], sl.A[5], 1.0, sl.x2, cg, s.c2);  // Jz(B2)
+    k_adj_jz<<<B, 256, 0, st>>>(D, sl.A[4], sl.A[5], 1.0, x2, cg, s.c2);  // Jz(B2)
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.c1, s.c2, -cg)) != MHD_OK) return r;
     k_adj_curl<<<B, 256, 0, st>>>(D, s.c1, cg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
@@ -284,13 +287,13 @@ mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl
     if ((r = dot_acc(a, s.y, s.c2, -1.0)) != MHD_OK) return r;
     // g2 = R(B1) with weight c1mg
     k_adj_jz<<<B, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
-    k_adj_jz<<<B, 256, 0, st>>>(D, sl.T[4], sl.T[5], 1.0, sl.x1, cg, s.c2);  // Jz(B1)
+    k_adj_jz<<<B, 256, 0, st>>>(D, sl.T[4], sl.T[5], 1.0, x1, cg, s.c2);  // Jz(B1)
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.c1, s.c2, -c1mg)) != MHD_OK) return r;
     k_adj_curl<<<B, 256, 0, st>>>(D, s.c1, c1mg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
                                   s.fb[0], s.fb[1]);
     // f2 = F(U1), U1 = (T hydro, B1), weight c1md
-    k_adj_curl<<<B, 256, 0, st>>>(D, sl.x1, cg, sl.T[4], sl.T[5], 1.0, nullptr, nullptr, 0.0,
+    k_adj_curl<<<B, 256, 0, st>>>(D, x1, cg, sl.T[4], sl.T[5], 1.0, nullptr, nullptr, 0.0,
                                   s.B1[0], s.B1[1]);
     MHD_TRY(cudaGetLastError());
     const double* U1[6] = {sl.T[0], sl.T[1], sl.T[2], sl.T[3], s.B1[0], s.B1[1]};
@@ -308,10 +311,12 @@ mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.y, s.c2, -1.0)) != MHD_OK) return r;
     // stage 1: T = U + cg f1, A = U + cd f1 (+ ...): lam = lambda_A + lambda_T + F'(U)^T w
-    const double* lamc[6] = {s.lam[0], s.lam[1], s.lam[2], s.lam[3], s.lam[4], s.lam[5]};
-    const double* lamTc[6] = {s.lamT[0], s.lamT[1], s.lamT[2], s.lamT[3], s.lamT[4], s.lamT[5]};
-    if ((r = axpby(a, 6, cd, lamc, cg, lamTc, s.w)) != MHD_OK) return r;
-    if ((r = axpby(a, 6, 1.0, lamc, 1.0, lamTc, s.lam)) != MHD_OK) return r;
+    {
+        Planes6C lt;
+        for (int k = 0; k < 6; ++k) lt.f[k] = s.lamT[k];
+        k_adj_close<<<B, 256, 0, st>>>(a->n, cd, cg, planes6(s.lam), lt, planes6(s.w));
+        MHD_TRY(cudaGetLastError());
+    }
     const double* wc[6] = {s.w[0], s.w[1], s.w[2], s.w[3], s.w[4], s.w[5]};
     return rate_vjp(a, U, wc, 1.0, 1, s.lam);
 }
@@ -424,7 +429,8 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
     a->ew_blocks = std::max(1, std::min((int)((a->n + 255) / 256), a->num_sms * 8));
     a->dot_blocks = std::max(1, std::min((int)((a->n + 255) / 256), a->num_sms * 2));
     // memory: checkpoints, slots, scratch
-    const size_t planes = (size_t)a->nseg * 6 + (size_t)a->nslots * kSlotPlanes + kScratchPlanes;
+    const size_t planes = (size_t)a->nseg * 6 + (size_t)a->nslots * kSlotPlanes +
+                          2 * (size_t)a->nsteps + kScratchPlanes;
     if (cudaMalloc(&a->pool, planes * a->n * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&a->coeffs, sizeof(StepCoeffs)) != cudaSuccess ||
         cudaMalloc(&a->status, sizeof(DeviceStatus)) != cudaSuccess ||
@@ -448,11 +454,11 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
     for (Slot& sl : a->slots) {
         for (int k = 0; k < 6; ++k) sl.T[k] = take();
         for (int k = 0; k < 6; ++k) sl.A[k] = take();
-        sl.x1 = take();
-        sl.x2 = take();
         sl.Bn[0] = take();
         sl.Bn[1] = take();
     }
+    a->xs.resize(2 * (size_t)a->nsteps);
+    for (auto& x : a->xs) x = take();
     AdjScratch& s = a->s;
     for (int k = 0; k < 6; ++k) s.lam[k] = take();
     for (int k = 0; k < 6; ++k) s.lamT[k] = take();
@@ -523,7 +529,7 @@ mhd_status mhd_adj_forward(mhd_adjoint* a, const double* const u0[6], double* co
             for (int k = 0; k < 6; ++k) U[k] = ck[k];
         }
         const Slot& sl = a->slots[step % 2];
-        if ((s = forward_step(a, U, sl)) != MHD_OK) return s;
+        if ((s = forward_step(a, U, sl, a->xs[2 * step], a->xs[2 * step + 1], true)) != MHD_OK) return s;
         next_state(sl, U);
     }
     if ((s = copy_planes(a, uT, U)) != MHD_OK) return s;
@@ -544,12 +550,13 @@ mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6], doub
     for (int seg = a->nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * a->every, s1 = std::min(a->nsteps, s0 + a->every);
         const double* const* ck = &a->ckpt[(size_t)seg * 6];
-        // recompute the segment, keeping every step's intermediates
+        // recompute the explicit stages of the segment, keeping every step's intermediates
         const double* U[6];
         for (int k = 0; k < 6; ++k) U[k] = ck[k];
         for (int step = s0; step < s1; ++step) {
             const Slot& sl = a->slots[step - s0];
-            if ((s = forward_step(a, U, sl)) != MHD_OK) return s;
+            if ((s = forward_step(a, U, sl, a->xs[2 * step], a->xs[2 * step + 1], false)) != MHD_OK)
+                return s;
             next_state(sl, U);
         }
         for (int step = s1 - 1; step >= s0; --step) {
@@ -559,7 +566,9 @@ mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6], doub
             } else {
                 next_state(a->slots[step - s0 - 1], Us);
             }
-            if ((s = adjoint_step(a, Us, a->slots[step - s0])) != MHD_OK) return s;
+            if ((s = adjoint_step(a, Us, a->slots[step - s0], a->xs[2 * step], a->xs[2 * step + 1])) !=
+                MHD_OK)
+                return s;
         }
     }
     const double* lamc[6] = {a->s.lam[0], a->s.lam[1], a->s.lam[2], a->s.lam[3], a->s.lam[4], a->s.lam[5]};
@@ -578,10 +587,10 @@ mhd_status mhd_adj_step_vjp(mhd_adjoint* a, const double* const u[6], const doub
     for (int k = 0; k < 6; ++k)
         if (!u[k] || !lam_next[k] || !lam[k]) return MHD_ERR_INVALID_ARGUMENT;
     a->have_forward = false;  // the slots are reused
-    if ((s = forward_step(a, u, a->slots[0])) != MHD_OK) return s;
+    if ((s = forward_step(a, u, a->slots[0], a->xs[0], a->xs[1], true)) != MHD_OK) return s;
     if ((s = copy_planes(a, a->s.lam, lam_next)) != MHD_OK) return s;
     MHD_TRY(cudaMemsetAsync(a->geta, 0, sizeof(double), a->stream));
-    if ((s = adjoint_step(a, u, a->slots[0])) != MHD_OK) return s;
+    if ((s = adjoint_step(a, u, a->slots[0], a->xs[0], a->xs[1])) != MHD_OK) return s;
     const double* lamc[6] = {a->s.lam[0], a->s.lam[1], a->s.lam[2], a->s.lam[3], a->s.lam[4], a->s.lam[5]};
     if ((s = copy_planes(a, lam, lamc)) != MHD_OK) return s;
     MHD_TRY(cudaMemcpyAsync(a->host_small, a->geta, sizeof(double), cudaMemcpyDeviceToHost, a->stream));
@@ -608,9 +617,10 @@ mhd_status mhd_adj_launch_counts(mhd_adjoint* a, int* forward_step, int* adjoint
     if (!a) return MHD_ERR_INVALID_ARGUMENT;
     // forward: stage 1, solve, stage 2, solve, finalize
     if (forward_step) *forward_step = 5;
-    // adjoint: 4 corner currents, 4 dot products (2 launches each), 4 curls, 2 solves,
-    // 2 explicit-rate VJPs (4 kernels + primitives each), 3 plane combinations
-    if (adjoint_step) *adjoint_step = 4 + 8 + 5 + 2 + 10 + 3;
+    // adjoint: 4 corner currents, 4 dot products (2 launches each), 5 curls, 2 solves,
+    // 2 explicit-rate VJPs (4 kernels + primitives each), 2 plane combinations; plus the
+    // recomputation of the step's explicit stages (stage 1, stage 2, finalize)
+    if (adjoint_step) *adjoint_step = 4 + 8 + 5 + 2 + 10 + 2 + 3;
     return MHD_OK;
 }
 

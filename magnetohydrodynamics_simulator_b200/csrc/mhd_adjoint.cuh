@@ -31,6 +31,8 @@ struct PrimAdj {
     double rho, vx, vy, p, bx, by;
 };
 
+constexpr double kInvGm1 = 1.0 / (kGammaGas - 1.0);  // d E / d p of the ideal-gas energy
+
 // fast_speed (HLL.hpp:107-122): given the adjoint of c_f, accumulate into w's adjoint and bn's.
 __device__ __forceinline__ void fast_speed_vjp(const Prim& w, double bn, double ac, PrimAdj& aw,
                                                double& abn) {
@@ -97,7 +99,7 @@ __device__ __forceinline__ void phys_flux_vjp(const Prim& w, const Flux& aF, Pri
     a.bx += avb * w.vx;
     a.by += avb * w.vy;
     // E = p/(gamma-1) + (rho v2 + b2)/2 ; pt = p + b2/2
-    a.p += aE / (kGammaGas - 1.0) + apt;
+    a.p += aE * kInvGm1 + apt;
     a.rho += aE * 0.5 * v2;
     const double av2 = aE * 0.5 * w.rho;
     const double ab2 = aE * 0.5 + 0.5 * apt;
@@ -114,7 +116,7 @@ __device__ __forceinline__ void conserved_vjp(const Prim& w, const Flux& aU, Pri
     a.rho += aU.rho + aU.mx * w.vx + aU.my * w.vy + aU.E * 0.5 * v2;
     a.vx += aU.mx * w.rho + aU.E * w.rho * w.vx;
     a.vy += aU.my * w.rho + aU.E * w.rho * w.vy;
-    a.p += aU.E / (kGammaGas - 1.0);
+    a.p += aU.E * kInvGm1;
     a.bx += aU.E * w.bx;
     a.by += aU.E * w.by;
     if (DIR == 0) a.by += aU.bt;
@@ -210,12 +212,13 @@ __device__ __forceinline__ double ct_weight(double v, int mode, int second) {
 
 // Adjoint of the corner field at corner (ic, jc) from the adjoint w of the face-B rates:
 // rate_bx(i,j) = -(ez(i,j+1) - ez(i,j))/dy, rate_by(i,j) = (ez(i+1,j) - ez(i,j))/dx.
-__device__ __forceinline__ double corner_field_adj(const Domain& D, const double* __restrict__ wbx,
+__device__ __forceinline__ double corner_field_adj(const Domain& D, double idx, double idy,
+                                                   const double* __restrict__ wbx,
                                                    const double* __restrict__ wby, int ic, int jc) {
     const int nx = D.nx, ny = D.ny;
     const int i = wrap(ic, nx), j = wrap(jc, ny), im = wrap(ic - 1, nx), jm = wrap(jc - 1, ny);
-    return (wbx[(size_t)j * nx + i] - wbx[(size_t)jm * nx + i]) / D.dy +
-           (wby[(size_t)j * nx + im] - wby[(size_t)j * nx + i]) / D.dx;
+    return (wbx[(size_t)j * nx + i] - wbx[(size_t)jm * nx + i]) * idy +
+           (wby[(size_t)j * nx + im] - wby[(size_t)j * nx + i]) * idx;
 }
 
 // Corner velocity component (solvers.hpp:294-346; the order of the sum as in the oracle).
@@ -244,7 +247,7 @@ struct CFaceAdjPlanes {
 // top face (y). w: the adjoint of the six rates.
 
 template <int DIR>
-static __global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256, 2)
 k_adj_faces(Domain D, PrimPlanes P, const double* __restrict__ bxf, const double* __restrict__ byf,
             CPlanes w, FaceAdjPlanes out) {
     const int nx = D.nx, ny = D.ny;
@@ -274,7 +277,8 @@ k_adj_faces(Domain D, PrimPlanes P, const double* __restrict__ bxf, const double
         if (DIR == 0) { L.bx = R.bx = bn; L.by = lo[4]; R.by = hi[4]; }
         else { L.by = R.by = bn; L.bx = lo[4]; R.bx = hi[4]; }
         // flux adjoint: rate_q(c) = -(F(c) - F(c-1))/h  =>  aF(c) = (w(c+1) - w(c))/h
-        const double ih = DIR == 0 ? 1.0 / D.dx : 1.0 / D.dy;
+        const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
+        const double ih = DIR == 0 ? idx : idy;
         Flux aF;
         aF.rho = (w.f[0][c1] - w.f[0][c0]) * ih;
         aF.mx = (w.f[1][c1] - w.f[1][c0]) * ih;
@@ -285,14 +289,14 @@ k_adj_faces(Domain D, PrimPlanes P, const double* __restrict__ bxf, const double
             // Fx.bt(i,j) = -eN of corner (i+1, j) = -eS of corner (i+1, j+1)
             const double vyc0 = corner_velocity(P.f[2], nx, ny, i + 1, j);
             const double vyc1 = corner_velocity(P.f[2], nx, ny, i + 1, j + 1);
-            aF.bt = -(corner_field_adj(D, w.f[4], w.f[5], i + 1, j) * ct_weight(vyc0, D.ct_mode, 0) +
-                      corner_field_adj(D, w.f[4], w.f[5], i + 1, j + 1) * ct_weight(vyc1, D.ct_mode, 1));
+            aF.bt = -(corner_field_adj(D, idx, idy, w.f[4], w.f[5], i + 1, j) * ct_weight(vyc0, D.ct_mode, 0) +
+                      corner_field_adj(D, idx, idy, w.f[4], w.f[5], i + 1, j + 1) * ct_weight(vyc1, D.ct_mode, 1));
         } else {
             // Fy.bt(i,j) = eE of corner (i, j+1) = eW of corner (i+1, j+1)
             const double vxc0 = corner_velocity(P.f[1], nx, ny, i, j + 1);
             const double vxc1 = corner_velocity(P.f[1], nx, ny, i + 1, j + 1);
-            aF.bt = corner_field_adj(D, w.f[4], w.f[5], i, j + 1) * ct_weight(vxc0, D.ct_mode, 0) +
-                    corner_field_adj(D, w.f[4], w.f[5], i + 1, j + 1) * ct_weight(vxc1, D.ct_mode, 1);
+            aF.bt = corner_field_adj(D, idx, idy, w.f[4], w.f[5], i, j + 1) * ct_weight(vxc0, D.ct_mode, 0) +
+                    corner_field_adj(D, idx, idy, w.f[4], w.f[5], i + 1, j + 1) * ct_weight(vxc1, D.ct_mode, 1);
         }
         PrimAdj aL = {0, 0, 0, 0, 0, 0}, aR = {0, 0, 0, 0, 0, 0};
         hll_vjp<DIR>(L, R, aF, aL, aR);
@@ -473,10 +477,28 @@ static __global__ void __launch_bounds__(256)
 k_adj_axpby(int nplanes, size_t n, double a, Planes6C x, double b, Planes6C y, Planes out) {
     for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
          g += (size_t)gridDim.x * blockDim.x) {
-        for (int k = 0; k < nplanes; ++k) {
-            double v = a * x.f[k][g];
-            if (y.f[k]) v += b * y.f[k][g];
-            out.f[k][g] = v;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            if (k < nplanes) {
+                double v = a * x.f[k][g];
+                if (y.f[k]) v += b * y.f[k][g];
+                out.f[k][g] = v;
+            }
+        }
+    }
+}
+
+// The two plane combinations that close the adjoint step, in one pass over six planes:
+// w = cd * lam + cg * lamT (the explicit-rate adjoint of stage 1) and lam += lamT.
+static __global__ void __launch_bounds__(256)
+k_adj_close(size_t n, double cd, double cg, Planes lam, Planes6C lamT, Planes w) {
+    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+         g += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double a = lam.f[k][g], t = lamT.f[k][g];
+            w.f[k][g] = cd * a + cg * t;
+            lam.f[k][g] = a + t;
         }
     }
 }
@@ -495,12 +517,14 @@ k_adj_dot_partial(size_t n, const double* __restrict__ a, const double* __restri
     if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
 }
 
+// One warp: lane l sums partials l, l+32, ... in order, then a fixed shuffle tree.
 static __global__ void k_adj_dot_final(const double* __restrict__ partial, int nblocks, double scale,
-                                double* acc) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+                                       double* acc) {
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partial[b];
-    *acc += scale * s;
+    for (int b = threadIdx.x; b < nblocks; b += 32) s += partial[b];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *acc += scale * s;
 }
 
 }  // namespace mhd
