@@ -25,19 +25,40 @@
 namespace mhd {
 
 constexpr int SW_OUT = 28;       // output columns per warp
-constexpr int SW_WARPS = 4;      // warps (independent strips) per block
+// One warp (an independent strip segment) per block: blocks retire warp by warp, so the tail of
+// a launch and the persistent batch kernels balance at warp granularity (measured on B200 against
+// 4-warp blocks at the same registers: stage 1 1.29 -> 1.25 ms, stage 2 1.24 -> 1.15 ms at 4096^2).
+#ifndef MHD_SW_WARPS
+#define MHD_SW_WARPS 1
+#endif
+constexpr int SW_WARPS = MHD_SW_WARPS;  // warps (independent strips) per block
 constexpr int SW_PRE = 5;        // rows swept before the first output row of a strip
 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
-// Blocks of 4 warps resident per SM: stage 1 fits 3 (~170 registers), stage 2 carries more state
-// and is kept at 2 (~220 registers) to avoid spills.
+// Resident warps per SM: stage 1 runs 12 (168 registers, a little spilling), stage 2 carries
+// more state and runs 8 (~240 registers, no spilling); more resident warps cost more in spills
+// than they hide in latency.
 #ifndef MHD_SWEEP_MIN_BLOCKS_1
-#define MHD_SWEEP_MIN_BLOCKS_1 3
+#define MHD_SWEEP_MIN_BLOCKS_1 (12 / MHD_SW_WARPS)
 #endif
 #ifndef MHD_SWEEP_MIN_BLOCKS_2
-#define MHD_SWEEP_MIN_BLOCKS_2 2
+#define MHD_SWEEP_MIN_BLOCKS_2 (8 / MHD_SW_WARPS)
+#endif
+// Limited slopes formed once per cell in stage 2 (fewer instructions, no extra spilling there);
+// in stage 1 the extra live values spill and cost more than they save (measured on B200).
+#ifndef MHD_SWEEP_YREUSE_1
+#define MHD_SWEEP_YREUSE_1 0
+#endif
+#ifndef MHD_SWEEP_XREUSE_1
+#define MHD_SWEEP_XREUSE_1 0
+#endif
+#ifndef MHD_SWEEP_YREUSE_2
+#define MHD_SWEEP_YREUSE_2 1
+#endif
+#ifndef MHD_SWEEP_XREUSE_2
+#define MHD_SWEEP_XREUSE_2 1
 #endif
 
 // The sweep of one warp over work item w (strip w % strips_x, segment w / strips_x) of one grid.
@@ -53,6 +74,10 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
     const int r0 = sy * G.seg_h;
     const int r1 = min(r0 + G.seg_h, ny);
     if (r0 >= r1) return;
+    // limited slopes formed once per cell (y: carried to the next row; x: shared with the lane on
+    // the left), or per face as the reference writes them -- the same operands either way
+    constexpr bool kYReuse = (MODE == 1) ? MHD_SWEEP_YREUSE_1 : MHD_SWEEP_YREUSE_2;
+    constexpr bool kXReuse = (MODE == 1) ? MHD_SWEEP_XREUSE_1 : MHD_SWEEP_XREUSE_2;
     const int i = c0 - 2 + lane;
     const int iw = wrap(i, nx);
     const bool out_lane = lane >= 2 && lane < 2 + SW_OUT && i < nx;
@@ -69,6 +94,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
     // ---- windows (index 0 = oldest row)
     double Prho[4], Pvx[4], Pvy[4], Pp[4], Pbxc[4];  // rows c-1 .. c+2
     double Pbyc[3];                                   // rows c .. c+2
+    double Sy[5];                                     // y slopes of row c (when carried)
     double Wbx[5];                                    // bxf rows c-1 .. c+3 (B1 in stage 2)
     double Wby[5];                                    // byf rows c-1 .. c+3
     double bxr_prev = 0.0;                            // bxf(i+1) of row c+2 (cell-centred bx)
@@ -85,6 +111,8 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
     for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; pend[k] = 0.0; }
 #pragma unroll
     for (int k = 0; k < 3; ++k) Pbyc[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Sy[k] = 0.0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) { Wbx[k] = 0.0; Wby[k] = 0.0; fy_prev[k] = 0.0; }
 
@@ -186,41 +214,66 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
         //                  Wbx/Wby[0..4] = c-1 .. c+3
 
         // ---- YFACE: top face of (i, c); D = upper y-extrapolation of row c, U = lower of c+1
+        //      (MUSCL.hpp:26-47). With kYReuse each row's limited slope is formed once, when the
+        //      row is c+1, and carried to the next row for its upper extrapolation.
         Flux fy;
         {
             Prim Dn, Up;
-            Dn.rho = recon_hi(Prho[0], Prho[1], Prho[2]);
-            Dn.vx = recon_hi(Pvx[0], Pvx[1], Pvx[2]);
-            Dn.vy = recon_hi(Pvy[0], Pvy[1], Pvy[2]);
-            Dn.p = recon_hi(Pp[0], Pp[1], Pp[2]);
-            Dn.bx = recon_hi(Pbxc[0], Pbxc[1], Pbxc[2]);
-            Up.rho = recon_lo(Prho[1], Prho[2], Prho[3]);
-            Up.vx = recon_lo(Pvx[1], Pvx[2], Pvx[3]);
-            Up.vy = recon_lo(Pvy[1], Pvy[2], Pvy[3]);
-            Up.p = recon_lo(Pp[1], Pp[2], Pp[3]);
-            Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
+            if constexpr (kYReuse) {
+                const double s_rho = minmod(Prho[2] - Prho[1], Prho[3] - Prho[2]);
+                const double s_vx = minmod(Pvx[2] - Pvx[1], Pvx[3] - Pvx[2]);
+                const double s_vy = minmod(Pvy[2] - Pvy[1], Pvy[3] - Pvy[2]);
+                const double s_p = minmod(Pp[2] - Pp[1], Pp[3] - Pp[2]);
+                const double s_bx = minmod(Pbxc[2] - Pbxc[1], Pbxc[3] - Pbxc[2]);
+                Dn.rho = Prho[1] + 0.5 * Sy[0];
+                Dn.vx = Pvx[1] + 0.5 * Sy[1];
+                Dn.vy = Pvy[1] + 0.5 * Sy[2];
+                Dn.p = Pp[1] + 0.5 * Sy[3];
+                Dn.bx = Pbxc[1] + 0.5 * Sy[4];
+                Up.rho = Prho[2] - 0.5 * s_rho;
+                Up.vx = Pvx[2] - 0.5 * s_vx;
+                Up.vy = Pvy[2] - 0.5 * s_vy;
+                Up.p = Pp[2] - 0.5 * s_p;
+                Up.bx = Pbxc[2] - 0.5 * s_bx;
+                Sy[0] = s_rho; Sy[1] = s_vx; Sy[2] = s_vy; Sy[3] = s_p; Sy[4] = s_bx;
+            } else {
+                Dn.rho = recon_hi(Prho[0], Prho[1], Prho[2]);
+                Dn.vx = recon_hi(Pvx[0], Pvx[1], Pvx[2]);
+                Dn.vy = recon_hi(Pvy[0], Pvy[1], Pvy[2]);
+                Dn.p = recon_hi(Pp[0], Pp[1], Pp[2]);
+                Dn.bx = recon_hi(Pbxc[0], Pbxc[1], Pbxc[2]);
+                Up.rho = recon_lo(Prho[1], Prho[2], Prho[3]);
+                Up.vx = recon_lo(Pvx[1], Pvx[2], Pvx[3]);
+                Up.vy = recon_lo(Pvy[1], Pvy[2], Pvy[3]);
+                Up.p = recon_lo(Pp[1], Pp[2], Pp[3]);
+                Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
+            }
             Dn.by = Up.by = Wby[2];  // byf of row c+1
             fy = hll<1>(Dn, Up);
         }
-        // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of i+1
+        // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of
+        //      i+1. With kXReuse every lane limits its own column's slope once and hands its lower
+        //      extrapolation to the lane on its left; otherwise each lane forms both from shuffled
+        //      neighbours (no shuffle waits on arithmetic).
         Flux fx;
         {
-            const double r_m = shup(Prho[1], 1), r_p = shdn(Prho[1], 1), r_pp = shdn(Prho[1], 2);
-            const double u_m = shup(Pvx[1], 1), u_p = shdn(Pvx[1], 1), u_pp = shdn(Pvx[1], 2);
-            const double v_m = shup(Pvy[1], 1), v_p = shdn(Pvy[1], 1), v_pp = shdn(Pvy[1], 2);
-            const double p_m = shup(Pp[1], 1), p_p = shdn(Pp[1], 1), p_pp = shdn(Pp[1], 2);
-            const double b_m = shup(Pbyc[0], 1), b_p = shdn(Pbyc[0], 1), b_pp = shdn(Pbyc[0], 2);
             Prim L, R;
-            L.rho = recon_hi(r_m, Prho[1], r_p);
-            L.vx = recon_hi(u_m, Pvx[1], u_p);
-            L.vy = recon_hi(v_m, Pvy[1], v_p);
-            L.p = recon_hi(p_m, Pp[1], p_p);
-            L.by = recon_hi(b_m, Pbyc[0], b_p);
-            R.rho = recon_lo(Prho[1], r_p, r_pp);
-            R.vx = recon_lo(Pvx[1], u_p, u_pp);
-            R.vy = recon_lo(Pvy[1], v_p, v_pp);
-            R.p = recon_lo(Pp[1], p_p, p_pp);
-            R.by = recon_lo(Pbyc[0], b_p, b_pp);
+            auto xrecon = [&](double q, double& hi, double& lo_right) {
+                if constexpr (kXReuse) {
+                    const double s = minmod(q - shup(q, 1), shdn(q, 1) - q);
+                    hi = q + 0.5 * s;
+                    lo_right = shdn(q - 0.5 * s, 1);
+                } else {
+                    const double qm = shup(q, 1), qp = shdn(q, 1), qpp = shdn(q, 2);
+                    hi = recon_hi(qm, q, qp);
+                    lo_right = recon_lo(q, qp, qpp);
+                }
+            };
+            xrecon(Prho[1], L.rho, R.rho);
+            xrecon(Pvx[1], L.vx, R.vx);
+            xrecon(Pvy[1], L.vy, R.vy);
+            xrecon(Pp[1], L.p, R.p);
+            xrecon(Pbyc[0], L.by, R.by);
             L.bx = R.bx = shdn(Wbx[1], 1);  // bxf(i+1, c)
             fx = hll<0>(L, R);
         }
