@@ -72,7 +72,9 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    """nvidia-smi clock / throttle-reason samples while the timed region runs. The sampler is
+    running (first sample received) before the region starts and takes one more sample after it
+    ends, so the reported samples bracket the region even when it is shorter than the interval."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -81,7 +83,8 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.device_index = device_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (wall time, csv line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -91,16 +94,25 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            deadline = time.time() + 10.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.time()
         if self.proc is not None:
+            deadline = time.time() + 2.0
+            while time.time() < deadline and self.proc.poll() is None and \
+                    not any(t >= self.t1 for t, _ in self.lines):
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -110,7 +122,11 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples inside the region, plus the last one before and the first one after it
+        inside = [ln for t, ln in self.lines if self.t0 <= t <= self.t1]
+        before = [ln for t, ln in self.lines if t < self.t0][-1:]
+        after = [ln for t, ln in self.lines if t > self.t1][:1]
+        for ln in before + inside + after:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -125,7 +141,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_inside_region": len(inside)}
 
 
 def make_state(n):

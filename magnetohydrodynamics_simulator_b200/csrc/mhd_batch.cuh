@@ -148,7 +148,7 @@ enum CgInstStatus : int { kCgActive = 0, kCgConverged = 1, kCgZero = 2, kCgBreak
 struct CgBInst {
     double cx, cy, diag, invdiag;  // matrix of this solve
     double alpha, beta;            // CG step scalars
-    double bb, absNew, thr, rr;
+    double bb, absNew, thr, rr, pAp;
     long long products;
     int status;
     int pad;
@@ -183,11 +183,12 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     return g;
 }
 
-// One sweep phase over this warp's items. PH as in cg_sweep_segment; NV sums per instance.
-// Ends with the block's partials of every instance published in part_out.
+// One sweep over this warp's items: PH 0 the right-hand side (cg_rhs_segment), 1 the first
+// iteration, 2 a later one (cg_iter_segment); NV sums per instance. Ends with the block's partials
+// of every instance published in part_out.
 template <int PH, int NV>
 __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh,
-                                          double (*wsum)[CGB_MAX_INST][3], double* ring, int k,
+                                          double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
     constexpr int NW = CGS_NT / 32;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -209,15 +210,15 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         s.invdiag = sh[li].invdiag;
         s.alpha = sh[li].alpha;
         s.beta = sh[li].beta;
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if constexpr (PH == 0) {
-            cg_sweep_segment<0>(g, s, e.w, dir, nullptr, nullptr, g.r[0], nullptr, ring, acc);
+            cg_rhs_segment(g, s, e.w, dir, g.r[0], ring, acc);
         } else {
             const double* rk = odd ? g.r[1] : g.r[0];
             double* rk1 = odd ? g.r[0] : g.r[1];
             const double* pkm1 = odd ? g.p[0] : g.p[1];
             double* pk = odd ? g.p[1] : g.p[0];
-            cg_sweep_segment<PH>(g, s, e.w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<PH == 1>(g, s, e.w, dir, rk, pkm1, rk1, pk, ring, acc);
         }
 #pragma unroll
         for (int c = 0; c < NV; ++c)
@@ -257,7 +258,7 @@ static __global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
 k_cg_batch(CgBatchArgs a) {
     constexpr int NW = CGS_NT / 32;
     __shared__ CgBInst sh[CGB_MAX_INST];
-    __shared__ double wsum[NW][CGB_MAX_INST][3];
+    __shared__ double wsum[NW][CGB_MAX_INST][4];
     __shared__ int sflag;
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double cg_ring_mem[];
@@ -298,7 +299,7 @@ k_cg_batch(CgBatchArgs a) {
     }
     __syncthreads();
 
-    // ---- phase A0: r0 = b, p0 = b/d, |b|^2, r.z, p.Ap
+    // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
     cgb_phase<0, 3>(a, sh, wsum, ring, 0, dir, part(phase));
     if (!barrier_or_quit()) return;
     for (int li = wid; li < a.ninst; li += NW) {
@@ -313,7 +314,8 @@ k_cg_batch(CgBatchArgs a) {
             if (!isfinite(S.bb)) S.status = kCgBreakdown;
             else if (S.bb == 0.0 || S.bb < S.thr) S.status = kCgZero;
             else if (I.max_iters <= 0) S.status = kCgCapped;
-            S.alpha = (S.status == kCgActive) ? S.absNew / v[2] : 0.0;
+            S.pAp = v[2];
+            S.alpha = (S.status == kCgActive) ? S.absNew / S.pAp : 0.0;
         }
     }
     ++phase;
@@ -321,29 +323,15 @@ k_cg_batch(CgBatchArgs a) {
     __syncthreads();
 
     for (int k = 0;; ++k) {
-        if (k > 0) {
-            // ---- phase A_k: p_k, q = A p_k, p.q
-            cgb_phase<1, 1>(a, sh, wsum, ring, k, dir, part(phase));
-            if (!barrier_or_quit()) return;
-            for (int li = wid; li < a.ninst; li += NW) {
-                if (sh[li].status != kCgActive) continue;
-                double v[1];
-                cgb_span_sum<1>(part(phase), li, v);
-                if (lane == 0) sh[li].alpha = sh[li].absNew / v[0];
-            }
-            ++phase;
-            dir = -dir;
-            __syncthreads();
-        }
-        // ---- phase B_k: x, r_{k+1}, p_k; r.r, r.z
-        if (k == 0) cgb_phase<2, 2>(a, sh, wsum, ring, k, dir, part(phase));
-        else cgb_phase<3, 2>(a, sh, wsum, ring, k, dir, part(phase));
+        // ---- iteration k: p_k, q_k, x_{k+1}, r_{k+1}; r.r, r.z, z.Az, z.q_k
+        if (k == 0) cgb_phase<1, 4>(a, sh, wsum, ring, k, dir, part(phase));
+        else cgb_phase<2, 4>(a, sh, wsum, ring, k, dir, part(phase));
         if (!barrier_or_quit()) return;
         int active = 0;
         for (int li = wid; li < a.ninst; li += NW) {
             if (sh[li].status != kCgActive) continue;
-            double v[2];
-            cgb_span_sum<2>(part(phase), li, v);
+            double v[4];
+            cgb_span_sum<4>(part(phase), li, v);
             if (lane == 0) {
                 CgBInst& S = sh[li];
                 S.products += 1;
@@ -355,7 +343,13 @@ k_cg_batch(CgBatchArgs a) {
                     const double absOld = S.absNew;
                     S.absNew = v[1];
                     S.beta = S.absNew / absOld;
-                    active = 1;
+                    S.pAp = v[2] + 2.0 * S.beta * v[3] + S.beta * S.beta * S.pAp;
+                    if (!(S.pAp > 0.0)) {
+                        S.status = kCgBreakdown;
+                    } else {
+                        S.alpha = S.absNew / S.pAp;
+                        active = 1;
+                    }
                 }
             }
         }
@@ -372,9 +366,9 @@ k_cg_batch(CgBatchArgs a) {
         const BatchInst& I = a.insts[e.inst];
         const int nx = I.D.nx, ny = I.D.ny;
         const int sx = e.w % I.cg_strips_x, sy = e.w / I.cg_strips_x;
-        const int i = sx * CG_W - 1 + lane;
+        const int i = sx * CG_W - CG_HALO + lane;
         const int r0 = sy * I.cg_seg_h, r1 = min(r0 + I.cg_seg_h, ny);
-        if (lane >= 1 && lane <= CG_W && i < nx)
+        if (lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx)
             for (int j = r0; j < r1; ++j) I.x[(size_t)j * nx + i] = 0.0;
     }
     if (blockIdx.x == 0) {

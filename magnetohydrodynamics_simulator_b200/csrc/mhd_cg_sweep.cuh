@@ -1,20 +1,24 @@
 // Matrix-free conjugate gradient on the corner nodes as a persistent, cooperatively launched warp
 // sweep (reference: solvers.hpp:404-489 with Eigen's ConjugateGradient defaults -- x0 = 0, Jacobi
-// scaling by the constant diagonal, stop when |r|^2 < max(tol^2 |b|^2, DBL_MIN), at most max_iters
-// matrix-vector products).
+// scaling by the constant diagonal d, stop when |r|^2 < max(tol^2 |b|^2, DBL_MIN), at most
+// max_iters matrix-vector products).
 //
-// Each warp owns a strip of 30 corner columns and a segment of rows; its 32 lanes hold the strip and
-// one halo column on each side. The 5-point product is formed from a 3-row register window
-// (y neighbours) and shuffles (x neighbours); rows are prefetched 8 deep into shared memory with
-// cp.async. Per iteration:
-//   phase A: p_k = r_k/d + beta p_{k-1} (rows j-1..j+1), q = A p_k, partial p.q          reads r, p
-//   phase B: the same p_k and q; x += alpha p_k; r_{k+1} = r_k - alpha q; partial r.r, r.z;
-//            writes x, r_{k+1}, p_k                                              reads r, p, x
-// r and p are double-buffered (a phase reads one copy's halo and writes the other). Phases A and B
-// sweep their rows in opposite directions, so each phase starts on the rows the previous phase
-// touched last (still in L2). Partial sums are reduced in a fixed order (lane tree, warp order,
-// block order), identically in every block, so every block takes the same decisions and the
-// result is deterministic. Grid-wide waits spin with a wall-clock limit (grid_barrier).
+// Each warp owns a strip of CG_W = 28 corner columns and a segment of rows; its 32 lanes hold the
+// strip and two halo columns on each side. 5-point products are formed from register windows over
+// rows (y neighbours) and shuffles (x neighbours); rows are prefetched into a per-warp shared-memory
+// ring with cp.async. One sweep per iteration (after the right-hand-side sweep):
+//   p_k = z_k + beta_k p_{k-1}; q_k = A p_k; x_{k+1} = x_k + alpha_k p_k;
+//   r_{k+1} = r_k - alpha_k q_k; z_{k+1} = r_{k+1}/d; partials r.r, r.z, z.Az, z.q_k
+//   (reads r_k, p_{k-1}, x_k; writes x_{k+1}, r_{k+1}, p_k)
+// The next step length needs p_{k+1}.A p_{k+1}; with p_{k+1} = z_{k+1} + beta p_k and A symmetric
+// it is z.Az + 2 beta z.q_k + beta^2 p_k.q_k, all known after this sweep, so no second sweep over
+// the vectors is needed. In exact arithmetic these are Eigen's iterates; the step lengths differ
+// from a two-sweep CG by rounding only. r and p are double-buffered (a sweep reads one copy's halo
+// rows and writes the other). Consecutive sweeps run their rows in opposite directions, so each
+// starts on the rows the previous one touched last (still in L2). Partial sums are reduced in a
+// fixed order (lane tree, warp order, block order), identically in every block, so every block
+// takes the same decisions and the result is deterministic. Grid-wide waits spin with a
+// wall-clock limit (grid_barrier).
 #pragma once
 
 #include "mhd_kernels.cuh"
@@ -98,93 +102,64 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Per-warp ring of prefetched rows in shared memory. A slot holds, for one row, up to 3 vectors at
-// the warp's 32 columns (lane l's element at v*32 + l) and, in the right-hand-side phase, lane 0's
-// extra face value at 96. Every lane reads back only what it copied itself, so
-// cp.async.wait_group alone orders the accesses.
-constexpr int CG_RING = 8;    // rows in flight per warp (power of two)
-constexpr int CG_SLOT = 104;  // doubles per slot (832 bytes, 16-byte multiple)
-constexpr int CG_W = 30;      // output columns per warp: lanes 1..30; lanes 0 and 31 are halo
+// the warp's 32 columns (lane l's element at v*32 + l). Every lane reads back only what it copied
+// itself, so cp.async.wait_group alone orders the accesses.
+constexpr int CG_RING = 8;    // row slots per warp (power of two)
+constexpr int CG_SLOT = 96;   // doubles per slot (768 bytes, 16-byte multiple)
+constexpr int CG_HALO = 2;    // halo lanes on each side
+constexpr int CG_W = 32 - 2 * CG_HALO;  // output columns per warp: lanes 2..29
 constexpr size_t kCgRingBytes = (size_t)(CGS_NT / 32) * CG_RING * CG_SLOT * sizeof(double);
 
-// One sweep over the warp's segment. PH: 0 = A0 (right-hand side, r0 = b, p0 = b/d),
-// 1 = A_k (k >= 1), 2 = B_0, 3 = B_k. acc[] receives this lane's partial sums. Lane l holds corner
-// column c0 - 1 + l; every lane does the same work and lanes 1..30 own the results. Row k of the
-// sweep (k = 0 is the row behind the first one) is copied into slot k % CG_RING, CG_RING - 3 rows
-// before it enters the 3-row stencil window.
-template <int PH>
-__device__ __forceinline__ void cg_sweep_segment(const CgSweepArgs& a, const CgScal& s, int w,
-                                                 int dir, const double* rk, const double* pkm1,
-                                                 double* rk1, double* pk, double* ring,
-                                                 double (&acc)[3]) {
+// Right-hand-side sweep over the warp's segment: r0 = b = eta J_z(B) (written to r0), p0 = z0 = b/d,
+// partials |b|^2, b.z0, p0.A p0 (acc[0..2]). Lane l holds corner column c0 - 2 + l; lanes 2..29
+// own the results. Sweep row k (k = 0 is the row behind the first one) sits in slot k % CG_RING.
+__device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgScal& s, int w, int dir,
+                                               double* r0, double* ring, double (&acc)[4]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
     const int sx = w % a.strips_x, sy = w / a.strips_x;
     const int c0 = sx * CG_W;
-    const int r0 = sy * a.seg_h;
-    const int r1 = min(r0 + a.seg_h, ny);
-    if (r0 >= r1) return;
-    const int i = c0 - 1 + lane;
-    const bool owner = lane >= 1 && lane <= CG_W && i < nx;
+    const int r0w = sy * a.seg_h;
+    const int r1w = min(r0w + a.seg_h, ny);
+    if (r0w >= r1w) return;
+    const int i = c0 - CG_HALO + lane;
+    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
     const int iw = wrap(i, nx);
-    const int iwl = wrap(i - 1, nx);  // lane 0's left neighbour (right-hand-side phase)
     const double idx = 1.0 / a.D.dx, idy = 1.0 / a.D.dy;
-    const int jfirst = (dir > 0) ? r0 : r1 - 1;
-    const int jlast = (dir > 0) ? r1 - 1 : r0;
-    const int nrows = r1 - r0;
+    const int jfirst = (dir > 0) ? r0w : r1w - 1;
+    const int nrows = r1w - r0w;
     auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
     auto slot = [&](int k) { return ring + (unsigned)(k & (CG_RING - 1)) * CG_SLOT; };
-
     // copy sweep row k (grid row jfirst + (k-1) dir) into its slot and commit one group
     auto issue = [&](int k) {
         if (k <= nrows + 1) {
             double* sl = slot(k);
             const int j = jfirst + (k - 1) * dir;
             const size_t rp = rowp(j);
-            if constexpr (PH == 0) {
-                const size_t rb = rowp(j - 1);
-                cp_async8(&sl[lane], &a.byf[rp + iw]);
-                cp_async8(&sl[32 + lane], &a.bxf[rp + iw]);
-                cp_async8(&sl[64 + lane], &a.bxf[rb + iw]);
-                if (lane == 0) cp_async8(&sl[96], &a.byf[rp + iwl]);
-            } else {
-                cp_async8(&sl[lane], &rk[rp + iw]);
-                if constexpr (PH != 2) cp_async8(&sl[32 + lane], &pkm1[rp + iw]);
-                if constexpr (PH == 3) cp_async8(&sl[64 + lane], &a.x[rp + iw]);
-            }
+            const size_t rb = rowp(j - 1);
+            cp_async8(&sl[lane], &a.byf[rp + iw]);
+            cp_async8(&sl[32 + lane], &a.bxf[rp + iw]);
+            cp_async8(&sl[64 + lane], &a.bxf[rb + iw]);
         }
         cp_async_commit();
     };
-    // p, r and x at this lane's column of sweep row k, from its slot
-    auto compute = [&](int k, double& p_own, double& r_own, double& x_own) {
+    // b and p = b/d of sweep row k (lane 0's b is never used: its left neighbour is not loaded)
+    auto compute = [&](int k, double& p_own, double& r_own) {
         const double* sl = slot(k);
-        if constexpr (PH == 0) {
-            const double by = sl[lane];
-            double byl = __shfl_up_sync(0xffffffffu, by, 1);
-            if (lane == 0) byl = sl[96];
-            const double b = corner_rhs(a.D, idx, idy, by, byl, sl[32 + lane], sl[64 + lane]);
-            r_own = b;
-            p_own = __dmul_rn(s.invdiag, b);
-        } else if constexpr (PH == 2) {
-            r_own = sl[lane];
-            p_own = __dmul_rn(s.invdiag, r_own);
-        } else {
-            r_own = sl[lane];
-            p_own = cg_dir(s.invdiag, r_own, s.beta, sl[32 + lane]);
-        }
-        if constexpr (PH == 3) x_own = sl[64 + lane];
-        else x_own = 0.0;
+        const double by = sl[lane];
+        const double byl = __shfl_up_sync(0xffffffffu, by, 1);
+        const double b = corner_rhs(a.D, idx, idy, by, byl, sl[32 + lane], sl[64 + lane]);
+        r_own = b;
+        p_own = __dmul_rn(s.invdiag, b);
     };
-
 #pragma unroll
     for (int k = 0; k < CG_RING; ++k) issue(k);
     cp_async_wait<CG_RING - 3>();  // rows 0, 1, 2 have landed
-    // window: p at rows j - dir (behind), j (current), j + dir (ahead)
-    double pb, pc, pa, rc, ra, xc, xa, dr, dx_;
-    compute(0, pb, dr, dx_);
-    compute(1, pc, rc, xc);
-    compute(2, pa, ra, xa);
+    double pb, pc, pa, rc, ra, dr;
+    compute(0, pb, dr);
+    compute(1, pc, rc);
+    compute(2, pa, ra);
     (void)dr;
-    (void)dx_;
     size_t g = (size_t)jfirst * nx + i;  // owner lanes' element of the current row
     const long long gstep = (long long)dir * nx;
     for (int t = 0;; ++t) {
@@ -195,40 +170,115 @@ __device__ __forceinline__ void cg_sweep_segment(const CgSweepArgs& a, const CgS
         const double p_hi = (dir > 0) ? pa : pb;  // row j+1
         const double q = stencil(p_lo, pl, pc, pr, p_hi, s);
         if (owner) {
-            if constexpr (PH == 0) {
-                acc[0] += rc * rc;
-                acc[1] += rc * pc;
-                acc[2] += pc * q;
-                rk1[g] = rc;  // r0 = b
-            } else if constexpr (PH == 1) {
-                acc[0] += pc * q;
-            } else {
-                const double xv = (PH == 2) ? s.alpha * pc : xc + s.alpha * pc;
-                const double rnew = rc - s.alpha * q;
-                a.x[g] = xv;
-                rk1[g] = rnew;
-                pk[g] = pc;
-                acc[0] += rnew * rnew;
-                acc[1] += rnew * __dmul_rn(s.invdiag, rnew);
-            }
+            acc[0] += rc * rc;
+            acc[1] += rc * pc;
+            acc[2] += pc * q;
+            r0[g] = rc;
         }
         if (t == nrows - 1) break;
         g += gstep;
         // row t+3 (j + 2dir) enters the window
         cp_async_wait<CG_RING - 3>();
-        double pn, rn, xn;
-        compute(t + 3, pn, rn, xn);
+        double pn, rn;
+        compute(t + 3, pn, rn);
         pb = pc; pc = pa; pa = pn;
         rc = ra; ra = rn;
-        xc = xa; xa = xn;
     }
-    (void)jlast;
+    cp_async_wait<0>();  // leave no copy in flight into the ring
+}
+
+// One CG iteration k over the warp's segment (the sweep of the header comment). FIRST: k = 0,
+// p_0 = z_0 and x_0 = 0 (p_{-1} and x are not read). acc[0..3] receive r.r, r.z, z.Az, z.q_k of
+// the owned cells. Sweep row t holds grid row jfirst + (t - 2) dir, t = 0 .. nrows + 3; at sweep
+// row t the warp forms p_k of row t, q_k, r_{k+1}, z_{k+1} of row t-1 and A z_{k+1} and the outputs
+// of row t-2. Row t is copied into slot t % CG_RING by the end of sweep row t - 6.
+template <bool FIRST>
+__device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int w, int dir,
+                                                const double* rk, const double* pkm1, double* rk1,
+                                                double* pk, double* ring, double (&acc)[4]) {
+    const int lane = threadIdx.x & 31;
+    const int nx = a.D.nx, ny = a.D.ny;
+    const int sx = w % a.strips_x, sy = w / a.strips_x;
+    const int c0 = sx * CG_W;
+    const int r0w = sy * a.seg_h;
+    const int r1w = min(r0w + a.seg_h, ny);
+    if (r0w >= r1w) return;
+    const int i = c0 - CG_HALO + lane;
+    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
+    const int iw = wrap(i, nx);
+    const int jfirst = (dir > 0) ? r0w : r1w - 1;
+    const int total = (r1w - r0w) + 4;
+    auto slot = [&](int t) { return ring + (unsigned)(t & (CG_RING - 1)) * CG_SLOT; };
+    auto issue = [&](int t) {
+        if (t < total) {
+            double* sl = slot(t);
+            const size_t rp = (size_t)wrap(jfirst + (t - 2) * dir, ny) * nx + iw;
+            cp_async8(&sl[lane], &rk[rp]);
+            if constexpr (!FIRST) {
+                cp_async8(&sl[32 + lane], &pkm1[rp]);
+                cp_async8(&sl[64 + lane], &a.x[rp]);
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < CG_RING - 2; ++t) issue(t);
+    double p_a = 0.0, p_b = 0.0;       // p_k of rows t-2, t-1
+    double q_o = 0.0;                  // q_k of row t-2
+    double r_o = 0.0, z_o = 0.0;       // r_{k+1}, z_{k+1} of row t-2
+    double z_a = 0.0;                  // z_{k+1} of row t-3
+    size_t g = (size_t)jfirst * nx + i;  // owner lanes' element of the output row
+    const long long gstep = (long long)dir * nx;
+    for (int t = 0; t < total; ++t) {
+        cp_async_wait<CG_RING - 3>();  // row t has landed (rows t+1 .. t+5 may be in flight)
+        const double* sl = slot(t);
+        double p_c;
+        if constexpr (FIRST) p_c = __dmul_rn(s.invdiag, sl[lane]);
+        else p_c = cg_dir(s.invdiag, sl[lane], s.beta, sl[32 + lane]);
+        double q_b = 0.0, r_b = 0.0, z_b = 0.0;
+        if (t >= 2) {
+            // q_k, r_{k+1}, z_{k+1} of row t-1
+            const double pl = __shfl_up_sync(0xffffffffu, p_b, 1);
+            const double pr = __shfl_down_sync(0xffffffffu, p_b, 1);
+            const double p_lo = (dir > 0) ? p_a : p_c;
+            const double p_hi = (dir > 0) ? p_c : p_a;
+            q_b = stencil(p_lo, pl, p_b, pr, p_hi, s);
+            r_b = slot(t - 1)[lane] - s.alpha * q_b;
+            z_b = __dmul_rn(s.invdiag, r_b);
+        }
+        if (t >= 4) {
+            // A z_{k+1} and the outputs of row t-2
+            const double zl = __shfl_up_sync(0xffffffffu, z_o, 1);
+            const double zr = __shfl_down_sync(0xffffffffu, z_o, 1);
+            const double z_lo = (dir > 0) ? z_a : z_b;
+            const double z_hi = (dir > 0) ? z_b : z_a;
+            const double az = stencil(z_lo, zl, z_o, zr, z_hi, s);
+            if (owner) {
+                double xv;
+                if constexpr (FIRST) xv = s.alpha * p_a;
+                else xv = slot(t - 2)[64 + lane] + s.alpha * p_a;
+                a.x[g] = xv;
+                rk1[g] = r_o;
+                pk[g] = p_a;
+                acc[0] += r_o * r_o;
+                acc[1] += r_o * z_o;
+                acc[2] += z_o * az;
+                acc[3] += z_o * q_o;
+            }
+            g += gstep;
+        }
+        p_a = p_b; p_b = p_c;
+        q_o = q_b;
+        z_a = z_o;
+        r_o = r_b; z_o = z_b;
+        issue(t + CG_RING - 2);  // into the slot of row t-2, no longer read
+    }
     cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
 // Block-reduce NV partial sums (fixed order) and publish them in this block's slot.
 template <int NV>
-__device__ __forceinline__ void publish(double (&acc)[3], double* slot, double* red) {
+__device__ __forceinline__ void publish(double (&acc)[4], double* slot, double* red) {
 #pragma unroll
     for (int k = 0; k < NV; ++k)
         for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
@@ -288,21 +338,21 @@ k_cg_sweep(CgSweepArgs a) {
         return false;
     };
 
-    // ---- phase A0
+    // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
     {
-        double acc[3] = {0.0, 0.0, 0.0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         for (int w = wfirst; w < a.nwarps; w += wstride)
-            cg_sweep_segment<0>(a, s, w, dir, nullptr, nullptr, a.r[0], nullptr, ring, acc);
+            cg_rhs_segment(a, s, w, dir, a.r[0], ring, acc);
         publish<3>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
     }
     if (!barrier_or_quit()) return;
-    double sums[3];
+    double sums[4];
     reduce_partials<3>(part(phase), G, sums, scal);
     ++phase;
     dir = -dir;
     const double bb = sums[0];
     double absNew = sums[1];
-    double pq = sums[2];
+    double pAp = sums[2];
     const double threshold = smax(a.tol * a.tol * bb, 2.2250738585072014e-308);
     long long products = 0;
     const bool zero_solution = (bb == 0.0) || (bb < threshold);
@@ -311,46 +361,38 @@ k_cg_sweep(CgSweepArgs a) {
     double rr_final = 0.0;
 
     if (!zero_solution && !breakdown) {
+        s.alpha = absNew / pAp;
         for (long long k = 0; k < a.max_iters; ++k) {
             const bool odd = (k & 1) != 0;
             const double* rk = odd ? a.r[1] : a.r[0];
             double* rk1 = odd ? a.r[0] : a.r[1];
             const double* pkm1 = odd ? a.p[0] : a.p[1];
             double* pk = odd ? a.p[1] : a.p[0];
-            if (k > 0) {
-                double acc[3] = {0.0, 0.0, 0.0};
-                for (int w = wfirst; w < a.nwarps; w += wstride)
-                    cg_sweep_segment<1>(a, s, w, dir, rk, pkm1, nullptr, nullptr, ring, acc);
-                publish<1>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
-                if (!barrier_or_quit()) return;
-                double v[1];
-                reduce_partials<1>(part(phase), G, v, scal);
-                ++phase;
-                dir = -dir;
-                pq = v[0];
-            }
-            s.alpha = absNew / pq;
             {
-                double acc[3] = {0.0, 0.0, 0.0};
+                double acc[4] = {0.0, 0.0, 0.0, 0.0};
                 for (int w = wfirst; w < a.nwarps; w += wstride) {
-                    if (k == 0) cg_sweep_segment<2>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
-                    else cg_sweep_segment<3>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    if (k == 0) cg_iter_segment<true>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    else cg_iter_segment<false>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
                 }
-                publish<2>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
+                publish<4>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
             }
             if (!barrier_or_quit()) return;
-            double v2[2];
-            reduce_partials<2>(part(phase), G, v2, scal);
+            double v[4];
+            reduce_partials<4>(part(phase), G, v, scal);
             ++phase;
             dir = -dir;
             ++products;
-            const double rr = v2[0];
+            const double rr = v[0];
             rr_final = rr;
             if (!isfinite(rr) || !isfinite(s.alpha)) { breakdown = true; break; }
             if (rr < threshold) { converged = true; break; }
+            // next step: beta = r.z / r.z_old, p.Ap = z.Az + 2 beta z.q + beta^2 p.Ap
             const double absOld = absNew;
-            absNew = v2[1];
+            absNew = v[1];
             s.beta = absNew / absOld;
+            pAp = v[2] + 2.0 * s.beta * v[3] + s.beta * s.beta * pAp;
+            if (!(pAp > 0.0)) { breakdown = true; break; }
+            s.alpha = absNew / pAp;
         }
     }
     if (zero_solution || breakdown) {
