@@ -357,7 +357,8 @@ def run_gpu_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [n, n], "eta": ETA, "cfl": COURANT,
+        "config": {"workload": WORKLOAD if n == N_GRID else f"orszag_tang_{n}x{n}_eta1e-4_cfl0.4",
+                   "grid": [n, n], "eta": ETA, "cfl": COURANT,
                    "parallelism": f"replicas{world}", "l2": "inputs exceed L2 (805 MB state)",
                    "cg_products_last_step": [k1, k2]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
