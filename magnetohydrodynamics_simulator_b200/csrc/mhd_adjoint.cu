@@ -176,12 +176,12 @@ mhd_status solve(mhd_adjoint* a, const double* bxf, const double* byf, double rh
 mhd_status forward_step(mhd_adjoint* a, const double* const U[6], const Slot& sl, double* x1,
                         double* x2, bool do_solve) {
     const Domain& D = a->dom;
-    k_stage_sweep<1><<<a->st_blocks[0], 32 * SW_WARPS, 0, a->stream>>>(
+    k_stage_sweep<1><<<a->st_blocks[0], 32 * SW_WARPS, sweep_smem_bytes(1), a->stream>>>(
         D, a->coeffs, cplanes6(U), nullptr, planes6(sl.T), planes6(sl.A), a->sg[0]);
     MHD_TRY(cudaGetLastError());
     mhd_status s;
     if (do_solve && (s = solve(a, sl.T[4], sl.T[5], a->eta, x1)) != MHD_OK) return s;
-    k_stage_sweep<2><<<a->st_blocks[1], 32 * SW_WARPS, 0, a->stream>>>(
+    k_stage_sweep<2><<<a->st_blocks[1], 32 * SW_WARPS, sweep_smem_bytes(2), a->stream>>>(
         D, a->coeffs, cplanes6(sl.T), x1, planes6(sl.T), planes6(sl.A), a->sg[1]);
     MHD_TRY(cudaGetLastError());
     if (do_solve && (s = solve(a, sl.A[4], sl.A[5], a->eta, x2)) != MHD_OK) return s;
@@ -383,8 +383,8 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
     for (int mode = 0; mode < 2; ++mode) {
         int occ = 0;
         const cudaError_t e = mode == 0
-            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<1>, 32 * SW_WARPS, 0)
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, 0);
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<1>, 32 * SW_WARPS, sweep_smem_bytes(1))
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, sweep_smem_bytes(2));
         if (e != cudaSuccess || occ < 1) return fail(MHD_ERR_CUDA);
         const long long resident = (long long)occ * a->num_sms * SW_WARPS;
         SweepGeom& g = a->sg[mode];

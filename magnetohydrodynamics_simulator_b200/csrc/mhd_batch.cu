@@ -223,14 +223,14 @@ mhd_status enqueue_step(mhd_batch* b, const double* dt_in, double dt_fixed, int 
         b->rec_cap, b->queues, kQueues, b->syncs, 2 * b->nchunks);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[0], b->stream));
-    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, 0, b->stream>>>(I, b->d_items,
+    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, sweep_smem_bytes(1), b->stream>>>(I, b->d_items,
                                                                         b->n_stage_items, b->queues);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[1], b->stream));
     mhd_status s = launch_cg_chunks(b, I, 0, record);
     if (s != MHD_OK) return s;
     if (ev) MHD_TRY(cudaEventRecord(ev[2], b->stream));
-    k_stage_batch<2><<<b->stage_grid[1], 32 * SW_WARPS, 0, b->stream>>>(
+    k_stage_batch<2><<<b->stage_grid[1], 32 * SW_WARPS, sweep_smem_bytes(2), b->stream>>>(
         I, b->d_items, b->n_stage_items, b->queues + 1);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[3], b->stream));
@@ -328,9 +328,9 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
         b->own_stream = true;
     }
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->stage_occ[0], k_stage_batch<1>,
-                                                      32 * SW_WARPS, 0) != cudaSuccess ||
+                                                      32 * SW_WARPS, sweep_smem_bytes(1)) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->stage_occ[1], k_stage_batch<2>,
-                                                      32 * SW_WARPS, 0) != cudaSuccess ||
+                                                      32 * SW_WARPS, sweep_smem_bytes(2)) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->fin_occ, k_finalize_batch, 32 * FS_WARPS,
                                                       0) != cudaSuccess ||
         cudaFuncSetAttribute(k_cg_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -92,6 +92,12 @@ template <int MODE>
 __global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
 k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ items, int nitems,
               int* queue) {
+#if defined(__CUDA_ARCH__)
+    extern __shared__ __align__(16) double sw_ring_mem[];
+#else
+    static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];
+#endif
+    double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
@@ -107,7 +113,7 @@ k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ 
         }
         const Domain D = I.D;
         const SweepGeom G = I.sg;
-        stage_sweep_warp<MODE>(D, I.C, in, (MODE == 1) ? nullptr : I.x, oa, ob, G, e.w);
+        stage_sweep_warp<MODE>(D, I.C, in, (MODE == 1) ? nullptr : I.x, oa, ob, G, e.w, ring);
     }
 }
 

@@ -165,14 +165,14 @@ mhd_status mark(mhd_context* c) {
 // The kernels of one step after the coefficients kernel.
 mhd_status enqueue_step_body(mhd_context* c, long long* prods_out) {
     MHD_MARK(c);
-    k_stage_sweep<1><<<c->st_blocks[0], 32 * SW_WARPS, 0, c->stream>>>(
+    k_stage_sweep<1><<<c->st_blocks[0], 32 * SW_WARPS, sweep_smem_bytes(1), c->stream>>>(
         c->dom, c->coeffs, cplanes(c->S), nullptr, planes(c->T), planes(c->A), c->sg[0]);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
     mhd_status s = launch_cg(c, c->T[4], c->T[5], 0, prods_out);
     if (s != MHD_OK) return s;
     MHD_MARK(c);
-    k_stage_sweep<2><<<c->st_blocks[1], 32 * SW_WARPS, 0, c->stream>>>(
+    k_stage_sweep<2><<<c->st_blocks[1], 32 * SW_WARPS, sweep_smem_bytes(2), c->stream>>>(
         c->dom, c->coeffs, cplanes(c->T), c->x, planes(c->T), planes(c->A), c->sg[1]);
     MHD_TRY(cudaGetLastError());
     MHD_MARK(c);
@@ -330,11 +330,18 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
     }
     // Explicit-stage sweep: strips of SW_OUT columns, each split into row segments so that the
     // warps of one wave cover the grid.
+    {
+        const int carve = env_int("MHD_B200_SWEEP_CARVEOUT", -1);
+        if (carve >= 0) {
+            cudaFuncSetAttribute(k_stage_sweep<1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+            cudaFuncSetAttribute(k_stage_sweep<2>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        }
+    }
     for (int mode = 0; mode < 2; ++mode) {
         int occ = 0;
         const cudaError_t e = mode == 0
-            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<1>, 32 * SW_WARPS, 0)
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, 0);
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<1>, 32 * SW_WARPS, sweep_smem_bytes(1))
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_sweep<2>, 32 * SW_WARPS, sweep_smem_bytes(2));
         if (e != cudaSuccess || occ < 1) return fail(MHD_ERR_CUDA);
         const long long resident = (long long)occ * c->num_sms * SW_WARPS;
         SweepGeom& g = c->sg[mode];
@@ -344,6 +351,9 @@ mhd_status mhd_create(const mhd_params* p, void* stream, mhd_context** out) {
         g.segs_y = (p->ny + g.seg_h - 1) / g.seg_h;
         g.nwarps = g.strips_x * g.segs_y;
         c->st_blocks[mode] = (g.nwarps + SW_WARPS - 1) / SW_WARPS;
+        if (getenv("MHD_B200_VERBOSE"))
+            fprintf(stderr, "mhd_b200: stage %d: %d blocks/SM, rows per warp %d, %d warps\n", mode + 1,
+                    occ, g.seg_h, g.nwarps);
     }
     {
         int occ = 0;

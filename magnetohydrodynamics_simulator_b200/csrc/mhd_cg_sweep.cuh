@@ -80,27 +80,6 @@ __device__ __forceinline__ double corner_rhs(const Domain& D, double idx, double
     return D.eta * (dBy_dx - dBx_dy);
 }
 
-// Asynchronous 8-byte global -> shared copy (cp.async), its commit and its wait.
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
-#if defined(__CUDA_ARCH__)
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-#else
-    *smem = *gmem;  // host compilation of the kernel sources: a plain copy
-#endif
-}
-__device__ __forceinline__ void cp_async_commit() {
-#if defined(__CUDA_ARCH__)
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-#endif
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-#if defined(__CUDA_ARCH__)
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-#endif
-}
-
 // Per-warp ring of prefetched rows in shared memory. A slot holds, for one row, up to 3 vectors at
 // the warp's 32 columns (lane l's element at v*32 + l). Every lane reads back only what it copied
 // itself, so cp.async.wait_group alone orders the accesses.

@@ -110,6 +110,27 @@ __device__ __forceinline__ unsigned long long global_timer_ns() {
 #endif
 }
 
+// Asynchronous 8-byte global -> shared copy (cp.async), its commit and its wait.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+#if defined(__CUDA_ARCH__)
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+#else
+    *smem = *gmem;  // host compilation of the kernel sources: a plain copy
+#endif
+}
+__device__ __forceinline__ void cp_async_commit() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+#endif
+}
+
 template <int NT>
 __device__ __forceinline__ double block_max(double v, double* red) {
     for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));

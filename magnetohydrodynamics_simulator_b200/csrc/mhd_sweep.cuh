@@ -4,10 +4,13 @@
 // i = c0 - 2 + l (the 2-cell MUSCL halo on each side is covered by lanes 0-1 and 30-31). The warp
 // sweeps the rows of its strip upwards; every quantity that the reference computes on whole
 // planes (solvers.hpp:393-402) is computed here one row at a time, with
-//   * the y-direction stencil (rows c-1 .. c+2) held in registers as a rolling window,
-//   * the x-direction stencil (columns i-1 .. i+2) read from neighbouring lanes by shuffles,
-//   * the next row's loads issued one iteration before they are used.
-// No shared memory and no block-level barrier is used in the sweep.
+//   * the input rows (and stage 2's E1) copied by cp.async into a per-warp ring of 8 row slots in
+//     shared memory, four rows ahead of their first use, so that no register holds raw input,
+//   * the y-direction stencil of the primitives (rows c-1 .. c+2) held in registers as a rolling
+//     window,
+//   * the x-direction stencil (columns i-1 .. i+2) read from neighbouring lanes by shuffles.
+// Every lane reads back only the ring entries it copied or wrote itself (x neighbours come by
+// shuffle), so cp.async.wait_group alone orders the accesses; there is no block-level barrier.
 //
 // Pipeline at sweep row c (all rows periodic):
 //   arrive  row c+3 of the input (stage 2: B1 = U1*_B + dt*g*rate(E1) of row c+3)
@@ -25,6 +28,13 @@
 namespace mhd {
 
 constexpr int SW_OUT = 28;       // output columns per warp
+// The input rows are kept in a per-warp shared-memory ring filled by cp.async, not in registers.
+// Slot layout: rho, mx, my, E, bxf, byf of the warp's 32 columns at q*32 + lane, lane 31's
+// right-hand neighbour bxf(i+1) at 192; stage 2 adds E1 at SW_E1 + lane and lane 31's right-hand
+// E1 at SW_E1 + 32.
+constexpr int SW_RING = 8;       // row slots per warp (power of two): rows c-1 .. c+6
+constexpr int SW_E1 = 196;       // offset of E1 in a stage-2 slot
+constexpr int SW_SLOT = 230;     // doubles per slot (1840 bytes, 16-byte multiple)
 // One warp (an independent strip segment) per block: blocks retire warp by warp, so the tail of
 // a launch and the persistent batch kernels balance at warp granularity (measured on B200 against
 // 4-warp blocks at the same registers: stage 1 1.29 -> 1.25 ms, stage 2 1.24 -> 1.15 ms at 4096^2).
@@ -37,14 +47,14 @@ constexpr int SW_PRE = 5;        // rows swept before the first output row of a 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
-// Resident warps per SM: stage 1 runs 12 (168 registers, a little spilling), stage 2 carries
-// more state and runs 8 (~240 registers, no spilling); more resident warps cost more in spills
-// than they hide in latency.
+// Resident warps per SM: 12 for both stages, i.e. 3 per SM sub-partition, whose 16K registers
+// allow at most 168 per thread (the next step, 16 warps, allows 128 and spills). With the input
+// rows in the shared-memory ring both stages fit 168 registers without spilling.
 #ifndef MHD_SWEEP_MIN_BLOCKS_1
 #define MHD_SWEEP_MIN_BLOCKS_1 (12 / MHD_SW_WARPS)
 #endif
 #ifndef MHD_SWEEP_MIN_BLOCKS_2
-#define MHD_SWEEP_MIN_BLOCKS_2 (8 / MHD_SW_WARPS)
+#define MHD_SWEEP_MIN_BLOCKS_2 (12 / MHD_SW_WARPS)
 #endif
 // Limited slopes formed once per cell in stage 2 (fewer instructions, no extra spilling there);
 // in stage 1 the extra live values spill and cost more than they save (measured on B200).
@@ -66,7 +76,7 @@ template <int MODE>
 __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
                                                  const CPlanes& in, const double* __restrict__ xsolve,
                                                  const Planes& outA, const Planes& outB,
-                                                 const SweepGeom& G, int w) {
+                                                 const SweepGeom& G, int w, double* ring) {
     const int lane = threadIdx.x & 31;
     const int nx = D.nx, ny = D.ny;
     const int sx = w % G.strips_x, sy = w / G.strips_x;
@@ -95,114 +105,87 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
     double Prho[4], Pvx[4], Pvy[4], Pp[4], Pbxc[4];  // rows c-1 .. c+2
     double Pbyc[3];                                   // rows c .. c+2
     double Sy[5];                                     // y slopes of row c (when carried)
-    double Wbx[5];                                    // bxf rows c-1 .. c+3 (B1 in stage 2)
-    double Wby[5];                                    // byf rows c-1 .. c+3
-    double bxr_prev = 0.0;                            // bxf(i+1) of row c+2 (cell-centred bx)
-    double pend[4];                                   // conserved hydro of row c+2
-    double arr[6];                                    // arriving input row (c+3)
-    double arr_bxr = 0.0;                             // lane 31: bxf one column to the right
-    double ax_cur = 0.0, ax_nxt = 0.0;                // stage 2: E1 rows c+3, c+4
-    double axr_cur = 0.0, axr_nxt = 0.0;              // lane 31: E1 one column to the right
     double fy_prev[5];                                // y-face flux of row c-1
     double fxbt_prev = 0.0, ez_prev = 0.0, jz_prev = 0.0;
-    double accH[4] = {0.0, 0.0, 0.0, 0.0};            // stage 2: accumulator hydro of row c
-    double accB[2] = {0.0, 0.0};                      // stage 2: accumulator faces of row c-1
 #pragma unroll
-    for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; pend[k] = 0.0; }
+    for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; }
 #pragma unroll
     for (int k = 0; k < 3; ++k) Pbyc[k] = 0.0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Sy[k] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) { Wbx[k] = 0.0; Wby[k] = 0.0; fy_prev[k] = 0.0; }
+    for (int k = 0; k < 5; ++k) { Sy[k] = 0.0; fy_prev[k] = 0.0; }
 
     const int cstart = r0 - SW_PRE;
-    // preload: input row cstart+3 arrives at the first iteration; E1 rows one ahead
-    {
-        const size_t rp = rowp(cstart + 3);
+    // The input rows live in the ring: sweep row r sits in slot (r - cstart + 1) % SW_RING; it is
+    // copied while the warp works on row r - 7 and read up to row r + 1. Stage 2 also copies E1 and
+    // turns the row's faces into B1 when the row arrives (B1 is what every later read of the row
+    // needs).
+    auto slot = [&](int r) -> double* {
+        return ring + (unsigned)((r - cstart + 1) & (SW_RING - 1)) * SW_SLOT;
+    };
+    auto issue_row = [&](int r) {
+        if (r <= r1 + (MODE == 1 ? 3 : 4)) {
+            double* sl = slot(r);
+            const size_t rp = rowp(r);
 #pragma unroll
-        for (int q = 0; q < 6; ++q) arr[q] = __ldg(&in.f[q][rp + iw]);
-        arr_bxr = (lane == 31) ? __ldg(&in.f[4][rp + iw_r]) : 0.0;
-        if (MODE == 2) {
-            ax_cur = __ldg(&xsolve[rp + iw]);
-            axr_cur = (lane == 31) ? __ldg(&xsolve[rp + iw_r]) : 0.0;
-            const size_t rn = rowp(cstart + 4);
-            ax_nxt = __ldg(&xsolve[rn + iw]);
-            axr_nxt = (lane == 31) ? __ldg(&xsolve[rn + iw_r]) : 0.0;
+            for (int q = 0; q < 6; ++q) cp_async8(&sl[q * 32 + lane], &in.f[q][rp + iw]);
+            if (lane == 31) cp_async8(&sl[192], &in.f[4][rp + iw_r]);
+            if constexpr (MODE == 2) {
+                cp_async8(&sl[SW_E1 + lane], &xsolve[rp + iw]);
+                if (lane == 31) cp_async8(&sl[SW_E1 + 32], &xsolve[rp + iw_r]);
+            }
         }
-    }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int r = 0; r < SW_RING; ++r) issue_row(cstart - 1 + r);
 
     for (int c = cstart; c <= r1; ++c) {
-        // ---- arrive row c+3; issue the loads of row c+4 (and E1 row c+5)
-        double a[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) a[q] = arr[q];
-        const double a_bxr = arr_bxr;
-        double ax0 = ax_cur, ax1 = ax_nxt, axr0 = axr_cur, axr1 = axr_nxt;
-        {
-            const size_t rp = rowp(c + 4);
-#pragma unroll
-            for (int q = 0; q < 6; ++q) arr[q] = __ldg(&in.f[q][rp + iw]);
-            arr_bxr = (lane == 31) ? __ldg(&in.f[4][rp + iw_r]) : 0.0;
-            if (MODE == 2) {
-                ax_cur = ax_nxt;
-                axr_cur = axr_nxt;
-                const size_t rn = rowp(c + 5);
-                ax_nxt = __ldg(&xsolve[rn + iw]);
-                axr_nxt = (lane == 31) ? __ldg(&xsolve[rn + iw_r]) : 0.0;
-            }
-        }
-        // stage 2: accumulator of the rows written next iteration (hydro row c+1, faces row c)
-        double nH[4] = {0.0, 0.0, 0.0, 0.0}, nB[2] = {0.0, 0.0};
-        if (MODE == 2 && out_lane) {
-            if (c + 1 >= r0 && c + 1 < r1) {
-                const size_t g = (size_t)(c + 1) * nx + i;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) nH[q] = outB.f[q][g];
-            }
-            if (c >= r0 && c < r1) {
-                const size_t g = (size_t)c * nx + i;
-                nB[0] = outB.f[4][g];
-                nB[1] = outB.f[5][g];
-            }
-        }
-        // ---- B faces of row c+3 (and bxf one column to the right, for the cell-centred bx;
-        //      lane 31 has its own copy of that column)
-        double bx3 = a[4], by3 = a[5];
-        double bxr3 = a_bxr;
-        if (MODE == 2) {
-            // B1 = U1*_B + dt*g*(rate of E1) (solvers.hpp:484-485, 528-529)
+        if constexpr (MODE == 1) cp_async_wait<SW_RING - 5>();  // rows up to c+3 have landed
+        else cp_async_wait<SW_RING - 6>();                       // rows up to c+4 have landed
+        // stage 2: the accumulator values this row's outputs add to (hydro row c, faces row c-1),
+        // loaded here and used at the end of the row
+        double accH[4] = {0.0, 0.0, 0.0, 0.0}, accB[2] = {0.0, 0.0};
+        if constexpr (MODE == 2) {
+            // B1 = U1*_B + dt*g*(rate of E1) of row c+3 (solvers.hpp:484-485, 528-529), written
+            // over the row's faces in the ring (lane 31 also converts its right-hand bxf)
+            double* s3 = slot(c + 3);
+            const double* s4 = slot(c + 4);
+            const double ax0 = s3[SW_E1 + lane], ax1 = s4[SW_E1 + lane];
             double axr = shdn(ax0, 1);
-            if (lane == 31) axr = axr0;
+            if (lane == 31) axr = s3[SW_E1 + 32];
             const double rbx = -(ax1 - ax0) * idy;
             const double rby = (axr - ax0) * idx;
-            bx3 += rbx * cg;
-            by3 += rby * cg;
-            if (lane == 31) bxr3 += (-(axr1 - axr0) * idy) * cg;
-        }
-        {
-            const double right = shdn(bx3, 1);
-            if (lane != 31) bxr3 = right;
-        }
-        // shift the face windows: new row c+3 enters at index 4
+            s3[4 * 32 + lane] = s3[4 * 32 + lane] + rbx * cg;
+            s3[5 * 32 + lane] = s3[5 * 32 + lane] + rby * cg;
+            if (lane == 31) s3[192] = s3[192] + (-(s4[SW_E1 + 32] - s3[SW_E1 + 32]) * idy) * cg;
+            if (out_lane) {
+                if (c >= r0 && c < r1) {
+                    const size_t g = (size_t)c * nx + i;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { Wbx[k] = Wbx[k + 1]; Wby[k] = Wby[k + 1]; }
-        Wbx[4] = bx3;
-        Wby[4] = by3;
-
-        // ---- PRIM row c+2 (faces: bxf rows index 3, byf rows index 3 and 4)
+                    for (int q = 0; q < 4; ++q) accH[q] = outB.f[q][g];
+                }
+                if (c - 1 >= r0 && c - 1 < r1) {
+                    const size_t g = (size_t)(c - 1) * nx + i;
+                    accB[0] = outB.f[4][g];
+                    accB[1] = outB.f[5][g];
+                }
+            }
+        }
+        // ---- PRIM row c+2 (Grid.hpp:82-136): conserved hydro and bxf of row c+2, byf of rows c+2
+        //      and c+3; bxf one column to the right from the next lane (lane 31: its own copy)
         double nrho, nvx, nvy, np, nbxc, nbyc;
         {
-            nbxc = (Wbx[3] + bxr_prev) / 2.0;
-            nbyc = (Wby[3] + Wby[4]) / 2.0;
-            double rho = pend[0];
+            const double* s2 = slot(c + 2);
+            const double bxf2 = s2[4 * 32 + lane];
+            double bxr2 = shdn(bxf2, 1);
+            if (lane == 31) bxr2 = s2[192];
+            nbxc = (bxf2 + bxr2) / 2.0;
+            nbyc = (s2[5 * 32 + lane] + slot(c + 3)[5 * 32 + lane]) / 2.0;
+            double rho = s2[lane];
             if (MODE == 2 && rho < kRhoFloor) rho = kRhoFloor;  // floored in place (solvers.hpp:522-523)
-            np = primitives(rho, pend[1], pend[2], pend[3], nbxc, nbyc, nvx, nvy);
+            np = primitives(rho, s2[32 + lane], s2[64 + lane], s2[96 + lane], nbxc, nbyc, nvx, nvy);
             nrho = rho;
         }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) pend[q] = a[q];  // conserved row c+3 becomes the next PRIM input
-        bxr_prev = bxr3;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             Prho[k] = Prho[k + 1]; Pvx[k] = Pvx[k + 1]; Pvy[k] = Pvy[k + 1];
@@ -210,8 +193,8 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
         }
         Prho[3] = nrho; Pvx[3] = nvx; Pvy[3] = nvy; Pp[3] = np; Pbxc[3] = nbxc;
         Pbyc[0] = Pbyc[1]; Pbyc[1] = Pbyc[2]; Pbyc[2] = nbyc;
-        // window rows now: P*[0..3] = c-1 .. c+2, Pbyc[0..2] = c .. c+2,
-        //                  Wbx/Wby[0..4] = c-1 .. c+3
+        // window rows now: P*[0..3] = c-1 .. c+2, Pbyc[0..2] = c .. c+2; ring rows c-1 .. c+3
+        //                  (stage 2: their faces hold B1)
 
         // ---- YFACE: top face of (i, c); D = upper y-extrapolation of row c, U = lower of c+1
         //      (MUSCL.hpp:26-47). With kYReuse each row's limited slope is formed once, when the
@@ -248,7 +231,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
                 Up.p = recon_lo(Pp[1], Pp[2], Pp[3]);
                 Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
             }
-            Dn.by = Up.by = Wby[2];  // byf of row c+1
+            Dn.by = Up.by = slot(c + 1)[5 * 32 + lane];  // byf of row c+1
             fy = hll<1>(Dn, Up);
         }
         // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of
@@ -274,7 +257,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             xrecon(Pvy[1], L.vy, R.vy);
             xrecon(Pp[1], L.p, R.p);
             xrecon(Pbyc[0], L.by, R.by);
-            L.bx = R.bx = shdn(Wbx[1], 1);  // bxf(i+1, c)
+            L.bx = R.bx = shdn(slot(c)[4 * 32 + lane], 1);  // bxf(i+1, c)
             fx = hll<0>(L, R);
         }
         // ---- CORNER (i, c): eN = -Fx^By(i-1, c), eS = -Fx^By(i-1, c-1), eE = Fy^Bx(i, c-1),
@@ -291,8 +274,9 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
         }
         double jz = 0.0;
         if (MODE == 2) {  // eta*J_z(B1) at corner (i, c) (solvers.hpp:450-461)
-            const double dBy_dx = (Wby[1] - shup(Wby[1], 1)) * idx;
-            const double dBx_dy = (Wbx[1] - Wbx[0]) * idy;
+            const double by1 = slot(c)[5 * 32 + lane];
+            const double dBy_dx = (by1 - shup(by1, 1)) * idx;
+            const double dBx_dy = (slot(c)[4 * 32 + lane] - slot(c - 1)[4 * 32 + lane]) * idy;
             jz = D.eta * (dBy_dx - dBx_dy);
         }
         // ---- hydro rates of row c
@@ -304,10 +288,11 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             f[3] = -((fx.E - shup(fx.E, 1)) * idx + (fy.E - fy_prev[3]) * idy);
             if (out_lane && c >= r0 && c < r1) {
                 const size_t g = (size_t)c * nx + i;
-                if (MODE == 1) {
+                if constexpr (MODE == 1) {
+                    const double* sc = slot(c);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const double u = __ldg(&in.f[q][g]);
+                        const double u = sc[q * 32 + lane];
                         outA.f[q][g] = u + f[q] * cA;                       // predictor
                         const double ua = (q == 0 && u < kRhoFloor) ? kRhoFloor : u;
                         outB.f[q][g] = ua + f[q] * cB;                      // accumulator
@@ -329,8 +314,9 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             }
             if (out_lane && c - 1 >= r0 && c - 1 < r1) {
                 const size_t g = (size_t)(c - 1) * nx + i;
-                if (MODE == 1) {
-                    const double ubx = Wbx[0], uby = Wby[0];  // U^n faces of row c-1
+                if constexpr (MODE == 1) {
+                    const double* sp = slot(c - 1);
+                    const double ubx = sp[4 * 32 + lane], uby = sp[5 * 32 + lane];  // U^n faces, row c-1
                     outA.f[4][g] = ubx + fbx * cA;
                     outA.f[5][g] = uby + fby * cA;
                     outB.f[4][g] = ubx + fbx * cB;
@@ -350,22 +336,29 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
         fxbt_prev = fx.bt;
         ez_prev = ez;
         jz_prev = jz;
-        if (MODE == 2) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) accH[q] = nH[q];
-            accB[0] = nB[0];
-            accB[1] = nB[1];
-        }
+        issue_row(c + 7);  // into the slot of row c-1, no longer read
     }
+    cp_async_wait<0>();  // leave no copy in flight into the ring
+}
+
+// Dynamic shared memory of a block of the explicit-stage kernels (their warps' row rings).
+constexpr size_t sweep_smem_bytes(int mode) {
+    return (void)mode, (size_t)SW_WARPS * SW_RING * SW_SLOT * sizeof(double);
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
 k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
               const double* __restrict__ xsolve, Planes outA, Planes outB, SweepGeom G) {
+#if defined(__CUDA_ARCH__)
+    extern __shared__ __align__(16) double sw_ring_mem[];
+#else
+    static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];  // host compilation: one copy
+#endif
+    double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
     const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
-    stage_sweep_warp<MODE>(D, C, in, xsolve, outA, outB, G, w);
+    stage_sweep_warp<MODE>(D, C, in, xsolve, outA, outB, G, w, ring);
 }
 
 }  // namespace mhd
