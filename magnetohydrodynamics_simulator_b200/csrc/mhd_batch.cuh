@@ -97,23 +97,28 @@ k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ 
 #else
     static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];
 #endif
-    double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
+    __shared__ SweepPtrTable tab[SW_WARPS];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    double* const ring = sw_ring_mem + (size_t)wl * SW_RING * SW_SLOT;
+    SweepPtrTable& t = tab[wl];
+    const SmemPlanes pl{&t};
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
         const WorkItem e = items[it];
         const BatchInst& I = insts[e.inst];
-        CPlanes in;
-        Planes oa, ob;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            in.f[q] = (MODE == 1) ? I.S[q] : I.T[q];
-            oa.f[q] = I.T[q];
-            ob.f[q] = I.A[q];
+        __syncwarp();  // the previous item's sweep has read its table
+        if (lane < 6) {
+            t.in[lane] = (MODE == 1) ? I.S[lane] : I.T[lane];
+            t.a[lane] = I.T[lane];
+            t.b[lane] = I.A[lane];
+        } else if (lane == 6) {
+            t.x = (MODE == 1) ? nullptr : I.x;
         }
+        __syncwarp();
         const Domain D = I.D;
         const SweepGeom G = I.sg;
-        stage_sweep_warp<MODE>(D, I.C, in, (MODE == 1) ? nullptr : I.x, oa, ob, G, e.w, ring);
+        stage_sweep_warp<MODE>(D, I.C, pl, G, e.w, ring);
     }
 }
 

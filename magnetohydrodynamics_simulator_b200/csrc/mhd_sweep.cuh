@@ -71,12 +71,45 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 #define MHD_SWEEP_XREUSE_2 1
 #endif
 
+// Where a sweep finds its planes: in(q) the six input planes, x() the corner field E1 (stage 2),
+// a(q) / b(q) the two output plane sets (stage 1: predictor / accumulator; stage 2: - /
+// accumulator, read and written).
+// ParamPlanes: kernel parameters (constant bank; no registers held).
+struct ParamPlanes {
+    CPlanes in_;
+    const double* x_;
+    Planes a_, b_;
+    __device__ __forceinline__ const double* in(int q) const { return in_.f[q]; }
+    __device__ __forceinline__ const double* x() const { return x_; }
+    __device__ __forceinline__ double* a(int q) const { return a_.f[q]; }
+    __device__ __forceinline__ double* b(int q) const { return b_.f[q]; }
+};
+// SmemPlanes: a per-warp copy of an instance's pointers in shared memory, read with a volatile
+// load at each use, so that a persistent kernel stepping many instances keeps none of them live in
+// registers (18 pointers would cost 36 registers per thread).
+struct SweepPtrTable {
+    const double* in[6];
+    const double* x;
+    double* a[6];
+    double* b[6];
+};
+struct SmemPlanes {
+    const SweepPtrTable* t;
+    template <class T>
+    __device__ __forceinline__ static T vload(T const* p) {
+        return *static_cast<T const volatile*>(p);
+    }
+    __device__ __forceinline__ const double* in(int q) const { return vload(&t->in[q]); }
+    __device__ __forceinline__ const double* x() const { return vload(&t->x); }
+    __device__ __forceinline__ double* a(int q) const { return vload(&t->a[q]); }
+    __device__ __forceinline__ double* b(int q) const { return vload(&t->b[q]); }
+};
+
 // The sweep of one warp over work item w (strip w % strips_x, segment w / strips_x) of one grid.
-template <int MODE>
+template <int MODE, class PL>
 __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
-                                                 const CPlanes& in, const double* __restrict__ xsolve,
-                                                 const Planes& outA, const Planes& outB,
-                                                 const SweepGeom& G, int w, double* ring) {
+                                                 const PL& pl, const SweepGeom& G, int w,
+                                                 double* ring) {
     const int lane = threadIdx.x & 31;
     const int nx = D.nx, ny = D.ny;
     const int sx = w % G.strips_x, sy = w / G.strips_x;
@@ -127,11 +160,11 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             double* sl = slot(r);
             const size_t rp = rowp(r);
 #pragma unroll
-            for (int q = 0; q < 6; ++q) cp_async8(&sl[q * 32 + lane], &in.f[q][rp + iw]);
-            if (lane == 31) cp_async8(&sl[192], &in.f[4][rp + iw_r]);
+            for (int q = 0; q < 6; ++q) cp_async8(&sl[q * 32 + lane], &pl.in(q)[rp + iw]);
+            if (lane == 31) cp_async8(&sl[192], &pl.in(4)[rp + iw_r]);
             if constexpr (MODE == 2) {
-                cp_async8(&sl[SW_E1 + lane], &xsolve[rp + iw]);
-                if (lane == 31) cp_async8(&sl[SW_E1 + 32], &xsolve[rp + iw_r]);
+                cp_async8(&sl[SW_E1 + lane], &pl.x()[rp + iw]);
+                if (lane == 31) cp_async8(&sl[SW_E1 + 32], &pl.x()[rp + iw_r]);
             }
         }
         cp_async_commit();
@@ -162,12 +195,12 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
                 if (c >= r0 && c < r1) {
                     const size_t g = (size_t)c * nx + i;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) accH[q] = outB.f[q][g];
+                    for (int q = 0; q < 4; ++q) accH[q] = pl.b(q)[g];
                 }
                 if (c - 1 >= r0 && c - 1 < r1) {
                     const size_t g = (size_t)(c - 1) * nx + i;
-                    accB[0] = outB.f[4][g];
-                    accB[1] = outB.f[5][g];
+                    accB[0] = pl.b(4)[g];
+                    accB[1] = pl.b(5)[g];
                 }
             }
         }
@@ -293,13 +326,13 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const double u = sc[q * 32 + lane];
-                        outA.f[q][g] = u + f[q] * cA;                       // predictor
+                        pl.a(q)[g] = u + f[q] * cA;                       // predictor
                         const double ua = (q == 0 && u < kRhoFloor) ? kRhoFloor : u;
-                        outB.f[q][g] = ua + f[q] * cB;                      // accumulator
+                        pl.b(q)[g] = ua + f[q] * cB;                      // accumulator
                     }
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) outB.f[q][g] = accH[q] + f[q] * cB;
+                    for (int q = 0; q < 4; ++q) pl.b(q)[g] = accH[q] + f[q] * cB;
                 }
             }
         }
@@ -317,17 +350,17 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
                 if constexpr (MODE == 1) {
                     const double* sp = slot(c - 1);
                     const double ubx = sp[4 * 32 + lane], uby = sp[5 * 32 + lane];  // U^n faces, row c-1
-                    outA.f[4][g] = ubx + fbx * cA;
-                    outA.f[5][g] = uby + fby * cA;
-                    outB.f[4][g] = ubx + fbx * cB;
-                    outB.f[5][g] = uby + fby * cB;
+                    pl.a(4)[g] = ubx + fbx * cA;
+                    pl.a(5)[g] = uby + fby * cA;
+                    pl.b(4)[g] = ubx + fbx * cB;
+                    pl.b(5)[g] = uby + fby * cB;
                 } else {
                     double ax = accB[0] + fbx * cB;
                     double ay = accB[1] + fby * cB;
                     ax += g2x * c1mg;
                     ay += g2y * c1mg;
-                    outB.f[4][g] = ax;
-                    outB.f[5][g] = ay;
+                    pl.b(4)[g] = ax;
+                    pl.b(5)[g] = ay;
                 }
             }
         }
@@ -358,7 +391,8 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
     double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
     const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
-    stage_sweep_warp<MODE>(D, C, in, xsolve, outA, outB, G, w, ring);
+    const ParamPlanes pl{in, xsolve, outA, outB};
+    stage_sweep_warp<MODE>(D, C, pl, G, w, ring);
 }
 
 }  // namespace mhd
