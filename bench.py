@@ -438,6 +438,8 @@ def measure_batched(torch, m, steps):
         "zones_per_step": int(zones), "value": zones * steps / (batch_ms * 1e-3), "unit": UNIT,
         "ms_per_step": batch_ms / steps, "launches_per_step": launches,
         "tuning": {k: tuning[k] for k in ("stage_rows", "cg_rows", "cg_order")},
+        "tuning_step_ms": {"explicit_kernels": tuning["stage_ms"], "implicit_solves": tuning["cg_ms"],
+                           "note": "device time of one autotuning step of the chosen decomposition"},
         "plain_loop": {"value": zones * steps / (plain_ms * 1e-3), "unit": UNIT,
                        "ms_per_step": plain_ms / steps,
                        "how": "one context per instance on one stream, run(steps) in turn"},
