@@ -219,7 +219,7 @@ mhd_status rate_vjp(mhd_adjoint* a, const double* const U[6], const double* cons
                     int accumulate, double* const out[6]) {
     const Domain& D = a->dom;
     AdjScratch& s = a->s;
-    k_primitives<<<a->ew_blocks, 256, 0, a->stream>>>(D, cplanes6(U), s.P[0], s.P[1], s.P[2], s.P[3],
+    k_primitives<<<cell_grid(D.nx, D.ny), 256, 0, a->stream>>>(D, cplanes6(U), s.P[0], s.P[1], s.P[2], s.P[3],
                                                       s.P[4], s.P[5]);
     MHD_TRY(cudaGetLastError());
     PrimPlanes P;
@@ -232,14 +232,14 @@ mhd_status rate_vjp(mhd_adjoint* a, const double* const U[6], const double* cons
         cX.f[k] = s.X[k];
         cY.f[k] = s.Y[k];
     }
-    k_adj_faces<0><<<a->ew_blocks, 256, 0, a->stream>>>(D, P, U[4], U[5], cplanes6(w), X);
+    k_adj_faces<0><<<cell_grid(D.nx, D.ny), 256, 0, a->stream>>>(D, P, U[4], U[5], cplanes6(w), X);
     MHD_TRY(cudaGetLastError());
-    k_adj_faces<1><<<a->ew_blocks, 256, 0, a->stream>>>(D, P, U[4], U[5], cplanes6(w), Y);
+    k_adj_faces<1><<<cell_grid(D.nx, D.ny), 256, 0, a->stream>>>(D, P, U[4], U[5], cplanes6(w), Y);
     MHD_TRY(cudaGetLastError());
-    k_adj_cells<<<a->ew_blocks, 256, 0, a->stream>>>(D, cplanes6(U), P, cX, cY, scale, accumulate,
+    k_adj_cells<<<cell_grid(D.nx, D.ny), 256, 0, a->stream>>>(D, cplanes6(U), P, cX, cY, scale, accumulate,
                                                      planes6(out), s.bc[0], s.bc[1]);
     MHD_TRY(cudaGetLastError());
-    k_adj_bfaces<<<a->ew_blocks, 256, 0, a->stream>>>(D, s.bc[0], s.bc[1], s.X[10], s.Y[10], scale,
+    k_adj_bfaces<<<cell_grid(D.nx, D.ny), 256, 0, a->stream>>>(D, s.bc[0], s.bc[1], s.X[10], s.Y[10], scale,
                                                       accumulate, out[4], out[5]);
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
@@ -269,31 +269,32 @@ mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl
     const double cg = a->dt * a->g, cd = a->dt * a->d;
     const double c1md = a->dt * (1.0 - a->d), c1mg = a->dt * (1.0 - a->g);
     const int B = a->ew_blocks;
+    const dim3 CG2 = cell_grid(D.nx, D.ny);
     cudaStream_t st = a->stream;
     mhd_status r;
     // final combination: B^{n+1} = A_B + cg * eta * C Jz(B2)
-    k_adj_jz<<<B, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
-    k_adj_jz<<<B, 256, 0, st>>>(D, sl.A[4], sl.A[5], 1.0, x2, cg, s.c2);  // Jz(B2)
+    k_adj_jz<<<CG2, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
+    k_adj_jz<<<CG2, 256, 0, st>>>(D, sl.A[4], sl.A[5], 1.0, x2, cg, s.c2);  // Jz(B2)
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.c1, s.c2, -cg)) != MHD_OK) return r;
-    k_adj_curl<<<B, 256, 0, st>>>(D, s.c1, cg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
+    k_adj_curl<<<CG2, 256, 0, st>>>(D, s.c1, cg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
                                   s.fb[0], s.fb[1]);  // lambda_B2
     MHD_TRY(cudaGetLastError());
     // B2 = A_B + cg S(A_B)
     if ((r = solve(a, s.fb[0], s.fb[1], cg, s.y)) != MHD_OK) return r;
-    k_adj_curl<<<B, 256, 0, st>>>(D, s.y, eta, s.lam[4], s.lam[5], 1.0, s.fb[0], s.fb[1], 1.0,
+    k_adj_curl<<<CG2, 256, 0, st>>>(D, s.y, eta, s.lam[4], s.lam[5], 1.0, s.fb[0], s.fb[1], 1.0,
                                   s.lam[4], s.lam[5]);  // lambda_A_B
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.y, s.c2, -1.0)) != MHD_OK) return r;
     // g2 = R(B1) with weight c1mg
-    k_adj_jz<<<B, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
-    k_adj_jz<<<B, 256, 0, st>>>(D, sl.T[4], sl.T[5], 1.0, x1, cg, s.c2);  // Jz(B1)
+    k_adj_jz<<<CG2, 256, 0, st>>>(D, s.lam[4], s.lam[5], 1.0, nullptr, 0.0, s.c1);
+    k_adj_jz<<<CG2, 256, 0, st>>>(D, sl.T[4], sl.T[5], 1.0, x1, cg, s.c2);  // Jz(B1)
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.c1, s.c2, -c1mg)) != MHD_OK) return r;
-    k_adj_curl<<<B, 256, 0, st>>>(D, s.c1, c1mg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
+    k_adj_curl<<<CG2, 256, 0, st>>>(D, s.c1, c1mg * eta, nullptr, nullptr, 0.0, nullptr, nullptr, 0.0,
                                   s.fb[0], s.fb[1]);
     // f2 = F(U1), U1 = (T hydro, B1), weight c1md
-    k_adj_curl<<<B, 256, 0, st>>>(D, x1, cg, sl.T[4], sl.T[5], 1.0, nullptr, nullptr, 0.0,
+    k_adj_curl<<<CG2, 256, 0, st>>>(D, x1, cg, sl.T[4], sl.T[5], 1.0, nullptr, nullptr, 0.0,
                                   s.B1[0], s.B1[1]);
     MHD_TRY(cudaGetLastError());
     const double* U1[6] = {sl.T[0], sl.T[1], sl.T[2], sl.T[3], s.B1[0], s.B1[1]};
@@ -306,7 +307,7 @@ mhd_status adjoint_step(mhd_adjoint* a, const double* const U[6], const Slot& sl
         if ((r = axpby(a, 2, 1.0, x2p, 1.0, y2p, o2p)) != MHD_OK) return r;
     }
     if ((r = solve(a, s.lamT[4], s.lamT[5], cg, s.y)) != MHD_OK) return r;
-    k_adj_curl<<<B, 256, 0, st>>>(D, s.y, eta, s.lamT[4], s.lamT[5], 1.0, nullptr, nullptr, 0.0,
+    k_adj_curl<<<CG2, 256, 0, st>>>(D, s.y, eta, s.lamT[4], s.lamT[5], 1.0, nullptr, nullptr, 0.0,
                                   s.lamT[4], s.lamT[5]);
     MHD_TRY(cudaGetLastError());
     if ((r = dot_acc(a, s.y, s.c2, -1.0)) != MHD_OK) return r;

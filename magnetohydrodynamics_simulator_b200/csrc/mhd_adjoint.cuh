@@ -251,10 +251,9 @@ static __global__ void __launch_bounds__(256, 2)
 k_adj_faces(Domain D, PrimPlanes P, const double* __restrict__ bxf, const double* __restrict__ byf,
             CPlanes w, FaceAdjPlanes out) {
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         // cells along the normal: c-1, c, c+1, c+2 (c = this cell)
         auto cell = [&](int k) -> size_t {
             return DIR == 0 ? (size_t)j * nx + wrap(i + k, nx) : (size_t)wrap(j + k, ny) * nx + i;
@@ -337,10 +336,9 @@ static __global__ void __launch_bounds__(256)
 k_adj_cells(Domain D, CPlanes U, PrimPlanes P, CFaceAdjPlanes X, CFaceAdjPlanes Y, double scale,
             int accumulate, Planes out, double* __restrict__ bxc_adj, double* __restrict__ byc_adj) {
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         double ax[5], ay[5];
         const int qx[5] = {0, 1, 2, 3, 5}, qy[5] = {0, 1, 2, 3, 4};
 #pragma unroll
@@ -405,10 +403,9 @@ k_adj_bfaces(Domain D, const double* __restrict__ bxc_adj, const double* __restr
              const double* __restrict__ xbn, const double* __restrict__ ybn, double scale,
              int accumulate, double* __restrict__ out_bx, double* __restrict__ out_by) {
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         const size_t gxm = (size_t)j * nx + wrap(i - 1, nx);
         const size_t gym = (size_t)wrap(j - 1, ny) * nx + i;
         const double abx = 0.5 * (bxc_adj[g] + bxc_adj[gxm]) + xbn[gxm];
@@ -426,11 +423,10 @@ static __global__ void __launch_bounds__(256)
 k_adj_jz(Domain D, const double* __restrict__ bx, const double* __restrict__ by, double s,
          const double* __restrict__ x, double t, double* __restrict__ out) {
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
     const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         const size_t gxm = (size_t)j * nx + wrap(i - 1, nx);
         const size_t gym = (size_t)wrap(j - 1, ny) * nx + i;
         double v = s * ((by[g] - by[gxm]) * idx - (bx[g] - bx[gym]) * idy);
@@ -453,11 +449,10 @@ k_adj_curl(Domain D, const double* __restrict__ E, double s, const double* base_
            const double* base_by, double a, const double* extra_bx, const double* extra_by,
            double b, double* out_bx, double* out_by) {
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
     const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         const size_t gxp = (size_t)j * nx + wrap(i + 1, nx);
         const size_t gyp = (size_t)wrap(j + 1, ny) * nx + i;
         double rbx = E ? s * (-(E[gyp] - E[g]) * idy) : 0.0;

@@ -537,8 +537,7 @@ mhd_status mhd_get_primitives(mhd_context* c, double* const prim[6], int layout,
         (layout == MHD_LAYOUT_PADDED && ng < 0))
         return MHD_ERR_INVALID_ARGUMENT;
     if (!c->have_state) return MHD_ERR_NO_STATE;
-    const int blocks = std::max(1, std::min((int)((c->n + 255) / 256), c->num_sms * 8));
-    k_primitives<<<blocks, 256, 0, c->stream>>>(c->dom, cplanes(c->S), c->T[0], c->T[1], c->T[2],
+    k_primitives<<<cell_grid(c->dom.nx, c->dom.ny), 256, 0, c->stream>>>(c->dom, cplanes(c->S), c->T[0], c->T[1], c->T[2],
                                                  c->T[3], c->T[4], c->T[5]);
     MHD_TRY(cudaGetLastError());
     for (int k = 0; k < 6; ++k) {

@@ -100,6 +100,12 @@ __device__ __forceinline__ int wrap(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
+// Launch shape of the 2-D grid-stride per-cell kernels: columns on x (256-thread blocks), rows on
+// y (at most 65535 row blocks).
+inline dim3 cell_grid(int nx, int ny) {
+    return dim3((unsigned)((nx + 255) / 256), (unsigned)(ny < 65535 ? ny : 65535));
+}
+
 __device__ __forceinline__ unsigned long long global_timer_ns() {
 #if defined(__CUDA_ARCH__)
     unsigned long long t;
@@ -458,11 +464,11 @@ static __global__ void k_divb_final(const double* partial, int nblocks, long lon
 static __global__ void __launch_bounds__(256)
 k_primitives(Domain D, CPlanes u, double* rho_f, double* vx, double* vy, double* p, double* bxc,
              double* byc) {
+    // 2-D launch: columns on x, rows on y (grid-stride in both)
     const int nx = D.nx, ny = D.ny;
-    const size_t n = (size_t)nx * ny;
-    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-         g += (size_t)gridDim.x * blockDim.x) {
-        const int j = (int)(g / nx), i = (int)(g - (size_t)j * nx);
+    for (int j = blockIdx.y; j < ny; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+        const size_t g = (size_t)j * nx + i;
         const double bx = (u.f[4][g] + u.f[4][(size_t)j * nx + wrap(i + 1, nx)]) / 2.0;
         const double by = (u.f[5][g] + u.f[5][(size_t)wrap(j + 1, ny) * nx + i]) / 2.0;
         double rho = u.f[0][g], ux, uy;
