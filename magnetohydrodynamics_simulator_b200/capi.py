@@ -62,7 +62,7 @@ class BatchTuning(ctypes.Structure):
         ("stage_rows", ctypes.c_int),
         ("cg_rows", ctypes.c_int),
         ("cg_order", ctypes.c_int),
-        ("pad", ctypes.c_int),
+        ("stage_tail_rows", ctypes.c_int),
         ("stage_ms", ctypes.c_double),
         ("cg_ms", ctypes.c_double),
     ]
@@ -306,6 +306,9 @@ class Context:
         return int(self.lib.mhd_launches_per_step(self.h))
 
 
+_TUNING_KEYS = ("stage_rows", "cg_rows", "cg_order", "stage_tail_rows", "stage_ms", "cg_ms")
+
+
 class Batch:
     """Many independent periodic simulations of uneven sizes stepped together (one launch per
     stage for the whole batch). Each instance is specified like a Context: a dict with keys
@@ -397,15 +400,15 @@ class Batch:
     def autotune(self) -> dict:
         t = BatchTuning()
         _check(self.lib.mhd_batch_autotune(self.h, ctypes.byref(t)), "mhd_batch_autotune")
-        return {k: getattr(t, k) for k in ("stage_rows", "cg_rows", "cg_order", "stage_ms", "cg_ms")}
+        return {k: getattr(t, k) for k in _TUNING_KEYS}
 
     def tuning(self) -> dict:
         t = BatchTuning()
         _check(self.lib.mhd_batch_get_tuning(self.h, ctypes.byref(t)), "mhd_batch_get_tuning")
-        return {k: getattr(t, k) for k in ("stage_rows", "cg_rows", "cg_order", "stage_ms", "cg_ms")}
+        return {k: getattr(t, k) for k in _TUNING_KEYS}
 
-    def set_tuning(self, stage_rows: int, cg_rows: int, cg_order: int = 0):
-        t = BatchTuning(stage_rows, cg_rows, cg_order, 0, 0.0, 0.0)
+    def set_tuning(self, stage_rows: int, cg_rows: int, cg_order: int = 0, stage_tail_rows: int = 0):
+        t = BatchTuning(stage_rows, cg_rows, cg_order, stage_tail_rows, 0.0, 0.0)
         _check(self.lib.mhd_batch_set_tuning(self.h, ctypes.byref(t)), "mhd_batch_set_tuning")
 
     def synchronize_status(self):

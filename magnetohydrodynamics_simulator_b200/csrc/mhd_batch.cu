@@ -25,8 +25,10 @@ namespace {
 constexpr int kBatchPlanes = 23;
 constexpr int kQueues = 3;  // work counters: stage 1, stage 2, finalize
 
-// Candidate decompositions the autotuner times (rows per work item; solver dealing order).
-constexpr int kStageRowsCand[] = {16, 32, 64, 128, 256};
+// Candidate decompositions the autotuner times: explicit-stage (rows per item, tail rows per
+// item), solver rows per item (each with both dealing orders).
+constexpr int kStageCand[][2] = {{64, 0},   {128, 0},  {256, 0},  {128, 32}, {256, 32},
+                                 {256, 64}, {512, 32}, {384, 32}, {192, 32}, {512, 64}};
 constexpr int kCgRowsCand[] = {8, 16, 32, 64, 128};
 
 }  // namespace
@@ -47,8 +49,10 @@ struct mhd_batch {
     std::vector<BatchInst> h_insts[2];
     int parity = 0;  // descriptor array of the next step
     // work items: explicit stages / finalize, then the solver's (chunk by chunk)
-    WorkItem* d_items = nullptr;
-    size_t items_cap = 0;
+    void* d_items_mem = nullptr;          // both lists in one allocation
+    SweepItem* d_sweep_items = nullptr;  // explicit stages and finalize
+    WorkItem* d_cg_items = nullptr;      // solver, chunk by chunk
+    size_t items_cap = 0;                // bytes
     int n_stage_items = 0;
     int n_cg_items = 0;
     int nchunks = 0;
@@ -99,74 +103,78 @@ int grid_for(int occ_blocks, int num_sms, int nitems, int warps_per_block) {
 }
 
 // Build the work-item lists and the descriptors' decomposition for tuning t, and upload both.
+// Explicit stages: every 28-column strip of every instance is cut into items of stage_rows rows;
+// with stage_tail_rows > 0 the last min(stage_rows, ny) rows of each strip are cut into items of
+// stage_tail_rows rows instead. Items run largest first (the kernels take them from a counter), so
+// the small ones fill the end of the launch.
 mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
-    if (t.stage_rows < 1 || t.cg_rows < 1 || (t.cg_order != 0 && t.cg_order != 1))
+    if (t.stage_rows < 1 || t.cg_rows < 1 || (t.cg_order != 0 && t.cg_order != 1) ||
+        t.stage_tail_rows < 0)
         return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaStreamSynchronize(b->stream));  // in-flight steps still read the old lists
-    std::vector<WorkItem> st_items, cg_items;
-    std::vector<int> st_rows;
+    std::vector<SweepItem> st_items;
     std::vector<int> cg_nw(b->count);
     for (int i = 0; i < b->count; ++i) {
         const int nx = b->prm[i].nx, ny = b->prm[i].ny;
-        SweepGeom sg;
-        sg.strips_x = (nx + SW_OUT - 1) / SW_OUT;
-        sg.seg_h = std::min(t.stage_rows, ny);
-        sg.segs_y = (ny + sg.seg_h - 1) / sg.seg_h;
-        sg.nwarps = sg.strips_x * sg.segs_y;
+        const int strips = (nx + SW_OUT - 1) / SW_OUT;
+        const int big = std::min(t.stage_rows, ny);
+        const int tail_start = (t.stage_tail_rows > 0) ? ny - big : ny;
+        for (int sx = 0; sx < strips; ++sx) {
+            int r = 0;
+            for (; r < tail_start; r = std::min(r + big, tail_start))
+                st_items.push_back(SweepItem{i, sx, r, std::min(r + big, tail_start)});
+            for (; r < ny; r += t.stage_tail_rows)
+                st_items.push_back(SweepItem{i, sx, r, std::min(r + t.stage_tail_rows, ny)});
+        }
         const int cg_strips = (nx + CG_W - 1) / CG_W;
         const int cg_seg = std::min(t.cg_rows, ny);
         cg_nw[i] = cg_strips * ((ny + cg_seg - 1) / cg_seg);
         for (int p = 0; p < 2; ++p) {
             BatchInst& I = b->h_insts[p][i];
-            I.sg = sg;
             I.cg_strips_x = cg_strips;
             I.cg_seg_h = cg_seg;
         }
-        for (int w = 0; w < sg.nwarps; ++w) {
-            st_items.push_back(WorkItem{i, w});
-            const int sy = w / sg.strips_x;
-            st_rows.push_back(std::min(sg.seg_h, ny - sy * sg.seg_h));
-        }
     }
-    // largest items first (the explicit kernels take items from a counter)
-    std::vector<int> order(st_items.size());
-    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int c) { return st_rows[a] > st_rows[c]; });
-    std::vector<WorkItem> items;
-    items.reserve(st_items.size());
-    for (int k : order) items.push_back(st_items[k]);
+    std::stable_sort(st_items.begin(), st_items.end(), [](const SweepItem& a, const SweepItem& c) {
+        return (a.r1 - a.r0) > (c.r1 - c.r0);
+    });
     // solver items, chunk by chunk
+    std::vector<WorkItem> cg_items;
     b->chunk_item0.assign(b->nchunks, 0);
     b->chunk_nitems.assign(b->nchunks, 0);
     int max_chunk_items = 0;
     for (int c = 0; c < b->nchunks; ++c) {
         const int i0 = c * CGB_MAX_INST, i1 = std::min(b->count, i0 + CGB_MAX_INST);
-        b->chunk_item0[c] = (int)items.size();
-        const size_t before = items.size();
+        b->chunk_item0[c] = (int)cg_items.size();
+        const size_t before = cg_items.size();
         if (t.cg_order == 0) {
             for (int i = i0; i < i1; ++i)
-                for (int w = 0; w < cg_nw[i]; ++w) items.push_back(WorkItem{i, w});
+                for (int w = 0; w < cg_nw[i]; ++w) cg_items.push_back(WorkItem{i, w});
         } else {
             int most = 0;
             for (int i = i0; i < i1; ++i) most = std::max(most, cg_nw[i]);
             for (int w = 0; w < most; ++w)
                 for (int i = i0; i < i1; ++i)
-                    if (w < cg_nw[i]) items.push_back(WorkItem{i, w});
+                    if (w < cg_nw[i]) cg_items.push_back(WorkItem{i, w});
         }
-        b->chunk_nitems[c] = (int)(items.size() - before);
+        b->chunk_nitems[c] = (int)(cg_items.size() - before);
         max_chunk_items = std::max(max_chunk_items, b->chunk_nitems[c]);
     }
     b->n_stage_items = (int)st_items.size();
-    b->n_cg_items = (int)(items.size() - st_items.size());
-    if (items.size() > b->items_cap) {
-        cudaFree(b->d_items);
-        b->d_items = nullptr;
+    b->n_cg_items = (int)cg_items.size();
+    const size_t bytes = st_items.size() * sizeof(SweepItem) + cg_items.size() * sizeof(WorkItem);
+    if (bytes > b->items_cap) {
+        cudaFree(b->d_items_mem);
+        b->d_items_mem = nullptr;
         b->items_cap = 0;
-        MHD_TRY(cudaMalloc(&b->d_items, items.size() * sizeof(WorkItem)));
-        b->items_cap = items.size();
+        MHD_TRY(cudaMalloc(&b->d_items_mem, bytes));
+        b->items_cap = bytes;
     }
-    MHD_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(WorkItem),
+    b->d_sweep_items = static_cast<SweepItem*>(b->d_items_mem);
+    b->d_cg_items = reinterpret_cast<WorkItem*>(b->d_sweep_items + st_items.size());
+    MHD_TRY(cudaMemcpy(b->d_sweep_items, st_items.data(), st_items.size() * sizeof(SweepItem),
+                       cudaMemcpyHostToDevice));
+    MHD_TRY(cudaMemcpy(b->d_cg_items, cg_items.data(), cg_items.size() * sizeof(WorkItem),
                        cudaMemcpyHostToDevice));
     for (int p = 0; p < 2; ++p)
         MHD_TRY(cudaMemcpy(b->d_insts[p], b->h_insts[p].data(), b->count * sizeof(BatchInst),
@@ -178,6 +186,7 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     b->tuning.stage_rows = t.stage_rows;
     b->tuning.cg_rows = t.cg_rows;
     b->tuning.cg_order = t.cg_order;
+    b->tuning.stage_tail_rows = t.stage_tail_rows;
     return MHD_OK;
 }
 
@@ -187,7 +196,7 @@ mhd_status launch_cg_chunks(mhd_batch* b, const BatchInst* insts, int solve, boo
         a.insts = insts;
         a.inst0 = c * CGB_MAX_INST;
         a.ninst = std::min(CGB_MAX_INST, b->count - a.inst0);
-        a.items = b->d_items + b->chunk_item0[c];
+        a.items = b->d_cg_items + b->chunk_item0[c];
         a.nitems = b->chunk_nitems[c];
         a.partials = b->partials;
         a.sync = b->syncs + 2 * c + solve;
@@ -223,7 +232,7 @@ mhd_status enqueue_step(mhd_batch* b, const double* dt_in, double dt_fixed, int 
         b->rec_cap, b->queues, kQueues, b->syncs, 2 * b->nchunks);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[0], b->stream));
-    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, sweep_smem_bytes(1), b->stream>>>(I, b->d_items,
+    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, sweep_smem_bytes(1), b->stream>>>(I, b->d_sweep_items,
                                                                         b->n_stage_items, b->queues);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[1], b->stream));
@@ -231,13 +240,13 @@ mhd_status enqueue_step(mhd_batch* b, const double* dt_in, double dt_fixed, int 
     if (s != MHD_OK) return s;
     if (ev) MHD_TRY(cudaEventRecord(ev[2], b->stream));
     k_stage_batch<2><<<b->stage_grid[1], 32 * SW_WARPS, sweep_smem_bytes(2), b->stream>>>(
-        I, b->d_items, b->n_stage_items, b->queues + 1);
+        I, b->d_sweep_items, b->n_stage_items, b->queues + 1);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[3], b->stream));
     s = launch_cg_chunks(b, I, 1, record);
     if (s != MHD_OK) return s;
     if (ev) MHD_TRY(cudaEventRecord(ev[4], b->stream));
-    k_finalize_batch<<<b->fin_grid, 32 * FS_WARPS, 0, b->stream>>>(I, b->d_items, b->n_stage_items,
+    k_finalize_batch<<<b->fin_grid, 32 * FS_WARPS, 0, b->stream>>>(I, b->d_sweep_items, b->n_stage_items,
                                                                    b->queues + 2);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[5], b->stream));
@@ -406,7 +415,8 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
             cudaSuccess)
         return fail(MHD_ERR_CUDA);
     mhd_batch_tuning t{};
-    t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", 32);
+    t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", 256);
+    t.stage_tail_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_TAIL_ROWS", 32);
     t.cg_rows = mhd_host::env_int("MHD_B200_BATCH_CG_ROWS", 32);
     t.cg_order = mhd_host::env_int("MHD_B200_BATCH_CG_ORDER", 0);
     const mhd_status s = apply_tuning(b, t);
@@ -424,7 +434,7 @@ mhd_status mhd_batch_destroy(mhd_batch* b) {
     cudaFree(b->status);
     cudaFree(b->d_insts[0]);
     cudaFree(b->d_insts[1]);
-    cudaFree(b->d_items);
+    cudaFree(b->d_items_mem);
     cudaFree(b->partials);
     cudaFree(b->syncs);
     cudaFree(b->queues);
@@ -596,7 +606,7 @@ mhd_status mhd_batch_get_tuning(mhd_batch* b, mhd_batch_tuning* t) {
 }
 
 // Autotuner: one CFL step of the current states per candidate, timed per kernel with events;
-// the explicit-stage row height and the solver's (row height, dealing order) are chosen
+// the explicit-stage (row height, tail height) and the solver's (row height, dealing order) are chosen
 // independently (they set disjoint kernels' decompositions). States, device statuses, step
 // coefficients and the descriptor parity are restored after every trial.
 mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
@@ -647,16 +657,18 @@ mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
         return MHD_OK;
     };
     if ((s = planes_copy(true)) != MHD_OK) return s;
-    constexpr int nst = sizeof(kStageRowsCand) / sizeof(int);
+    constexpr int nst = sizeof(kStageCand) / sizeof(kStageCand[0]);
     constexpr int ncg = sizeof(kCgRowsCand) / sizeof(int);
     double best_stage = 1e300, best_cg = 1e300;
-    int best_stage_rows = before.stage_rows, best_cg_rows = before.cg_rows, best_order = before.cg_order;
-    // trial -1 warms the kernels up; trials 0 .. 2*ncg-1 cover every solver candidate and every
-    // stage candidate (twice, the better time counts)
+    int best_stage_rows = before.stage_rows, best_tail = before.stage_tail_rows;
+    int best_cg_rows = before.cg_rows, best_order = before.cg_order;
+    // trial -1 warms the kernels up; trials 0 .. 2*ncg-1 cover every solver candidate (both dealing
+    // orders) and every explicit-stage candidate
     for (int trial = -1; trial < 2 * ncg; ++trial) {
         mhd_batch_tuning t{};
         const int tk = std::max(trial, 0);
-        t.stage_rows = kStageRowsCand[tk % nst];
+        t.stage_rows = kStageCand[tk % nst][0];
+        t.stage_tail_rows = kStageCand[tk % nst][1];
         t.cg_rows = kCgRowsCand[tk % ncg];
         t.cg_order = tk / ncg;
         if ((s = apply_tuning(b, t)) != MHD_OK) return s;
@@ -671,6 +683,7 @@ mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
         if (stage_ms < best_stage) {
             best_stage = stage_ms;
             best_stage_rows = t.stage_rows;
+            best_tail = t.stage_tail_rows;
         }
         if (cg_ms < best_cg) {
             best_cg = cg_ms;
@@ -680,6 +693,7 @@ mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
     }
     mhd_batch_tuning chosen{};
     chosen.stage_rows = best_stage_rows;
+    chosen.stage_tail_rows = best_tail;
     chosen.cg_rows = best_cg_rows;
     chosen.cg_order = best_order;
     if ((s = apply_tuning(b, chosen)) != MHD_OK) return s;

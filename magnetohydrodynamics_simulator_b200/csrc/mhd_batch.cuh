@@ -4,9 +4,9 @@
 // matrix coefficient and its own convergence, exactly as if it were stepped alone
 // (integrator_main.cpp:76-112 per instance).
 //
-// Work is described by flat lists of warp work items (instance, item), where item indexes the
-// instance's strip/segment decomposition: 28-column strips for the explicit stages and the
-// finalize (SweepGeom), 30-column strips for the solver. The explicit kernels are persistent and
+// Work is described by flat lists of warp work items: (instance, strip, rows) for the explicit
+// stages and the finalize (28-column strips, any row ranges), (instance, item) for the solver
+// (its strip/segment decomposition, 28-column strips of cg_seg_h rows). The explicit kernels are persistent and
 // pull items from a global counter (largest items first). The solver kernel deals its items to
 // warps in a fixed order, because its sums must be reduced in a fixed order.
 //
@@ -40,9 +40,16 @@ struct BatchInst {
     double hmin, courant, safety;
 };
 
+// Work item of the solver: item w of the instance's strip/segment decomposition.
 struct WorkItem {
     int inst;
     int w;
+};
+// Work item of the explicit stages and the finalize: rows [r0, r1) of column strip sx.
+struct SweepItem {
+    int inst;
+    int sx;
+    int r0, r1;
 };
 
 static_assert(SW_OUT == FS_OUT, "stages and finalize share one work-item list");
@@ -90,7 +97,7 @@ __device__ __forceinline__ int batch_next_item(int* queue) {
 
 template <int MODE>
 __global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
-k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ items, int nitems,
+k_stage_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__ items, int nitems,
               int* queue) {
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double sw_ring_mem[];
@@ -105,7 +112,7 @@ k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ 
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
-        const WorkItem e = items[it];
+        const SweepItem e = items[it];
         const BatchInst& I = insts[e.inst];
         __syncwarp();  // the previous item's sweep has read its table
         if (lane < 6) {
@@ -117,25 +124,23 @@ k_stage_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ 
         }
         __syncwarp();
         const Domain D = I.D;
-        const SweepGeom G = I.sg;
-        stage_sweep_warp<MODE>(D, I.C, pl, G, e.w, ring);
+        stage_sweep_warp<MODE>(D, I.C, pl, e.sx, e.r0, e.r1, ring);
     }
 }
 
 static __global__ void __launch_bounds__(32 * FS_WARPS)
-k_finalize_batch(const BatchInst* __restrict__ insts, const WorkItem* __restrict__ items, int nitems,
+k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__ items, int nitems,
                  int* queue) {
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
-        const WorkItem e = items[it];
+        const SweepItem e = items[it];
         const BatchInst& I = insts[e.inst];
         Planes acc;
 #pragma unroll
         for (int q = 0; q < 6; ++q) acc.f[q] = I.A[q];
         const Domain D = I.D;
-        const SweepGeom G = I.sg;
-        finalize_sweep_warp(D, I.C, acc, I.x, I.S[4], I.S[5], I.st, G, e.w);
+        finalize_sweep_warp(D, I.C, acc, I.x, I.S[4], I.S[5], I.st, e.sx, e.r0, e.r1);
     }
 }
 

@@ -18,18 +18,15 @@ constexpr int FS_OUT = 28;
 constexpr int FS_WARPS = 8;
 constexpr int FS_PRE = 3;  // rows swept before the first output row
 
-// The sweep of one warp over work item w of one grid.
+// The sweep of one warp over rows [r0, r1) of column strip sx of one grid.
 __device__ __forceinline__ void finalize_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
                                                     const Planes& acc, const double* __restrict__ xsolve,
                                                     double* __restrict__ bx_out,
                                                     double* __restrict__ by_out, DeviceStatus* st,
-                                                    const SweepGeom& G, int w) {
+                                                    int sx, int r0, int r1) {
     const int lane = threadIdx.x & 31;
     const int nx = D.nx, ny = D.ny;
-    const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int c0 = sx * FS_OUT;
-    const int r0 = sy * G.seg_h;
-    const int r1 = min(r0 + G.seg_h, ny);
     if (r0 >= r1) return;
     const int i = c0 - 1 + lane;
     const int iw = wrap(i, nx);
@@ -118,7 +115,9 @@ k_finalize_sweep(Domain D, const StepCoeffs* __restrict__ C, Planes acc,
                  double* __restrict__ by_out, DeviceStatus* st, SweepGeom G) {
     const int w = blockIdx.x * FS_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
-    finalize_sweep_warp(D, C, acc, xsolve, bx_out, by_out, st, G, w);
+    const int sx = w % G.strips_x, sy = w / G.strips_x;
+    const int r0 = sy * G.seg_h;
+    finalize_sweep_warp(D, C, acc, xsolve, bx_out, by_out, st, sx, r0, min(r0 + G.seg_h, D.ny));
 }
 
 }  // namespace mhd

@@ -105,17 +105,14 @@ struct SmemPlanes {
     __device__ __forceinline__ double* b(int q) const { return vload(&t->b[q]); }
 };
 
-// The sweep of one warp over work item w (strip w % strips_x, segment w / strips_x) of one grid.
+// The sweep of one warp over rows [r0, r1) of column strip sx of one grid.
 template <int MODE, class PL>
 __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
-                                                 const PL& pl, const SweepGeom& G, int w,
+                                                 const PL& pl, int sx, int r0, int r1,
                                                  double* ring) {
     const int lane = threadIdx.x & 31;
     const int nx = D.nx, ny = D.ny;
-    const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int c0 = sx * SW_OUT;
-    const int r0 = sy * G.seg_h;
-    const int r1 = min(r0 + G.seg_h, ny);
     if (r0 >= r1) return;
     // limited slopes formed once per cell (y: carried to the next row; x: shared with the lane on
     // the left), or per face as the reference writes them -- the same operands either way
@@ -392,7 +389,9 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
     const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
     const ParamPlanes pl{in, xsolve, outA, outB};
-    stage_sweep_warp<MODE>(D, C, pl, G, w, ring);
+    const int sx = w % G.strips_x, sy = w / G.strips_x;
+    const int r0 = sy * G.seg_h;
+    stage_sweep_warp<MODE>(D, C, pl, sx, r0, min(r0 + G.seg_h, D.ny), ring);
 }
 
 }  // namespace mhd

@@ -208,11 +208,13 @@ def test_autotune_restores_state_and_keeps_parity(m):
         assert err <= RUN_TOL, (i, err)
 
 
-@pytest.mark.parametrize("stage_rows,cg_rows,cg_order", [(1, 1, 0), (7, 3, 1), (300, 300, 0)])
-def test_every_decomposition_gives_the_same_step(m, stage_rows, cg_rows, cg_order):
+@pytest.mark.parametrize("stage_rows,cg_rows,cg_order,tail", [(1, 1, 0, 0), (7, 3, 1, 0), (300, 300, 0, 0),
+                                                            (16, 8, 0, 5), (64, 32, 1, 3)])
+def test_every_decomposition_gives_the_same_step(m, stage_rows, cg_rows, cg_order, tail):
     insts = _instances(SPECS)
     b = _batch(m, insts)
-    b.set_tuning(stage_rows, cg_rows, cg_order)
+    b.set_tuning(stage_rows, cg_rows, cg_order, tail)
+    assert b.tuning()["stage_tail_rows"] == tail
     dts = [1e-3] * len(insts)
     b.step(dts)
     b.synchronize()
