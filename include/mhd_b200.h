@@ -178,10 +178,11 @@ typedef struct mhd_batch mhd_batch;
 
 /* Work decomposition of the batch kernels, chosen by mhd_batch_autotune. */
 typedef struct mhd_batch_tuning {
-    int stage_rows;  /* rows per work item of the explicit stages and the finalize (>= 1) */
+    int stage_rows;  /* rows per work item of the explicit stages and the finalize (>= 1; a strip
+                      * is cut into equal items of at most this many rows) */
     int cg_rows;     /* rows per work item of the implicit solve (>= 1) */
     int cg_order;    /* solver items dealt to warps 0: instance by instance, 1: interleaved */
-    int stage_tail_rows; /* > 0: the last stage_rows rows of every strip go in items of this many
+    int stage_tail_rows; /* > 0: the last min(stage_rows, ny) rows of every strip go in items of this many
                           * rows, which largest-first scheduling runs last (fills the launch's
                           * tail); 0: none */
     double stage_ms; /* device time of the explicit kernels in the tuning step (output only) */

@@ -3,10 +3,12 @@
 // (mhd_batch.cuh), the launch sequence of one batched step, the CUDA-graph driver loop, the
 // autotuner and per-instance diagnostics.
 //
-// Device memory: instance i owns 23 dense nx_i*ny_i FP64 planes in one pool (the same plan as a
-// single context: S[6] state, T[6] predictor, A[6] accumulator, x, r[2], p[2]) plus its own
-// StepCoeffs and DeviceStatus. The descriptor array (BatchInst) is kept for even and odd steps,
-// which differ only in the trading hydro planes of S and A.
+// Device memory: instance i owns 23 dense nx_i*ny_i FP64 planes (the same plan as a single
+// context: S[6] state, T[6] predictor, A[6] accumulator, x, r[2], p[2]) plus its own StepCoeffs
+// and DeviceStatus. The pool is plane-major: each of the 23 planes is one arena of all instances,
+// instance i at the same zone offset in every arena, so a kernel reaches any plane of any instance
+// from the arena bases (kernel parameters) and one offset. The descriptor array (BatchInst) is
+// kept for even and odd steps, which differ only in the trading hydro planes of S and A.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,12 +50,16 @@ struct mhd_batch {
     BatchInst* d_insts[2] = {nullptr, nullptr};
     std::vector<BatchInst> h_insts[2];
     int parity = 0;  // descriptor array of the next step
+    ParamPlanes stage_base[2][2];  // [parity][stage - 1]: plane arenas of the explicit stages
+    FinParams fin_base[2];         // [parity]: plane arenas of the finalize
     // work items: explicit stages / finalize, then the solver's (chunk by chunk)
     void* d_items_mem = nullptr;          // both lists in one allocation
-    SweepItem* d_sweep_items = nullptr;  // explicit stages and finalize
+    SweepItem* d_sweep_items = nullptr;  // explicit stages
+    SweepItem* d_fin_items = nullptr;    // finalize
     WorkItem* d_cg_items = nullptr;      // solver, chunk by chunk
     size_t items_cap = 0;                // bytes
     int n_stage_items = 0;
+    int n_fin_items = 0;
     int n_cg_items = 0;
     int nchunks = 0;
     std::vector<int> chunk_item0, chunk_nitems;
@@ -102,30 +108,70 @@ int grid_for(int occ_blocks, int num_sms, int nitems, int warps_per_block) {
     return (int)std::max(1LL, std::min((long long)occ_blocks * num_sms, need));
 }
 
+// Smallest item height whose items (every 28-column strip cut into equal items of at most that
+// many rows) number at most `waves` x `warps`, i.e. fill that many waves of the resident warps.
+int balanced_rows(const mhd_batch* b, long long warps, int waves) {
+    const long long slots = std::max(1LL, warps * waves);
+    auto items_at = [&](int h) {
+        long long n = 0;
+        for (int i = 0; i < b->count; ++i)
+            n += (long long)((b->prm[i].nx + SW_OUT - 1) / SW_OUT) * ((b->prm[i].ny + h - 1) / h);
+        return n;
+    };
+    int lo = 1, hi = 1;
+    for (int i = 0; i < b->count; ++i) hi = std::max(hi, b->prm[i].ny);
+    if (items_at(hi) > slots) return hi;  // more strips than slots: whole strips
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (items_at(mid) <= slots) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+int balanced_stage_rows(const mhd_batch* b, int waves) {
+    return balanced_rows(b, (long long)std::min(b->stage_occ[0], b->stage_occ[1]) * b->num_sms * SW_WARPS,
+                         waves);
+}
+
+// Items of at most `rows` rows (equal heights within a strip) over every strip, largest first.
+void strip_items(const mhd_batch* b, int rows, int tail_rows, std::vector<SweepItem>& out) {
+    for (int i = 0; i < b->count; ++i) {
+        const int nx = b->prm[i].nx, ny = b->prm[i].ny;
+        const int strips = (nx + SW_OUT - 1) / SW_OUT;
+        const int big = std::min(rows, ny);
+        const int tail_start = (tail_rows > 0) ? ny - big : ny;
+        const int pieces = (tail_start + big - 1) / big;  // equal items over rows [0, tail_start)
+        for (int sx = 0; sx < strips; ++sx) {
+            for (int k = 0; k < pieces; ++k)
+                out.push_back(SweepItem{i, sx, (int)((long long)k * tail_start / pieces),
+                                        (int)((long long)(k + 1) * tail_start / pieces)});
+            for (int r = tail_start; r < ny; r += tail_rows)
+                out.push_back(SweepItem{i, sx, r, std::min(r + tail_rows, ny)});
+        }
+    }
+    std::stable_sort(out.begin(), out.end(), [](const SweepItem& a, const SweepItem& c) {
+        return (a.r1 - a.r0) > (c.r1 - c.r0);
+    });
+}
+
 // Build the work-item lists and the descriptors' decomposition for tuning t, and upload both.
-// Explicit stages: every 28-column strip of every instance is cut into items of stage_rows rows;
-// with stage_tail_rows > 0 the last min(stage_rows, ny) rows of each strip are cut into items of
-// stage_tail_rows rows instead. Items run largest first (the kernels take them from a counter), so
-// the small ones fill the end of the launch.
+// Explicit stages: every 28-column strip of every instance is cut into equal items of at most
+// stage_rows rows; with stage_tail_rows > 0 only the strip's first ny - min(stage_rows, ny) rows
+// are, and the rest go in items of stage_tail_rows rows. Items run largest first (the kernels take
+// them from a counter), so the small ones fill the end of the launch. Finalize: items that fill
+// one wave of its resident warps (at least 16 rows), as a single context's finalize.
 mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     if (t.stage_rows < 1 || t.cg_rows < 1 || (t.cg_order != 0 && t.cg_order != 1) ||
         t.stage_tail_rows < 0)
         return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaStreamSynchronize(b->stream));  // in-flight steps still read the old lists
-    std::vector<SweepItem> st_items;
+    std::vector<SweepItem> st_items, fin_items;
+    strip_items(b, t.stage_rows, t.stage_tail_rows, st_items);
+    strip_items(b, std::max(16, balanced_rows(b, (long long)b->fin_occ * b->num_sms * FS_WARPS, 1)), 0,
+                fin_items);
     std::vector<int> cg_nw(b->count);
     for (int i = 0; i < b->count; ++i) {
         const int nx = b->prm[i].nx, ny = b->prm[i].ny;
-        const int strips = (nx + SW_OUT - 1) / SW_OUT;
-        const int big = std::min(t.stage_rows, ny);
-        const int tail_start = (t.stage_tail_rows > 0) ? ny - big : ny;
-        for (int sx = 0; sx < strips; ++sx) {
-            int r = 0;
-            for (; r < tail_start; r = std::min(r + big, tail_start))
-                st_items.push_back(SweepItem{i, sx, r, std::min(r + big, tail_start)});
-            for (; r < ny; r += t.stage_tail_rows)
-                st_items.push_back(SweepItem{i, sx, r, std::min(r + t.stage_tail_rows, ny)});
-        }
         const int cg_strips = (nx + CG_W - 1) / CG_W;
         const int cg_seg = std::min(t.cg_rows, ny);
         cg_nw[i] = cg_strips * ((ny + cg_seg - 1) / cg_seg);
@@ -135,9 +181,6 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
             I.cg_seg_h = cg_seg;
         }
     }
-    std::stable_sort(st_items.begin(), st_items.end(), [](const SweepItem& a, const SweepItem& c) {
-        return (a.r1 - a.r0) > (c.r1 - c.r0);
-    });
     // solver items, chunk by chunk
     std::vector<WorkItem> cg_items;
     b->chunk_item0.assign(b->nchunks, 0);
@@ -161,8 +204,10 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
         max_chunk_items = std::max(max_chunk_items, b->chunk_nitems[c]);
     }
     b->n_stage_items = (int)st_items.size();
+    b->n_fin_items = (int)fin_items.size();
     b->n_cg_items = (int)cg_items.size();
-    const size_t bytes = st_items.size() * sizeof(SweepItem) + cg_items.size() * sizeof(WorkItem);
+    const size_t bytes = (st_items.size() + fin_items.size()) * sizeof(SweepItem) +
+                         cg_items.size() * sizeof(WorkItem);
     if (bytes > b->items_cap) {
         cudaFree(b->d_items_mem);
         b->d_items_mem = nullptr;
@@ -171,8 +216,11 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
         b->items_cap = bytes;
     }
     b->d_sweep_items = static_cast<SweepItem*>(b->d_items_mem);
-    b->d_cg_items = reinterpret_cast<WorkItem*>(b->d_sweep_items + st_items.size());
+    b->d_fin_items = b->d_sweep_items + st_items.size();
+    b->d_cg_items = reinterpret_cast<WorkItem*>(b->d_fin_items + fin_items.size());
     MHD_TRY(cudaMemcpy(b->d_sweep_items, st_items.data(), st_items.size() * sizeof(SweepItem),
+                       cudaMemcpyHostToDevice));
+    MHD_TRY(cudaMemcpy(b->d_fin_items, fin_items.data(), fin_items.size() * sizeof(SweepItem),
                        cudaMemcpyHostToDevice));
     MHD_TRY(cudaMemcpy(b->d_cg_items, cg_items.data(), cg_items.size() * sizeof(WorkItem),
                        cudaMemcpyHostToDevice));
@@ -181,7 +229,7 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
                            cudaMemcpyHostToDevice));
     b->stage_grid[0] = grid_for(b->stage_occ[0], b->num_sms, b->n_stage_items, SW_WARPS);
     b->stage_grid[1] = grid_for(b->stage_occ[1], b->num_sms, b->n_stage_items, SW_WARPS);
-    b->fin_grid = grid_for(b->fin_occ, b->num_sms, b->n_stage_items, FS_WARPS);
+    b->fin_grid = grid_for(b->fin_occ, b->num_sms, b->n_fin_items, FS_WARPS);
     b->cg_grid = grid_for(b->cg_occ, b->num_sms, max_chunk_items, CGS_NT / 32);
     b->tuning.stage_rows = t.stage_rows;
     b->tuning.cg_rows = t.cg_rows;
@@ -232,22 +280,22 @@ mhd_status enqueue_step(mhd_batch* b, const double* dt_in, double dt_fixed, int 
         b->rec_cap, b->queues, kQueues, b->syncs, 2 * b->nchunks);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[0], b->stream));
-    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, sweep_smem_bytes(1), b->stream>>>(I, b->d_sweep_items,
-                                                                        b->n_stage_items, b->queues);
+    k_stage_batch<1><<<b->stage_grid[0], 32 * SW_WARPS, sweep_smem_bytes(1), b->stream>>>(
+        I, b->d_sweep_items, b->n_stage_items, b->queues, b->stage_base[b->parity][0]);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[1], b->stream));
     mhd_status s = launch_cg_chunks(b, I, 0, record);
     if (s != MHD_OK) return s;
     if (ev) MHD_TRY(cudaEventRecord(ev[2], b->stream));
     k_stage_batch<2><<<b->stage_grid[1], 32 * SW_WARPS, sweep_smem_bytes(2), b->stream>>>(
-        I, b->d_sweep_items, b->n_stage_items, b->queues + 1);
+        I, b->d_sweep_items, b->n_stage_items, b->queues + 1, b->stage_base[b->parity][1]);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[3], b->stream));
     s = launch_cg_chunks(b, I, 1, record);
     if (s != MHD_OK) return s;
     if (ev) MHD_TRY(cudaEventRecord(ev[4], b->stream));
-    k_finalize_batch<<<b->fin_grid, 32 * FS_WARPS, 0, b->stream>>>(I, b->d_sweep_items, b->n_stage_items,
-                                                                   b->queues + 2);
+    k_finalize_batch<<<b->fin_grid, 32 * FS_WARPS, 0, b->stream>>>(I, b->d_fin_items, b->n_fin_items,
+                                                                   b->queues + 2, b->fin_base[b->parity]);
     MHD_TRY(cudaGetLastError());
     if (ev) MHD_TRY(cudaEventRecord(ev[5], b->stream));
     b->parity ^= 1;
@@ -372,10 +420,13 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
         cudaGetLastError();
         return fail(MHD_ERR_OUT_OF_MEMORY);
     }
-    // descriptors
+    // descriptors. The pool is plane-major: plane k (S 0-5, T 6-11, A 12-17, x, r0, r1, p0, p1)
+    // is one arena of total_cells zones, with instance i at the same zone offset in every arena.
     for (int p = 0; p < 2; ++p) b->h_insts[p].assign(count, BatchInst{});
-    double* q = b->pool;
+    const size_t tot = b->total_cells;
+    size_t off = 0;
     for (int i = 0; i < count; ++i) {
+        double* const q = b->pool + off;
         const mhd_params& p = b->prm[i];
         const size_t n = b->ncell[i];
         BatchInst I{};
@@ -387,14 +438,15 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
         I.D.ct_mode = p.ct_mode;
         I.C = b->coeffs + i;
         I.st = b->status + i;
-        for (int k = 0; k < 6; ++k) I.S[k] = q + (size_t)k * n;
-        for (int k = 0; k < 6; ++k) I.T[k] = q + (size_t)(6 + k) * n;
-        for (int k = 0; k < 6; ++k) I.A[k] = q + (size_t)(12 + k) * n;
-        I.x = q + 18 * n;
-        I.r[0] = q + 19 * n;
-        I.r[1] = q + 20 * n;
-        I.p[0] = q + 21 * n;
-        I.p[1] = q + 22 * n;
+        I.off = (long long)off;
+        for (int k = 0; k < 6; ++k) I.S[k] = q + (size_t)k * tot;
+        for (int k = 0; k < 6; ++k) I.T[k] = q + (size_t)(6 + k) * tot;
+        for (int k = 0; k < 6; ++k) I.A[k] = q + (size_t)(12 + k) * tot;
+        I.x = q + 18 * tot;
+        I.r[0] = q + 19 * tot;
+        I.r[1] = q + 20 * tot;
+        I.p[0] = q + 21 * tot;
+        I.p[1] = q + 22 * tot;
         I.max_iters = p.cg_max_iters > 0 ? p.cg_max_iters : 2LL * (long long)n;
         I.tol = p.cg_tol > 0 ? p.cg_tol : 2.220446049250313e-16;
         I.alpha = 0.0;
@@ -405,7 +457,28 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
         b->h_insts[0][i] = I;
         for (int k = 0; k < 4; ++k) std::swap(I.S[k], I.A[k]);  // odd steps
         b->h_insts[1][i] = I;
-        q += (size_t)kBatchPlanes * n;
+        off += n;
+    }
+    // the arenas are instance 0's planes (offset 0)
+    for (int p = 0; p < 2; ++p) {
+        const BatchInst& I0 = b->h_insts[p][0];
+        ParamPlanes& s1 = b->stage_base[p][0];
+        ParamPlanes& s2 = b->stage_base[p][1];
+        for (int k = 0; k < 6; ++k) {
+            s1.in_.f[k] = I0.S[k];
+            s1.a_.f[k] = I0.T[k];
+            s1.b_.f[k] = I0.A[k];
+            s2.in_.f[k] = I0.T[k];
+            s2.a_.f[k] = nullptr;
+            s2.b_.f[k] = I0.A[k];
+        }
+        s1.x_ = nullptr;
+        s2.x_ = I0.x;
+        FinParams& fp = b->fin_base[p];
+        for (int k = 0; k < 6; ++k) fp.acc_.f[k] = I0.A[k];
+        fp.x_ = I0.x;
+        fp.bx_ = I0.S[4];
+        fp.by_ = I0.S[5];
     }
     if (cudaMemsetAsync(b->status, 0, count * sizeof(DeviceStatus), b->stream) != cudaSuccess ||
         cudaMemsetAsync(b->coeffs, 0, count * sizeof(StepCoeffs), b->stream) != cudaSuccess ||
@@ -415,8 +488,8 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
             cudaSuccess)
         return fail(MHD_ERR_CUDA);
     mhd_batch_tuning t{};
-    t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", 256);
-    t.stage_tail_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_TAIL_ROWS", 32);
+    t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", balanced_stage_rows(b, 2));
+    t.stage_tail_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_TAIL_ROWS", 0);
     t.cg_rows = mhd_host::env_int("MHD_B200_BATCH_CG_ROWS", 32);
     t.cg_order = mhd_host::env_int("MHD_B200_BATCH_CG_ORDER", 0);
     const mhd_status s = apply_tuning(b, t);
@@ -657,20 +730,25 @@ mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
         return MHD_OK;
     };
     if ((s = planes_copy(true)) != MHD_OK) return s;
-    constexpr int nst = sizeof(kStageCand) / sizeof(kStageCand[0]);
+    // explicit-stage candidates: the fixed list and items that fill 1-4 or 6 waves exactly
+    std::vector<std::pair<int, int>> stage_cand;
+    for (const auto& c : kStageCand) stage_cand.emplace_back(c[0], c[1]);
+    for (int waves : {1, 2, 3, 4, 6}) stage_cand.emplace_back(balanced_stage_rows(b, waves), 0);
+    const int nst = (int)stage_cand.size();
     constexpr int ncg = sizeof(kCgRowsCand) / sizeof(int);
     double best_stage = 1e300, best_cg = 1e300;
     int best_stage_rows = before.stage_rows, best_tail = before.stage_tail_rows;
     int best_cg_rows = before.cg_rows, best_order = before.cg_order;
-    // trial -1 warms the kernels up; trials 0 .. 2*ncg-1 cover every solver candidate (both dealing
-    // orders) and every explicit-stage candidate
-    for (int trial = -1; trial < 2 * ncg; ++trial) {
+    // trial -1 warms the kernels up; the others cover every solver candidate (both dealing orders)
+    // and every explicit-stage candidate
+    const int ntrials = std::max(nst, 2 * ncg);
+    for (int trial = -1; trial < ntrials; ++trial) {
         mhd_batch_tuning t{};
         const int tk = std::max(trial, 0);
-        t.stage_rows = kStageCand[tk % nst][0];
-        t.stage_tail_rows = kStageCand[tk % nst][1];
+        t.stage_rows = stage_cand[tk % nst].first;
+        t.stage_tail_rows = stage_cand[tk % nst].second;
         t.cg_rows = kCgRowsCand[tk % ncg];
-        t.cg_order = tk / ncg;
+        t.cg_order = (tk / ncg) & 1;
         if ((s = apply_tuning(b, t)) != MHD_OK) return s;
         if ((s = enqueue_step(b, nullptr, 0.0, 1, 0.0, false, ev)) != MHD_OK) return s;
         MHD_TRY(cudaStreamSynchronize(b->stream));

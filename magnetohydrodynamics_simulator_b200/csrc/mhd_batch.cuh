@@ -30,7 +30,7 @@ struct BatchInst {
     double* x;
     double* r[2];
     double* p[2];
-    SweepGeom sg;  // explicit stages and finalize (SW_OUT == FS_OUT columns per strip)
+    long long off;  // zone offset of the instance in every plane arena
     int cg_strips_x, cg_seg_h;
     long long max_iters;
     double tol;
@@ -95,52 +95,84 @@ __device__ __forceinline__ int batch_next_item(int* queue) {
     return __shfl_sync(0xffffffffu, it, 0);
 }
 
+// Stage 2 of the batch forms its y slopes per face: the carried slopes (10 registers) push the
+// persistent kernel, which holds an item loop around the sweep, into spills (measured on B200:
+// 4096^2 explicit stages 0.169 -> 0.161 ns per zone, 16 x 1024^2 0.161 -> 0.151).
+#ifndef MHD_BATCH_YREUSE_2
+#define MHD_BATCH_YREUSE_2 0
+#endif
+#ifndef MHD_BATCH_XREUSE_2
+#define MHD_BATCH_XREUSE_2 MHD_SWEEP_XREUSE_2
+#endif
+// Explicit stage MODE of the batch. base: the arenas of this step's parity (stage 1: in = state,
+// a = predictor, b = accumulator; stage 2: in = predictor, x = E1, b = accumulator).
 template <int MODE>
 __global__ void __launch_bounds__(32 * SW_WARPS, MODE == 1 ? MHD_SWEEP_MIN_BLOCKS_1 : MHD_SWEEP_MIN_BLOCKS_2)
 k_stage_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__ items, int nitems,
-              int* queue) {
+              int* queue, ParamPlanes base) {
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double sw_ring_mem[];
 #else
     static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];
 #endif
-    __shared__ SweepPtrTable tab[SW_WARPS];
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    __shared__ SweepInstRec rec[SW_WARPS];
+    const int wl = threadIdx.x >> 5;
     double* const ring = sw_ring_mem + (size_t)wl * SW_RING * SW_SLOT;
-    SweepPtrTable& t = tab[wl];
-    const SmemPlanes pl{&t};
+    const RecPlanes pl{base, &rec[wl]};
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
         const SweepItem e = items[it];
         const BatchInst& I = insts[e.inst];
-        __syncwarp();  // the previous item's sweep has read its table
-        if (lane < 6) {
-            t.in[lane] = (MODE == 1) ? I.S[lane] : I.T[lane];
-            t.a[lane] = I.T[lane];
-            t.b[lane] = I.A[lane];
-        } else if (lane == 6) {
-            t.x = (MODE == 1) ? nullptr : I.x;
+        __syncwarp();  // the previous item's sweep has read the record
+        if ((threadIdx.x & 31) == 0) {
+            rec[wl].D = I.D;
+            rec[wl].off = I.off;
         }
         __syncwarp();
-        const Domain D = I.D;
-        stage_sweep_warp<MODE>(D, I.C, pl, e.sx, e.r0, e.r1, ring);
+        stage_sweep_warp<MODE, RecPlanes, MODE == 1 ? MHD_SWEEP_YREUSE_1 : MHD_BATCH_YREUSE_2,
+                         MODE == 1 ? MHD_SWEEP_XREUSE_1 : MHD_BATCH_XREUSE_2>(I.C, pl, e.sx, e.r0,
+                                                                              e.r1, ring);
     }
 }
 
+// RecFin: the finalize's view of one batch instance (arena bases in kernel parameters, the
+// instance's offset and grid in the warp's shared record; see RecPlanes).
+struct RecFin {
+    FinParams base;
+    const SweepInstRec* rec;
+    __device__ __forceinline__ size_t off() const { return (size_t)RecPlanes::vload(&rec->off); }
+    __device__ __forceinline__ double* acc(int q) const { return base.acc_.f[q] + off(); }
+    __device__ __forceinline__ const double* x() const { return base.x_ + off(); }
+    __device__ __forceinline__ double* bx() const { return base.bx_ + off(); }
+    __device__ __forceinline__ double* by() const { return base.by_ + off(); }
+    __device__ __forceinline__ int nx() const { return RecPlanes::vload(&rec->D.nx); }
+    __device__ __forceinline__ int ny() const { return RecPlanes::vload(&rec->D.ny); }
+    __device__ __forceinline__ double dx() const { return RecPlanes::vload(&rec->D.dx); }
+    __device__ __forceinline__ double dy() const { return RecPlanes::vload(&rec->D.dy); }
+    __device__ __forceinline__ double eta() const { return RecPlanes::vload(&rec->D.eta); }
+};
+
+// Finalize of the batch. base: the arenas of this step's parity (acc = accumulator, x = E2,
+// bx / by = the state's face planes).
 static __global__ void __launch_bounds__(32 * FS_WARPS)
 k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__ items, int nitems,
-                 int* queue) {
+                 int* queue, FinParams base) {
+    __shared__ SweepInstRec rec[FS_WARPS];
+    const int wl = threadIdx.x >> 5;
+    const RecFin f{base, &rec[wl]};
     for (;;) {
         const int it = batch_next_item(queue);
         if (it >= nitems) break;
         const SweepItem e = items[it];
         const BatchInst& I = insts[e.inst];
-        Planes acc;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) acc.f[q] = I.A[q];
-        const Domain D = I.D;
-        finalize_sweep_warp(D, I.C, acc, I.x, I.S[4], I.S[5], I.st, e.sx, e.r0, e.r1);
+        __syncwarp();  // the previous item's sweep has read the record
+        if ((threadIdx.x & 31) == 0) {
+            rec[wl].D = I.D;
+            rec[wl].off = I.off;
+        }
+        __syncwarp();
+        finalize_sweep_warp(f, I.C, I.st, e.sx, e.r0, e.r1);
     }
 }
 

@@ -18,14 +18,34 @@ constexpr int FS_OUT = 28;
 constexpr int FS_WARPS = 8;
 constexpr int FS_PRE = 3;  // rows swept before the first output row
 
+// A finalize sweep reaches its grid through an accessor FA: acc(q) the accumulator planes (U2*),
+// x() the second solve's corner field E2, bx() / by() the face planes of U^{n+1}, and nx(), ny(),
+// dx(), dy(), eta() as the stage sweeps' accessors.
+//
+// FinParams: everything in kernel parameters.
+struct FinParams {
+    Planes acc_;
+    const double* x_;
+    double* bx_;
+    double* by_;
+    Domain D_;
+    __device__ __forceinline__ double* acc(int q) const { return acc_.f[q]; }
+    __device__ __forceinline__ const double* x() const { return x_; }
+    __device__ __forceinline__ double* bx() const { return bx_; }
+    __device__ __forceinline__ double* by() const { return by_; }
+    __device__ __forceinline__ int nx() const { return D_.nx; }
+    __device__ __forceinline__ int ny() const { return D_.ny; }
+    __device__ __forceinline__ double dx() const { return D_.dx; }
+    __device__ __forceinline__ double dy() const { return D_.dy; }
+    __device__ __forceinline__ double eta() const { return D_.eta; }
+};
+
 // The sweep of one warp over rows [r0, r1) of column strip sx of one grid.
-__device__ __forceinline__ void finalize_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
-                                                    const Planes& acc, const double* __restrict__ xsolve,
-                                                    double* __restrict__ bx_out,
-                                                    double* __restrict__ by_out, DeviceStatus* st,
-                                                    int sx, int r0, int r1) {
+template <class FA>
+__device__ __forceinline__ void finalize_sweep_warp(const FA& f, const StepCoeffs* __restrict__ C,
+                                                    DeviceStatus* st, int sx, int r0, int r1) {
     const int lane = threadIdx.x & 31;
-    const int nx = D.nx, ny = D.ny;
+    const int nx = f.nx();  // setup only: the loop reads the grid through f
     const int c0 = sx * FS_OUT;
     if (r0 >= r1) return;
     const int i = c0 - 1 + lane;
@@ -33,17 +53,17 @@ __device__ __forceinline__ void finalize_sweep_warp(const Domain& D, const StepC
     const bool out_lane = lane >= 1 && lane <= FS_OUT && i < nx;
     const double cg = C->c_g;
     // quotients by dx, dy as products with the hoisted reciprocals (within 1 ulp)
-    const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
-    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
+    const double idx = 1.0 / f.dx(), idy = 1.0 / f.dy();
+    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, f.ny()) * f.nx(); };
     auto sdn = [](double v) { return __shfl_down_sync(0xffffffffu, v, 1); };
     auto sup = [](double v) { return __shfl_up_sync(0xffffffffu, v, 1); };
 
     const int cstart = r0 - FS_PRE;
     // pipelines
-    double x_cur = __ldg(&xsolve[rowp(cstart + 2) + iw]);  // E2 row c+2
-    double x_in = __ldg(&xsolve[rowp(cstart + 3) + iw]);   // E2 row c+3 (arriving)
-    double b0x_in = acc.f[4][rowp(cstart + 2) + iw];       // U2*_B row c+2 (arriving)
-    double b0y_in = acc.f[5][rowp(cstart + 2) + iw];
+    double x_cur = __ldg(&f.x()[rowp(cstart + 2) + iw]);  // E2 row c+2
+    double x_in = __ldg(&f.x()[rowp(cstart + 3) + iw]);   // E2 row c+3 (arriving)
+    double b0x_in = f.acc(4)[rowp(cstart + 2) + iw];      // U2*_B row c+2 (arriving)
+    double b0y_in = f.acc(5)[rowp(cstart + 2) + iw];
     double b0x[2] = {0.0, 0.0}, b0y[2] = {0.0, 0.0};       // U2*_B rows c, c+1
     double bx2_prev = 0.0;                                 // B2_x row c+1
     double e3_prev = 0.0;                                  // E3 row c+1
@@ -57,31 +77,31 @@ __device__ __forceinline__ void finalize_sweep_warp(const Domain& D, const StepC
         const double ux = b0x_in, uy = b0y_in;  // U2*_B row c+2
         // issue the next row's loads
         x_cur = xa;
-        x_in = __ldg(&xsolve[rowp(c + 4) + iw]);
-        b0x_in = acc.f[4][rowp(c + 3) + iw];
-        b0y_in = acc.f[5][rowp(c + 3) + iw];
+        x_in = __ldg(&f.x()[rowp(c + 4) + iw]);
+        b0x_in = f.acc(4)[rowp(c + 3) + iw];
+        b0y_in = f.acc(5)[rowp(c + 3) + iw];
         double h_nx[4] = {0.0, 0.0, 0.0, 0.0};
         if (out_lane && c + 1 >= r0 && c + 1 < r1) {
-            const size_t g = (size_t)(c + 1) * nx + i;
+            const size_t g = (size_t)(c + 1) * f.nx() + i;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) h_nx[q] = acc.f[q][g];
+            for (int q = 0; q < 4; ++q) h_nx[q] = f.acc(q)[g];
         }
         // B2 of row c+2 (x neighbour of E2 from the next lane)
         const double bx2 = ux + (-(xa - xb) * idy) * cg;
         const double by2 = uy + ((sdn(xb) - xb) * idx) * cg;
         // E3 of row c+2
-        const double e3 = D.eta * ((by2 - sup(by2)) * idx - (bx2 - bx2_prev) * idy);
+        const double e3 = f.eta() * ((by2 - sup(by2)) * idx - (bx2 - bx2_prev) * idy);
         // B^{n+1} of row c+1
         const double bnx = b0x[1] + (-(e3 - e3_prev) * idy) * cg;
         const double bny = b0y[1] + ((sdn(e3_prev) - e3_prev) * idx) * cg;
         // outputs of row c: B^{n+1}, density floor, CFL speed
         const double bnx_right = sdn(bnx_prev);
         if (out_lane && c >= r0 && c < r1) {
-            const size_t g = (size_t)c * nx + i;
-            bx_out[g] = bnx_prev;
-            by_out[g] = bny_prev;
+            const size_t g = (size_t)c * f.nx() + i;
+            f.bx()[g] = bnx_prev;
+            f.by()[g] = bny_prev;
             double rho = h_cur[0];
-            if (rho < kRhoFloor) acc.f[0][g] = kRhoFloor;
+            if (rho < kRhoFloor) f.acc(0)[g] = kRhoFloor;
             const double bxc = (bnx_prev + bnx_right) / 2.0;
             const double byc = (bny_prev + bny) / 2.0;
             double vx, vy;
@@ -117,7 +137,8 @@ k_finalize_sweep(Domain D, const StepCoeffs* __restrict__ C, Planes acc,
     if (w >= G.nwarps) return;
     const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int r0 = sy * G.seg_h;
-    finalize_sweep_warp(D, C, acc, xsolve, bx_out, by_out, st, sx, r0, min(r0 + G.seg_h, D.ny));
+    const FinParams f{acc, xsolve, bx_out, by_out, D};
+    finalize_sweep_warp(f, C, st, sx, r0, min(r0 + G.seg_h, D.ny));
 }
 
 }  // namespace mhd

@@ -74,54 +74,74 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 // Where a sweep finds its planes: in(q) the six input planes, x() the corner field E1 (stage 2),
 // a(q) / b(q) the two output plane sets (stage 1: predictor / accumulator; stage 2: - /
 // accumulator, read and written).
-// ParamPlanes: kernel parameters (constant bank; no registers held).
+// A sweep reaches its grid through an accessor PL:
+//   in(q) the six input planes, x() the corner field E1 (stage 2), a(q) / b(q) the two output
+//   plane sets (stage 1: predictor / accumulator; stage 2: - / accumulator, read and written);
+//   nx(), ny(), dx(), dy(), eta(), ct_mode() the grid's size, spacing, resistivity and CT mode.
+//
+// ParamPlanes: everything in kernel parameters (constant bank; nothing has to stay in registers).
 struct ParamPlanes {
     CPlanes in_;
     const double* x_;
     Planes a_, b_;
+    Domain D_;
     __device__ __forceinline__ const double* in(int q) const { return in_.f[q]; }
     __device__ __forceinline__ const double* x() const { return x_; }
     __device__ __forceinline__ double* a(int q) const { return a_.f[q]; }
     __device__ __forceinline__ double* b(int q) const { return b_.f[q]; }
+    __device__ __forceinline__ int nx() const { return D_.nx; }
+    __device__ __forceinline__ int ny() const { return D_.ny; }
+    __device__ __forceinline__ double dx() const { return D_.dx; }
+    __device__ __forceinline__ double dy() const { return D_.dy; }
+    __device__ __forceinline__ double eta() const { return D_.eta; }
+    __device__ __forceinline__ int ct_mode() const { return D_.ct_mode; }
 };
-// SmemPlanes: a per-warp copy of an instance's pointers in shared memory, read with a volatile
-// load at each use, so that a persistent kernel stepping many instances keeps none of them live in
-// registers (18 pointers would cost 36 registers per thread).
-struct SweepPtrTable {
-    const double* in[6];
-    const double* x;
-    double* a[6];
-    double* b[6];
+
+// Per-warp record of the instance a batch warp is sweeping (shared memory).
+struct SweepInstRec {
+    Domain D;
+    long long off;  // zone offset of the instance in every plane arena
 };
-struct SmemPlanes {
-    const SweepPtrTable* t;
+// RecPlanes: one instance of a batch whose planes are arenas holding every instance at the same
+// zone offset. The arena bases are kernel parameters; the instance's offset and grid live in the
+// warp's shared record and are read (volatile) where they are used, so that a persistent kernel
+// stepping many instances holds none of them in registers across its sweep.
+struct RecPlanes {
+    ParamPlanes base;
+    const SweepInstRec* rec;
     template <class T>
     __device__ __forceinline__ static T vload(T const* p) {
         return *static_cast<T const volatile*>(p);
     }
-    __device__ __forceinline__ const double* in(int q) const { return vload(&t->in[q]); }
-    __device__ __forceinline__ const double* x() const { return vload(&t->x); }
-    __device__ __forceinline__ double* a(int q) const { return vload(&t->a[q]); }
-    __device__ __forceinline__ double* b(int q) const { return vload(&t->b[q]); }
+    __device__ __forceinline__ size_t off() const { return (size_t)vload(&rec->off); }
+    __device__ __forceinline__ const double* in(int q) const { return base.in_.f[q] + off(); }
+    __device__ __forceinline__ const double* x() const { return base.x_ + off(); }
+    __device__ __forceinline__ double* a(int q) const { return base.a_.f[q] + off(); }
+    __device__ __forceinline__ double* b(int q) const { return base.b_.f[q] + off(); }
+    __device__ __forceinline__ int nx() const { return vload(&rec->D.nx); }
+    __device__ __forceinline__ int ny() const { return vload(&rec->D.ny); }
+    __device__ __forceinline__ double dx() const { return vload(&rec->D.dx); }
+    __device__ __forceinline__ double dy() const { return vload(&rec->D.dy); }
+    __device__ __forceinline__ double eta() const { return vload(&rec->D.eta); }
+    __device__ __forceinline__ int ct_mode() const { return vload(&rec->D.ct_mode); }
 };
 
 // The sweep of one warp over rows [r0, r1) of column strip sx of one grid.
-template <int MODE, class PL>
-__device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoeffs* __restrict__ C,
-                                                 const PL& pl, int sx, int r0, int r1,
-                                                 double* ring) {
+template <int MODE, class PL, bool kYReuse = (MODE == 1) ? MHD_SWEEP_YREUSE_1 : MHD_SWEEP_YREUSE_2,
+          bool kXReuse = (MODE == 1) ? MHD_SWEEP_XREUSE_1 : MHD_SWEEP_XREUSE_2>
+__device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ C, const PL& pl,
+                                                 int sx, int r0, int r1, double* ring) {
     const int lane = threadIdx.x & 31;
-    const int nx = D.nx, ny = D.ny;
+    const int nx = pl.nx();  // setup only: the loop reads the grid through pl
     const int c0 = sx * SW_OUT;
     if (r0 >= r1) return;
-    // limited slopes formed once per cell (y: carried to the next row; x: shared with the lane on
-    // the left), or per face as the reference writes them -- the same operands either way
-    constexpr bool kYReuse = (MODE == 1) ? MHD_SWEEP_YREUSE_1 : MHD_SWEEP_YREUSE_2;
-    constexpr bool kXReuse = (MODE == 1) ? MHD_SWEEP_XREUSE_1 : MHD_SWEEP_XREUSE_2;
+    // kYReuse / kXReuse: limited slopes formed once per cell (y: carried to the next row; x: shared
+    // with the lane on the left), or per face as the reference writes them -- the same operands
+    // either way
     const int i = c0 - 2 + lane;
     const int iw = wrap(i, nx);
     const bool out_lane = lane >= 2 && lane < 2 + SW_OUT && i < nx;
-    const double idx = 1.0 / D.dx, idy = 1.0 / D.dy;
+    const double idx = 1.0 / pl.dx(), idy = 1.0 / pl.dy();
     const double cg = C->c_g;
     const double cA = (MODE == 1) ? C->c_g : C->c_1md;   // outA weight (stage 1: predictor)
     const double cB = (MODE == 1) ? C->c_d : C->c_1md;   // outB weight
@@ -129,7 +149,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
     // column of the lane to the right (for stage 2's B1 of lane 31)
     const int iw_r = wrap(i + 1, nx);
 
-    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, ny) * nx; };
+    auto rowp = [&](int j) -> size_t { return (size_t)wrap(j, pl.ny()) * pl.nx(); };
 
     // ---- windows (index 0 = oldest row)
     double Prho[4], Pvx[4], Pvy[4], Pp[4], Pbxc[4];  // rows c-1 .. c+2
@@ -190,12 +210,12 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             if (lane == 31) s3[192] = s3[192] + (-(s4[SW_E1 + 32] - s3[SW_E1 + 32]) * idy) * cg;
             if (out_lane) {
                 if (c >= r0 && c < r1) {
-                    const size_t g = (size_t)c * nx + i;
+                    const size_t g = (size_t)c * pl.nx() + i;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) accH[q] = pl.b(q)[g];
                 }
                 if (c - 1 >= r0 && c - 1 < r1) {
-                    const size_t g = (size_t)(c - 1) * nx + i;
+                    const size_t g = (size_t)(c - 1) * pl.nx() + i;
                     accB[0] = pl.b(4)[g];
                     accB[1] = pl.b(5)[g];
                 }
@@ -300,14 +320,14 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             const double eW = shup(fy_prev[4], 1);
             const double vxc = 0.25 * (Pvx[1] + shup(Pvx[1], 1) + Pvx[0] + shup(Pvx[0], 1));
             const double vyc = 0.25 * (Pvy[1] + shup(Pvy[1], 1) + Pvy[0] + shup(Pvy[0], 1));
-            ez = corner_ez(eN, eS, eE, eW, vxc, vyc, D.ct_mode);
+            ez = corner_ez(eN, eS, eE, eW, vxc, vyc, pl.ct_mode());
         }
         double jz = 0.0;
         if (MODE == 2) {  // eta*J_z(B1) at corner (i, c) (solvers.hpp:450-461)
             const double by1 = slot(c)[5 * 32 + lane];
             const double dBy_dx = (by1 - shup(by1, 1)) * idx;
             const double dBx_dy = (slot(c)[4 * 32 + lane] - slot(c - 1)[4 * 32 + lane]) * idy;
-            jz = D.eta * (dBy_dx - dBx_dy);
+            jz = pl.eta() * (dBy_dx - dBx_dy);
         }
         // ---- hydro rates of row c
         {
@@ -317,7 +337,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
             f[2] = -((fx.my - shup(fx.my, 1)) * idx + (fy.my - fy_prev[2]) * idy);
             f[3] = -((fx.E - shup(fx.E, 1)) * idx + (fy.E - fy_prev[3]) * idy);
             if (out_lane && c >= r0 && c < r1) {
-                const size_t g = (size_t)c * nx + i;
+                const size_t g = (size_t)c * pl.nx() + i;
                 if constexpr (MODE == 1) {
                     const double* sc = slot(c);
 #pragma unroll
@@ -343,7 +363,7 @@ __device__ __forceinline__ void stage_sweep_warp(const Domain& D, const StepCoef
                 g2y = (shdn(jz_prev, 1) - jz_prev) * idx;
             }
             if (out_lane && c - 1 >= r0 && c - 1 < r1) {
-                const size_t g = (size_t)(c - 1) * nx + i;
+                const size_t g = (size_t)(c - 1) * pl.nx() + i;
                 if constexpr (MODE == 1) {
                     const double* sp = slot(c - 1);
                     const double ubx = sp[4 * 32 + lane], uby = sp[5 * 32 + lane];  // U^n faces, row c-1
@@ -388,10 +408,10 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
     double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
     const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
-    const ParamPlanes pl{in, xsolve, outA, outB};
+    const ParamPlanes pl{in, xsolve, outA, outB, D};
     const int sx = w % G.strips_x, sy = w / G.strips_x;
     const int r0 = sy * G.seg_h;
-    stage_sweep_warp<MODE>(D, C, pl, sx, r0, min(r0 + G.seg_h, D.ny), ring);
+    stage_sweep_warp<MODE>(C, pl, sx, r0, min(r0 + G.seg_h, D.ny), ring);
 }
 
 }  // namespace mhd
