@@ -52,17 +52,14 @@ struct mhd_batch {
     int parity = 0;  // descriptor array of the next step
     ParamPlanes stage_base[2][2];  // [parity][stage - 1]: plane arenas of the explicit stages
     FinParams fin_base[2];         // [parity]: plane arenas of the finalize
-    // work items: explicit stages / finalize, then the solver's (chunk by chunk)
+    // work items of the explicit stages and of the finalize (the solver numbers its own)
     void* d_items_mem = nullptr;          // both lists in one allocation
     SweepItem* d_sweep_items = nullptr;  // explicit stages
     SweepItem* d_fin_items = nullptr;    // finalize
-    WorkItem* d_cg_items = nullptr;      // solver, chunk by chunk
     size_t items_cap = 0;                // bytes
     int n_stage_items = 0;
     int n_fin_items = 0;
-    int n_cg_items = 0;
     int nchunks = 0;
-    std::vector<int> chunk_item0, chunk_nitems;
     int stage_occ[2] = {0, 0}, fin_occ = 0, cg_occ = 0;
     int stage_grid[2] = {0, 0}, fin_grid = 0, cg_grid = 0;
     double* partials = nullptr;  // [2][CGB_MAX_INST][cg_occ * num_sms][4]
@@ -181,33 +178,17 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
             I.cg_seg_h = cg_seg;
         }
     }
-    // solver items, chunk by chunk
-    std::vector<WorkItem> cg_items;
-    b->chunk_item0.assign(b->nchunks, 0);
-    b->chunk_nitems.assign(b->nchunks, 0);
+    // the solver kernel numbers its items itself; its grid covers the largest chunk's items
     int max_chunk_items = 0;
     for (int c = 0; c < b->nchunks; ++c) {
         const int i0 = c * CGB_MAX_INST, i1 = std::min(b->count, i0 + CGB_MAX_INST);
-        b->chunk_item0[c] = (int)cg_items.size();
-        const size_t before = cg_items.size();
-        if (t.cg_order == 0) {
-            for (int i = i0; i < i1; ++i)
-                for (int w = 0; w < cg_nw[i]; ++w) cg_items.push_back(WorkItem{i, w});
-        } else {
-            int most = 0;
-            for (int i = i0; i < i1; ++i) most = std::max(most, cg_nw[i]);
-            for (int w = 0; w < most; ++w)
-                for (int i = i0; i < i1; ++i)
-                    if (w < cg_nw[i]) cg_items.push_back(WorkItem{i, w});
-        }
-        b->chunk_nitems[c] = (int)(cg_items.size() - before);
-        max_chunk_items = std::max(max_chunk_items, b->chunk_nitems[c]);
+        int n = 0;
+        for (int i = i0; i < i1; ++i) n += cg_nw[i];
+        max_chunk_items = std::max(max_chunk_items, n);
     }
     b->n_stage_items = (int)st_items.size();
     b->n_fin_items = (int)fin_items.size();
-    b->n_cg_items = (int)cg_items.size();
-    const size_t bytes = (st_items.size() + fin_items.size()) * sizeof(SweepItem) +
-                         cg_items.size() * sizeof(WorkItem);
+    const size_t bytes = (st_items.size() + fin_items.size()) * sizeof(SweepItem);
     if (bytes > b->items_cap) {
         cudaFree(b->d_items_mem);
         b->d_items_mem = nullptr;
@@ -217,12 +198,9 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     }
     b->d_sweep_items = static_cast<SweepItem*>(b->d_items_mem);
     b->d_fin_items = b->d_sweep_items + st_items.size();
-    b->d_cg_items = reinterpret_cast<WorkItem*>(b->d_fin_items + fin_items.size());
     MHD_TRY(cudaMemcpy(b->d_sweep_items, st_items.data(), st_items.size() * sizeof(SweepItem),
                        cudaMemcpyHostToDevice));
     MHD_TRY(cudaMemcpy(b->d_fin_items, fin_items.data(), fin_items.size() * sizeof(SweepItem),
-                       cudaMemcpyHostToDevice));
-    MHD_TRY(cudaMemcpy(b->d_cg_items, cg_items.data(), cg_items.size() * sizeof(WorkItem),
                        cudaMemcpyHostToDevice));
     for (int p = 0; p < 2; ++p)
         MHD_TRY(cudaMemcpy(b->d_insts[p], b->h_insts[p].data(), b->count * sizeof(BatchInst),
@@ -244,8 +222,7 @@ mhd_status launch_cg_chunks(mhd_batch* b, const BatchInst* insts, int solve, boo
         a.insts = insts;
         a.inst0 = c * CGB_MAX_INST;
         a.ninst = std::min(CGB_MAX_INST, b->count - a.inst0);
-        a.items = b->d_cg_items + b->chunk_item0[c];
-        a.nitems = b->chunk_nitems[c];
+        a.order = b->tuning.cg_order;
         a.partials = b->partials;
         a.sync = b->syncs + 2 * c + solve;
         a.solve_index = solve;

@@ -4,11 +4,11 @@
 // matrix coefficient and its own convergence, exactly as if it were stepped alone
 // (integrator_main.cpp:76-112 per instance).
 //
-// Work is described by flat lists of warp work items: (instance, strip, rows) for the explicit
-// stages and the finalize (28-column strips, any row ranges), (instance, item) for the solver
-// (its strip/segment decomposition, 28-column strips of cg_seg_h rows). The explicit kernels are persistent and
-// pull items from a global counter (largest items first). The solver kernel deals its items to
-// warps in a fixed order, because its sums must be reduced in a fixed order.
+// The explicit stages and the finalize work on flat lists of warp work items (instance, strip,
+// rows): 28-column strips cut into row ranges. Their kernels are persistent and pull items from a
+// global counter (largest items first). The solver's items are each instance's strip/segment
+// decomposition (28-column strips of cg_seg_h rows); its kernel deals the items of the instances
+// still iterating to warps in a fixed order, because its sums must be reduced in a fixed order.
 //
 // The descriptor array exists twice, for even and odd steps: the finalize leaves U^{n+1}'s hydro
 // planes in the accumulator, so the state and accumulator hydro pointers trade places every step.
@@ -40,11 +40,6 @@ struct BatchInst {
     double hmin, courant, safety;
 };
 
-// Work item of the solver: item w of the instance's strip/segment decomposition.
-struct WorkItem {
-    int inst;
-    int w;
-};
 // Work item of the explicit stages and the finalize: rows [r0, r1) of column strip sx.
 struct SweepItem {
     int inst;
@@ -181,13 +176,15 @@ k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restric
 // kernel, running their phases in lockstep (solvers.hpp:404-489 per instance, Eigen's
 // ConjugateGradient defaults as in k_cg_sweep).
 //
-// The items of all instances (instance-major) are dealt to the grid's warps in a fixed
-// round-robin order, so each instance is spread over all SMs and stays spread while the others
-// converge. In a phase every warp sums its partials per instance (item order), each block sums
-// its warps per instance (warp order) and publishes one partial per (instance, block); after the
-// grid barrier every block reduces each instance's block partials in the same fixed order, so all
-// blocks hold identical scalars and take identical decisions. Instances that converged (or whose
-// right-hand side vanished) skip their items; the loop ends when no instance is active.
+// In every phase the items of the instances still iterating (instance-major) are numbered
+// 0 .. n-1 through a prefix sum of their item counts, which every block rebuilds from the same
+// decisions, and dealt to the grid's warps in a fixed order (order 0: round robin, 1: contiguous
+// runs). So the work of a phase is spread evenly over all warps whichever instances remain, and the
+// sums keep a fixed order: every warp sums its partials per instance (item order), each block
+// sums its warps per instance (warp order) and publishes one partial per (instance, block); after
+// the grid barrier every block reduces each instance's block partials in the same fixed order, so
+// all blocks hold identical scalars and take identical decisions. The loop ends when no instance
+// is active.
 
 constexpr int CGB_MAX_INST = 64;
 
@@ -199,14 +196,13 @@ struct CgBInst {
     double bb, absNew, thr, rr, pAp;
     long long products;
     int status;
-    int pad;
+    int nitems;  // solver items of the instance (strips x row segments)
 };
 
 struct CgBatchArgs {
     const BatchInst* insts;  // descriptors of this step's parity
     int inst0, ninst;        // instances [inst0, inst0 + ninst) of this launch
-    const WorkItem* items;   // their solver items, instance-major
-    int nitems;
+    int order;               // item dealing: 0 round robin, 1 contiguous runs
     double* partials;        // [2][CGB_MAX_INST][gridDim.x][4]
     CgSync* sync;
     int solve_index;         // 0: B* = U1*_B (T planes), 1: B* = U2*_B (A planes)
@@ -231,11 +227,48 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     return g;
 }
 
+// Solver item w of instance inst.
+struct CgItem {
+    int inst;
+    int w;
+};
+
+// This warp's share of items 0 .. total-1: j = first, then j += step while j < end.
+__device__ __forceinline__ void cgb_deal(int order, int total, int& j, int& end, int& step) {
+    constexpr int NW = CGS_NT / 32;
+    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
+    if (order == 0) {
+        j = gw;
+        end = total;
+        step = nw;
+    } else {
+        const int q = (total + nw - 1) / nw;
+        j = min(total, gw * q);
+        end = min(total, j + q);
+        step = 1;
+    }
+}
+
+// Prefix sum over the chunk's instances of the item counts of those with pick(status) (thread 0),
+// then a block barrier. Every block computes the same prefix from the same statuses.
+template <class Pick>
+__device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, int* pref, Pick pick) {
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int li = 0; li < ninst; ++li) {
+            pref[li] = s;
+            if (pick(sh[li].status)) s += sh[li].nitems;
+        }
+        pref[ninst] = s;
+    }
+    __syncthreads();
+}
+
 // One sweep over this warp's items: PH 0 the right-hand side (cg_rhs_segment), 1 the first
 // iteration, 2 a later one (cg_iter_segment); NV sums per instance. Ends with the block's partials
 // of every instance published in part_out.
 template <int PH, int NV>
-__device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh,
+__device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const int* pref,
                                           double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
     constexpr int NW = CGS_NT / 32;
@@ -245,10 +278,11 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         for (int c = 0; c < NV; ++c) wsum[wid][li][c] = 0.0;
     __syncwarp();
     const bool odd = (k & 1) != 0;
-    for (int it = blockIdx.x * NW + wid; it < a.nitems; it += gridDim.x * NW) {
-        const WorkItem e = a.items[it];
-        const int li = e.inst - a.inst0;
-        if (PH != 0 && sh[li].status != kCgActive) continue;
+    int j, jend, jstep;
+    cgb_deal(a.order, pref[a.ninst], j, jend, jstep);
+    for (int li = 0; j < jend; j += jstep) {
+        while (pref[li + 1] <= j) ++li;  // j only grows: li advances over the prefix once
+        const CgItem e{a.inst0 + li, j - pref[li]};
         const BatchInst& I = a.insts[e.inst];
         const CgSweepArgs g = cgb_args(a, I);
         CgScal s;
@@ -307,6 +341,7 @@ k_cg_batch(CgBatchArgs a) {
     constexpr int NW = CGS_NT / 32;
     __shared__ CgBInst sh[CGB_MAX_INST];
     __shared__ double wsum[NW][CGB_MAX_INST][4];
+    __shared__ int pref[CGB_MAX_INST + 1];
     __shared__ int sflag;
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double cg_ring_mem[];
@@ -344,11 +379,14 @@ k_cg_batch(CgBatchArgs a) {
         S.products = 0;
         S.rr = 0.0;
         S.status = kCgActive;
+        S.nitems = I.cg_strips_x * ((I.D.ny + I.cg_seg_h - 1) / I.cg_seg_h);
     }
     __syncthreads();
+    auto is_active = [](int st) { return st == kCgActive; };
 
     // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
-    cgb_phase<0, 3>(a, sh, wsum, ring, 0, dir, part(phase));
+    cgb_prefix(sh, a.ninst, pref, is_active);
+    cgb_phase<0, 3>(a, sh, pref, wsum, ring, 0, dir, part(phase));
     if (!barrier_or_quit()) return;
     for (int li = wid; li < a.ninst; li += NW) {
         double v[3];
@@ -372,8 +410,9 @@ k_cg_batch(CgBatchArgs a) {
 
     for (int k = 0;; ++k) {
         // ---- iteration k: p_k, q_k, x_{k+1}, r_{k+1}; r.r, r.z, z.Az, z.q_k
-        if (k == 0) cgb_phase<1, 4>(a, sh, wsum, ring, k, dir, part(phase));
-        else cgb_phase<2, 4>(a, sh, wsum, ring, k, dir, part(phase));
+        cgb_prefix(sh, a.ninst, pref, is_active);
+        if (k == 0) cgb_phase<1, 4>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        else cgb_phase<2, 4>(a, sh, pref, wsum, ring, k, dir, part(phase));
         if (!barrier_or_quit()) return;
         int active = 0;
         for (int li = wid; li < a.ninst; li += NW) {
@@ -407,10 +446,12 @@ k_cg_batch(CgBatchArgs a) {
     }
 
     // x = 0 for a vanished right-hand side (Eigen returns the zero vector) and on breakdown
-    for (int it = blockIdx.x * NW + wid; it < a.nitems; it += gridDim.x * NW) {
-        const WorkItem e = a.items[it];
-        const int s0 = sh[e.inst - a.inst0].status;
-        if (s0 != kCgZero && s0 != kCgBreakdown) continue;
+    cgb_prefix(sh, a.ninst, pref, [](int st) { return st == kCgZero || st == kCgBreakdown; });
+    int j, jend, jstep;
+    cgb_deal(a.order, pref[a.ninst], j, jend, jstep);
+    for (int li = 0; j < jend; j += jstep) {
+        while (pref[li + 1] <= j) ++li;
+        const CgItem e{a.inst0 + li, j - pref[li]};
         const BatchInst& I = a.insts[e.inst];
         const int nx = I.D.nx, ny = I.D.ny;
         const int sx = e.w % I.cg_strips_x, sy = e.w / I.cg_strips_x;
