@@ -28,10 +28,10 @@ constexpr int kBatchPlanes = 23;
 constexpr int kQueues = 3;  // work counters: stage 1, stage 2, finalize
 
 // Candidate decompositions the autotuner times: explicit-stage (rows per item, tail rows per
-// item), solver rows per item (each with both dealing orders).
+// item), solver rows (each with both decompositions).
 constexpr int kStageCand[][2] = {{64, 0},   {128, 0},  {256, 0},  {128, 32}, {256, 32},
                                  {256, 64}, {512, 32}, {384, 32}, {192, 32}, {512, 64}};
-constexpr int kCgRowsCand[] = {8, 16, 32, 64, 128};
+constexpr int kCgRowsCand[] = {32, 64, 128, 256};
 
 }  // namespace
 
@@ -166,26 +166,17 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     strip_items(b, t.stage_rows, t.stage_tail_rows, st_items);
     strip_items(b, std::max(16, balanced_rows(b, (long long)b->fin_occ * b->num_sms * FS_WARPS, 1)), 0,
                 fin_items);
-    std::vector<int> cg_nw(b->count);
-    for (int i = 0; i < b->count; ++i) {
-        const int nx = b->prm[i].nx, ny = b->prm[i].ny;
-        const int cg_strips = (nx + CG_W - 1) / CG_W;
-        const int cg_seg = std::min(t.cg_rows, ny);
-        cg_nw[i] = cg_strips * ((ny + cg_seg - 1) / cg_seg);
-        for (int p = 0; p < 2; ++p) {
-            BatchInst& I = b->h_insts[p][i];
-            I.cg_strips_x = cg_strips;
-            I.cg_seg_h = cg_seg;
-        }
-    }
-    // the solver kernel numbers its items itself; its grid covers the largest chunk's items
-    int max_chunk_items = 0;
+    // solver: its grid covers the largest chunk at 8 or more rows per warp
+    for (int p = 0; p < 2; ++p)
+        for (int i = 0; i < b->count; ++i) b->h_insts[p][i].cg_strips_x = (b->prm[i].nx + CG_W - 1) / CG_W;
+    long long max_chunk_rows = 0;
     for (int c = 0; c < b->nchunks; ++c) {
         const int i0 = c * CGB_MAX_INST, i1 = std::min(b->count, i0 + CGB_MAX_INST);
-        int n = 0;
-        for (int i = i0; i < i1; ++i) n += cg_nw[i];
-        max_chunk_items = std::max(max_chunk_items, n);
+        long long n = 0;
+        for (int i = i0; i < i1; ++i) n += (long long)((b->prm[i].nx + CG_W - 1) / CG_W) * b->prm[i].ny;
+        max_chunk_rows = std::max(max_chunk_rows, n);
     }
+    const int cg_warps = (int)std::min((max_chunk_rows + 7) / 8, (long long)1 << 30);
     b->n_stage_items = (int)st_items.size();
     b->n_fin_items = (int)fin_items.size();
     const size_t bytes = (st_items.size() + fin_items.size()) * sizeof(SweepItem);
@@ -208,7 +199,7 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     b->stage_grid[0] = grid_for(b->stage_occ[0], b->num_sms, b->n_stage_items, SW_WARPS);
     b->stage_grid[1] = grid_for(b->stage_occ[1], b->num_sms, b->n_stage_items, SW_WARPS);
     b->fin_grid = grid_for(b->fin_occ, b->num_sms, b->n_fin_items, FS_WARPS);
-    b->cg_grid = grid_for(b->cg_occ, b->num_sms, max_chunk_items, CGS_NT / 32);
+    b->cg_grid = grid_for(b->cg_occ, b->num_sms, cg_warps, CGS_NT / 32);
     b->tuning.stage_rows = t.stage_rows;
     b->tuning.cg_rows = t.cg_rows;
     b->tuning.cg_order = t.cg_order;
@@ -223,6 +214,7 @@ mhd_status launch_cg_chunks(mhd_batch* b, const BatchInst* insts, int solve, boo
         a.inst0 = c * CGB_MAX_INST;
         a.ninst = std::min(CGB_MAX_INST, b->count - a.inst0);
         a.order = b->tuning.cg_order;
+        a.rows = b->tuning.cg_rows;
         a.partials = b->partials;
         a.sync = b->syncs + 2 * c + solve;
         a.solve_index = solve;
@@ -467,7 +459,7 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
     mhd_batch_tuning t{};
     t.stage_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_ROWS", balanced_stage_rows(b, 2));
     t.stage_tail_rows = mhd_host::env_int("MHD_B200_BATCH_STAGE_TAIL_ROWS", 0);
-    t.cg_rows = mhd_host::env_int("MHD_B200_BATCH_CG_ROWS", 32);
+    t.cg_rows = mhd_host::env_int("MHD_B200_BATCH_CG_ROWS", 128);
     t.cg_order = mhd_host::env_int("MHD_B200_BATCH_CG_ORDER", 0);
     const mhd_status s = apply_tuning(b, t);
     if (s != MHD_OK) return fail(s);

@@ -6,9 +6,9 @@
 //
 // The explicit stages and the finalize work on flat lists of warp work items (instance, strip,
 // rows): 28-column strips cut into row ranges. Their kernels are persistent and pull items from a
-// global counter (largest items first). The solver's items are each instance's strip/segment
-// decomposition (28-column strips of cg_seg_h rows); its kernel deals the items of the instances
-// still iterating to warps in a fixed order, because its sums must be reduced in a fixed order.
+// global counter (largest items first). The solver splits the rows of the instances still
+// iterating evenly over its warps in every phase, in a fixed order, because its sums must be
+// reduced in a fixed order.
 //
 // The descriptor array exists twice, for even and odd steps: the finalize leaves U^{n+1}'s hydro
 // planes in the accumulator, so the state and accumulator hydro pointers trade places every step.
@@ -31,7 +31,7 @@ struct BatchInst {
     double* r[2];
     double* p[2];
     long long off;  // zone offset of the instance in every plane arena
-    int cg_strips_x, cg_seg_h;
+    int cg_strips_x;  // 28-column strips of the solver
     long long max_iters;
     double tol;
     double alpha;  // fixed matrix coefficient when alpha_fixed
@@ -176,11 +176,17 @@ k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restric
 // kernel, running their phases in lockstep (solvers.hpp:404-489 per instance, Eigen's
 // ConjugateGradient defaults as in k_cg_sweep).
 //
-// In every phase the items of the instances still iterating (instance-major) are numbered
-// 0 .. n-1 through a prefix sum of their item counts, which every block rebuilds from the same
-// decisions, and dealt to the grid's warps in a fixed order (order 0: round robin, 1: contiguous
-// runs). So the work of a phase is spread evenly over all warps whichever instances remain, and the
-// sums keep a fixed order: every warp sums its partials per instance (item order), each block
+// In every phase the work of the instances still iterating is numbered 0 .. T-1 through a prefix
+// sum of their counts, which every block rebuilds from the same decisions, and split over the W
+// warps of the grid in one of two ways (the autotuner times both):
+//   order 0, rows: the strip rows, instance by instance, band of `rows` rows by band, strip by
+//     strip within a band, row by row; warp g sweeps rows [T g/W, T (g+1)/W) as one or more
+//     (instance, strip, row range) segments, so a block's warps sweep neighbouring strips of a band;
+//   order 1, tiles: tiles of 28 columns x `rows` rows, instance by instance, row of tiles by row;
+//     warp g sweeps tiles g, g + W, ...
+// Either way every warp gets an even share whichever instances remain, and the sums keep a fixed
+// order: So the work of a phase is spread
+// evenly over all warps whichever instances remain, and the sums keep a fixed order: every warp sums its partials per instance (item order), each block
 // sums its warps per instance (warp order) and publishes one partial per (instance, block); after
 // the grid barrier every block reduces each instance's block partials in the same fixed order, so
 // all blocks hold identical scalars and take identical decisions. The loop ends when no instance
@@ -196,13 +202,15 @@ struct CgBInst {
     double bb, absNew, thr, rr, pAp;
     long long products;
     int status;
-    int nitems;  // solver items of the instance (strips x row segments)
+    int ny, strips;   // rows, 28-column strips
+    long long units;  // work units of the instance: strip rows (order 0) or tiles (order 1)
 };
 
 struct CgBatchArgs {
     const BatchInst* insts;  // descriptors of this step's parity
     int inst0, ninst;        // instances [inst0, inst0 + ninst) of this launch
-    int order;               // item dealing: 0 round robin, 1 contiguous runs
+    int order;               // 0: even row ranges in bands of `rows` rows; 1: tiles of `rows` rows
+    int rows;
     double* partials;        // [2][CGB_MAX_INST][gridDim.x][4]
     CgSync* sync;
     int solve_index;         // 0: B* = U1*_B (T planes), 1: B* = U2*_B (A planes)
@@ -223,52 +231,70 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     g.p[0] = I.p[0];
     g.p[1] = I.p[1];
     g.strips_x = I.cg_strips_x;
-    g.seg_h = I.cg_seg_h;
     return g;
 }
 
-// Solver item w of instance inst.
-struct CgItem {
-    int inst;
-    int w;
-};
-
-// This warp's share of items 0 .. total-1: j = first, then j += step while j < end.
-__device__ __forceinline__ void cgb_deal(int order, int total, int& j, int& end, int& step) {
-    constexpr int NW = CGS_NT / 32;
-    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
-    if (order == 0) {
-        j = gw;
-        end = total;
-        step = nw;
-    } else {
-        const int q = (total + nw - 1) / nw;
-        j = min(total, gw * q);
-        end = min(total, j + q);
-        step = 1;
-    }
-}
-
-// Prefix sum over the chunk's instances of the item counts of those with pick(status) (thread 0),
+// Prefix sum over the chunk's instances of the work units of those with pick(status) (thread 0),
 // then a block barrier. Every block computes the same prefix from the same statuses.
 template <class Pick>
-__device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, int* pref, Pick pick) {
+__device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long long* pref, Pick pick) {
     if (threadIdx.x == 0) {
-        int s = 0;
+        long long s = 0;
         for (int li = 0; li < ninst; ++li) {
             pref[li] = s;
-            if (pick(sh[li].status)) s += sh[li].nitems;
+            if (pick(sh[li].status)) s += sh[li].units;
         }
         pref[ninst] = s;
     }
     __syncthreads();
 }
 
+// This warp's share of the phase as segments f(li, sx, r0, r1), in increasing unit number.
+template <class F>
+__device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst* sh,
+                                             const long long* pref, F&& f) {
+    constexpr int NW = CGS_NT / 32;
+    const long long nw = (long long)gridDim.x * NW;
+    const long long g = (long long)blockIdx.x * NW + (threadIdx.x >> 5);
+    const long long T = pref[a.ninst];
+    if (a.order != 0) {
+        int li = 0;
+        for (long long j = g; j < T; j += nw) {
+            while (pref[li + 1] <= j) ++li;
+            const int w = (int)(j - pref[li]);
+            const int sx = w % sh[li].strips;
+            const int r0 = (w / sh[li].strips) * a.rows;
+            f(li, sx, r0, min(r0 + a.rows, sh[li].ny));
+        }
+        return;
+    }
+    long long p = T * g / nw;
+    const long long p1 = T * (g + 1) / nw;
+    int li = 0;
+    while (p < p1) {
+        while (pref[li + 1] <= p) ++li;  // p only grows: li advances over the prefix once
+        const int ny = sh[li].ny;
+        const long long S = sh[li].strips;
+        const long long q = p - pref[li];
+        const int H = min(a.rows, ny);
+        const long long band = min(q / (S * H), (long long)((ny - 1) / H));  // last band: ny - b0 rows
+        const int b0 = (int)band * H;
+        const int h = min(H, ny - b0);
+        const long long t = q - band * S * H;  // within the band: strip t / h, row b0 + t % h
+        const int sx = (int)(t / h);
+        const int r0 = b0 + (int)(t - (long long)sx * h);
+        long long e = p + (b0 + h - r0);  // end of this strip's piece of the band
+        if (e > p1) e = p1;
+        f(li, sx, r0, r0 + (int)(e - p));
+        p = e;
+    }
+}
+
 // One sweep over this warp's items: PH 0 the right-hand side (cg_rhs_segment), 1 the first
 // iteration, 2 a later one (cg_iter_segment); NV sums per instance. Ends with the block's partials
 // of every instance published in part_out.
 template <int PH, int NV>
-__device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const int* pref,
+__device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const long long* pref,
                                           double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
     constexpr int NW = CGS_NT / 32;
@@ -278,12 +304,8 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         for (int c = 0; c < NV; ++c) wsum[wid][li][c] = 0.0;
     __syncwarp();
     const bool odd = (k & 1) != 0;
-    int j, jend, jstep;
-    cgb_deal(a.order, pref[a.ninst], j, jend, jstep);
-    for (int li = 0; j < jend; j += jstep) {
-        while (pref[li + 1] <= j) ++li;  // j only grows: li advances over the prefix once
-        const CgItem e{a.inst0 + li, j - pref[li]};
-        const BatchInst& I = a.insts[e.inst];
+    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+        const BatchInst& I = a.insts[a.inst0 + li];
         const CgSweepArgs g = cgb_args(a, I);
         CgScal s;
         s.cx = sh[li].cx;
@@ -294,13 +316,13 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         s.beta = sh[li].beta;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if constexpr (PH == 0) {
-            cg_rhs_segment(g, s, e.w, dir, g.r[0], ring, acc);
+            cg_rhs_segment(g, s, sx, r0, r1, dir, g.r[0], ring, acc);
         } else {
             const double* rk = odd ? g.r[1] : g.r[0];
             double* rk1 = odd ? g.r[0] : g.r[1];
             const double* pkm1 = odd ? g.p[0] : g.p[1];
             double* pk = odd ? g.p[1] : g.p[0];
-            cg_iter_segment<PH == 1>(g, s, e.w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<PH == 1>(g, s, sx, r0, r1, dir, rk, pkm1, rk1, pk, ring, acc);
         }
 #pragma unroll
         for (int c = 0; c < NV; ++c)
@@ -310,7 +332,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
             for (int c = 0; c < NV; ++c) wsum[wid][li][c] += acc[c];
         }
         __syncwarp();
-    }
+    });
     __syncthreads();
     for (int q = threadIdx.x; q < a.ninst * NV; q += CGS_NT) {
         const int li = q / NV, c = q - li * NV;
@@ -341,7 +363,7 @@ k_cg_batch(CgBatchArgs a) {
     constexpr int NW = CGS_NT / 32;
     __shared__ CgBInst sh[CGB_MAX_INST];
     __shared__ double wsum[NW][CGB_MAX_INST][4];
-    __shared__ int pref[CGB_MAX_INST + 1];
+    __shared__ long long pref[CGB_MAX_INST + 1];
     __shared__ int sflag;
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double cg_ring_mem[];
@@ -379,7 +401,10 @@ k_cg_batch(CgBatchArgs a) {
         S.products = 0;
         S.rr = 0.0;
         S.status = kCgActive;
-        S.nitems = I.cg_strips_x * ((I.D.ny + I.cg_seg_h - 1) / I.cg_seg_h);
+        S.ny = I.D.ny;
+        S.strips = I.cg_strips_x;
+        S.units = (long long)I.cg_strips_x *
+                  ((a.order == 0) ? I.D.ny : (I.D.ny + a.rows - 1) / a.rows);
     }
     __syncthreads();
     auto is_active = [](int st) { return st == kCgActive; };
@@ -447,19 +472,13 @@ k_cg_batch(CgBatchArgs a) {
 
     // x = 0 for a vanished right-hand side (Eigen returns the zero vector) and on breakdown
     cgb_prefix(sh, a.ninst, pref, [](int st) { return st == kCgZero || st == kCgBreakdown; });
-    int j, jend, jstep;
-    cgb_deal(a.order, pref[a.ninst], j, jend, jstep);
-    for (int li = 0; j < jend; j += jstep) {
-        while (pref[li + 1] <= j) ++li;
-        const CgItem e{a.inst0 + li, j - pref[li]};
-        const BatchInst& I = a.insts[e.inst];
-        const int nx = I.D.nx, ny = I.D.ny;
-        const int sx = e.w % I.cg_strips_x, sy = e.w / I.cg_strips_x;
+    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+        const BatchInst& I = a.insts[a.inst0 + li];
+        const int nx = I.D.nx;
         const int i = sx * CG_W - CG_HALO + lane;
-        const int r0 = sy * I.cg_seg_h, r1 = min(r0 + I.cg_seg_h, ny);
         if (lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx)
             for (int j = r0; j < r1; ++j) I.x[(size_t)j * nx + i] = 0.0;
-    }
+    });
     if (blockIdx.x == 0) {
         for (int li = tid; li < a.ninst; li += CGS_NT) {
             const BatchInst& I = a.insts[a.inst0 + li];

@@ -89,17 +89,16 @@ constexpr int CG_HALO = 2;    // halo lanes on each side
 constexpr int CG_W = 32 - 2 * CG_HALO;  // output columns per warp: lanes 2..29
 constexpr size_t kCgRingBytes = (size_t)(CGS_NT / 32) * CG_RING * CG_SLOT * sizeof(double);
 
-// Right-hand-side sweep over the warp's segment: r0 = b = eta J_z(B) (written to r0), p0 = z0 = b/d,
-// partials |b|^2, b.z0, p0.A p0 (acc[0..2]). Lane l holds corner column c0 - 2 + l; lanes 2..29
-// own the results. Sweep row k (k = 0 is the row behind the first one) sits in slot k % CG_RING.
-__device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgScal& s, int w, int dir,
-                                               double* r0, double* ring, double (&acc)[4]) {
+// Right-hand-side sweep over rows [r0w, r1w) of column strip sx: r0 = b = eta J_z(B) (written to
+// r0), p0 = z0 = b/d, partials |b|^2, b.z0, p0.A p0 (acc[0..2]). Lane l holds corner column
+// c0 - 2 + l; lanes 2..29 own the results. Sweep row k (k = 0 is the row behind the first one) sits
+// in slot k % CG_RING.
+__device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
+                                               int r1w, int dir, double* r0, double* ring,
+                                               double (&acc)[4]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
-    const int sx = w % a.strips_x, sy = w / a.strips_x;
     const int c0 = sx * CG_W;
-    const int r0w = sy * a.seg_h;
-    const int r1w = min(r0w + a.seg_h, ny);
     if (r0w >= r1w) return;
     const int i = c0 - CG_HALO + lane;
     const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
@@ -166,21 +165,20 @@ __device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgSca
     cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
-// One CG iteration k over the warp's segment (the sweep of the header comment). FIRST: k = 0,
+// One CG iteration k over rows [r0w, r1w) of column strip sx (the sweep of the header comment).
+// FIRST: k = 0,
 // p_0 = z_0 and x_0 = 0 (p_{-1} and x are not read). acc[0..3] receive r.r, r.z, z.Az, z.q_k of
 // the owned cells. Sweep row t holds grid row jfirst + (t - 2) dir, t = 0 .. nrows + 3; at sweep
 // row t the warp forms p_k of row t, q_k, r_{k+1}, z_{k+1} of row t-1 and A z_{k+1} and the outputs
 // of row t-2. Row t is copied into slot t % CG_RING by the end of sweep row t - 6.
 template <bool FIRST>
-__device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int w, int dir,
-                                                const double* rk, const double* pkm1, double* rk1,
-                                                double* pk, double* ring, double (&acc)[4]) {
+__device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
+                                                int r1w, int dir, const double* rk, const double* pkm1,
+                                                double* rk1, double* pk, double* ring,
+                                                double (&acc)[4]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
-    const int sx = w % a.strips_x, sy = w / a.strips_x;
     const int c0 = sx * CG_W;
-    const int r0w = sy * a.seg_h;
-    const int r1w = min(r0w + a.seg_h, ny);
     if (r0w >= r1w) return;
     const int i = c0 - CG_HALO + lane;
     const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
@@ -320,8 +318,10 @@ k_cg_sweep(CgSweepArgs a) {
     // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
     {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int w = wfirst; w < a.nwarps; w += wstride)
-            cg_rhs_segment(a, s, w, dir, a.r[0], ring, acc);
+        for (int w = wfirst; w < a.nwarps; w += wstride) {
+            const int sx = w % a.strips_x, r0w = (w / a.strips_x) * a.seg_h;
+            cg_rhs_segment(a, s, sx, r0w, min(r0w + a.seg_h, a.D.ny), dir, a.r[0], ring, acc);
+        }
         publish<3>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
     }
     if (!barrier_or_quit()) return;
@@ -350,8 +350,10 @@ k_cg_sweep(CgSweepArgs a) {
             {
                 double acc[4] = {0.0, 0.0, 0.0, 0.0};
                 for (int w = wfirst; w < a.nwarps; w += wstride) {
-                    if (k == 0) cg_iter_segment<true>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
-                    else cg_iter_segment<false>(a, s, w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    const int sx = w % a.strips_x, r0w = (w / a.strips_x) * a.seg_h;
+                    const int r1w = min(r0w + a.seg_h, a.D.ny);
+                    if (k == 0) cg_iter_segment<true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    else cg_iter_segment<false>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
                 }
                 publish<4>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
             }
