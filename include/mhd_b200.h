@@ -37,7 +37,8 @@ typedef enum {
     MHD_ERR_NO_DEVICE = 6,          /* no sm_100 device, or the library was not built for it */
     MHD_ERR_OUT_OF_MEMORY = 7,
     MHD_ERR_NO_STATE = 8,           /* a state must be set before stepping */
-    MHD_ERR_TOO_LARGE = 9           /* grid larger than the fixed scratch of the no-alloc call */
+    MHD_ERR_TOO_LARGE = 9,          /* grid larger than the fixed scratch of the no-alloc call */
+    MHD_ERR_IO = 10                 /* a snapshot file could not be written */
 } mhd_status;
 
 typedef enum { MHD_LAYOUT_DENSE = 0, MHD_LAYOUT_PADDED = 1 } mhd_layout;
@@ -165,6 +166,26 @@ void* mhd_stream(mhd_context* ctx);
 
 /* Number of kernel launches one mhd_step enqueues (for launch accounting). */
 int mhd_launches_per_step(mhd_context* ctx);
+
+/* Snapshots in the reference's file format: the bytes write_data_to_binary_file
+ * (diagnostics.hpp:90-131) writes for the Grid after fillGhostPeriodic + computePrimitives, as the
+ * driver calls it every snapshot_frequency steps (integrator_main.cpp:102-109). 9 doubles
+ * [nx, ny, ng, snapshot_rate, dx, dy, dt, divB_rms, divB_max], then 7 padded planes of
+ * (nx+2ng)*(ny+2ng) doubles with periodic ghost layers, in the order rho (floored), E, p, vx, vy,
+ * bxc, byc (the reader scripts/display_functions.py:3-22 reshapes them so). 0 <= ng <= min(nx, ny);
+ * the reference's Grid has ng = 2. */
+size_t mhd_snapshot_bytes(mhd_context* ctx, int ng);  /* 0 for an invalid ng */
+/* Write the current state's snapshot to the file `path` asynchronously: packed on the device in
+ * stream order (later steps do not disturb it), copied to pinned host memory on a copy stream of
+ * its own and written by a host thread while the caller keeps stepping. Two snapshots can be in
+ * flight; a third call waits for the older one. */
+mhd_status mhd_snapshot_write(mhd_context* ctx, const char* path, int ng, int snapshot_rate,
+                              double dt);
+/* Wait until every snapshot written so far is on disk; MHD_ERR_IO if a file could not be written
+ * (since the last wait). */
+mhd_status mhd_snapshot_wait(mhd_context* ctx);
+/* The same bytes into host memory `out` (mhd_snapshot_bytes long), synchronously. */
+mhd_status mhd_snapshot_pack(mhd_context* ctx, int ng, int snapshot_rate, double dt, void* out);
 
 /* ---------------------------------------------------------------------------------------------
  * Batched stepping (no counterpart in the reference, which advances one Grid per process):

@@ -5,6 +5,7 @@
 //   generate_A_matrix(grid, workspace, alpha)        solvers.hpp:404-443 (+ solver.compute)
 //   IMEX(grid, g1, g2, workspace, rv, tableau, solver, dt)   solvers.hpp:491-613
 //   CFL_condition_checker(grid)                      diagnostics.hpp:44-88
+//   write_data_to_binary_file(grid, frame, rate, dt) diagnostics.hpp:90-131
 //
 // The functions are templates over the caller's types, so this header needs none of the
 // reference's headers; GridT must provide the members of the reference's Grid (Grid.hpp:9-26):
@@ -20,6 +21,7 @@
 // host and device; for a device-resident run use mhd_run() of mhd_b200.h.
 #pragma once
 
+#include <cstdio>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -113,6 +115,20 @@ double CFL_condition_checker(const GridT& g) {
     double dt = 0.0;
     check(mhd_cfl_dt(c, &dt), "mhd_cfl_dt");
     return dt;
+}
+
+// write_data_to_binary_file(grid, frame_index, snapshot_rate, dt): the snapshot file
+// output/snapshot_NNNNNN.dat of the grid's state, in the reference's format; on disk when the call
+// returns, as in the reference. (A device-resident run overlaps its files with stepping through
+// mhd_snapshot_write of mhd_b200.h.)
+template <class GridT>
+void write_data_to_binary_file(GridT& g, int frame_index, int snapshot_rate, double dt) {
+    mhd_context* c = Session::of(g).ctx();
+    upload(c, g);
+    char path[64];
+    snprintf(path, sizeof(path), "output/snapshot_%06d.dat", frame_index);
+    check(mhd_snapshot_write(c, path, g.ng, snapshot_rate, dt), "mhd_snapshot_write");
+    check(mhd_snapshot_wait(c), "write_data_to_binary_file");
 }
 
 }  // namespace mhd_b200

@@ -26,6 +26,7 @@ STATUS_NAMES = {
     7: "MHD_ERR_OUT_OF_MEMORY",
     8: "MHD_ERR_NO_STATE",
     9: "MHD_ERR_TOO_LARGE",
+    10: "MHD_ERR_IO",
 }
 LAYOUT_DENSE = 0
 LAYOUT_PADDED = 1
@@ -101,6 +102,11 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_kernel_times.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.mhd_cfl_dt.argtypes = [vp, _dp]
     lib.mhd_divb.argtypes = [vp, _dp, _dp]
+    lib.mhd_snapshot_bytes.argtypes = [vp, ctypes.c_int]
+    lib.mhd_snapshot_bytes.restype = ctypes.c_size_t
+    lib.mhd_snapshot_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    lib.mhd_snapshot_wait.argtypes = [vp]
+    lib.mhd_snapshot_pack.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp]
     lib.mhd_synchronize.argtypes = [vp]
     lib.mhd_last_cg_products.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.mhd_state_device_pointers.argtypes = [vp, P6]
@@ -296,6 +302,28 @@ class Context:
         rms, mx = ctypes.c_double(), ctypes.c_double()
         _check(self.lib.mhd_divb(self.h, ctypes.byref(rms), ctypes.byref(mx)), "mhd_divb")
         return rms.value, mx.value
+
+    # -- snapshots in the reference's file format (diagnostics.hpp:90-131)
+    def snapshot_bytes(self, ng: int = 2) -> int:
+        return int(self.lib.mhd_snapshot_bytes(self.h, ng))
+
+    def snapshot_write(self, path: str, ng: int = 2, snapshot_rate: int = 1, dt: float = 0.0):
+        """Write the current state's snapshot file asynchronously (see mhd_snapshot_write)."""
+        _check(self.lib.mhd_snapshot_write(self.h, os.fsencode(path), ng, snapshot_rate, dt),
+               "mhd_snapshot_write")
+
+    def snapshot_wait(self):
+        _check(self.lib.mhd_snapshot_wait(self.h), "mhd_snapshot_wait")
+
+    def snapshot_pack(self, ng: int = 2, snapshot_rate: int = 1, dt: float = 0.0) -> np.ndarray:
+        """The snapshot file's doubles (9-double header, then 7 padded planes)."""
+        n = self.snapshot_bytes(ng)
+        if n == 0:
+            raise MHDError(1, "snapshot_pack: invalid ng")
+        out = np.empty(n // 8, dtype=np.float64)
+        _check(self.lib.mhd_snapshot_pack(self.h, ng, snapshot_rate, dt, out.ctypes.data),
+               "mhd_snapshot_pack")
+        return out
 
     @property
     def stream(self) -> int:

@@ -20,6 +20,7 @@
 
 #include "../../include/mhd_b200.h"
 #include "mhd_cg_sweep.cuh"
+#include "mhd_snapshot.h"
 #include "mhd_host_util.h"
 #include "mhd_kernels.cuh"
 #include "mhd_finalize_sweep.cuh"
@@ -78,6 +79,7 @@ struct mhd_context {
     bool timing = false;
     std::vector<cudaEvent_t> events;
     size_t events_used = 0;
+    mhd_host::SnapshotWriter* snap = nullptr;  // created by the first mhd_snapshot_write
 };
 
 namespace {
@@ -233,6 +235,21 @@ mhd_status check_ctx(mhd_context* c) {
     return MHD_OK;
 }
 
+// Enqueue on the context's stream: divB of the current state, then its snapshot into device
+// memory d (k_snapshot_pack).
+mhd_status enqueue_snapshot(mhd_context* c, int ng, int snapshot_rate, double dt, double* d) {
+    k_divb_partial<<<c->divb_blocks, 256, 0, c->stream>>>(c->dom, c->S[4], c->S[5], c->divb_partial);
+    MHD_TRY(cudaGetLastError());
+    k_divb_final<<<1, 32, 0, c->stream>>>(c->divb_partial, c->divb_blocks, (long long)c->n, c->divb_out);
+    MHD_TRY(cudaGetLastError());
+    const int nxt = c->dom.nx + 2 * ng, nyt = c->dom.ny + 2 * ng;
+    k_snapshot_pack<<<cell_grid(nxt, nyt), 256, 0, c->stream>>>(c->dom, cplanes(c->S), ng,
+                                                                (double)snapshot_rate, dt,
+                                                                c->divb_out, d);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
 mhd_status status_from_flags(unsigned flags) {
     if (flags & kStatusTimeout) return MHD_ERR_TIMEOUT;
     if (flags & kStatusNonFinite) return MHD_ERR_NONFINITE;
@@ -256,6 +273,7 @@ const char* mhd_status_string(mhd_status s) {
         case MHD_ERR_OUT_OF_MEMORY: return "out of device memory";
         case MHD_ERR_NO_STATE: return "no state set";
         case MHD_ERR_TOO_LARGE: return "grid exceeds the fixed scratch of the allocation-free call";
+        case MHD_ERR_IO: return "a snapshot file could not be written";
     }
     return "unknown status";
 }
@@ -432,6 +450,7 @@ mhd_status mhd_destroy(mhd_context* c) {
     if (!c) return MHD_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    delete c->snap;  // waits for the snapshots in flight
     cudaFree(c->pool);
     cudaFree(c->partials);
     cudaFree(c->sync);
@@ -700,6 +719,57 @@ mhd_status mhd_cfl_dt(mhd_context* c, double* dt) {
     const double dt_hyp = c->prm.courant * h / smaxv;
     *dt = std::min(dt_hyp, dt_res) * c->prm.safety;
     return MHD_OK;
+}
+
+size_t mhd_snapshot_bytes(mhd_context* c, int ng) {
+    if (!c || ng < 0 || ng > std::min(c->dom.nx, c->dom.ny)) return 0;
+    return (9 + 7 * (size_t)(c->dom.nx + 2 * ng) * (size_t)(c->dom.ny + 2 * ng)) * sizeof(double);
+}
+
+mhd_status mhd_snapshot_write(mhd_context* c, const char* path, int ng, int snapshot_rate,
+                              double dt) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    const size_t bytes = mhd_snapshot_bytes(c, ng);
+    if (!path || bytes == 0) return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    if (!c->snap) {
+        c->snap = new (std::nothrow) mhd_host::SnapshotWriter(c->device);
+        if (!c->snap) return MHD_ERR_OUT_OF_MEMORY;
+    }
+    int slot = 0;
+    double* d = nullptr;
+    if ((s = c->snap->acquire(bytes, &slot, &d)) != MHD_OK) return s;
+    if ((s = enqueue_snapshot(c, ng, snapshot_rate, dt, d)) != MHD_OK) {
+        c->snap->release(slot);
+        return s;
+    }
+    return c->snap->submit(slot, c->stream, path, bytes);
+}
+
+mhd_status mhd_snapshot_wait(mhd_context* c) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    return c->snap ? c->snap->wait() : MHD_OK;
+}
+
+mhd_status mhd_snapshot_pack(mhd_context* c, int ng, int snapshot_rate, double dt, void* out) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    const size_t bytes = mhd_snapshot_bytes(c, ng);
+    if (!out || bytes == 0) return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    double* d = nullptr;
+    MHD_TRY(cudaMallocAsync(&d, bytes, c->stream));
+    s = enqueue_snapshot(c, ng, snapshot_rate, dt, d);
+    if (s == MHD_OK) {
+        const cudaError_t e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, c->stream);
+        if (e != cudaSuccess) s = mhd_host::cuda_status(e);
+    }
+    cudaFreeAsync(d, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (s == MHD_OK && e != cudaSuccess) s = mhd_host::cuda_status(e);
+    return s;
 }
 
 mhd_status mhd_divb(mhd_context* c, double* rms, double* maxabs) {

@@ -482,6 +482,53 @@ k_primitives(Domain D, CPlanes u, double* rho_f, double* vx, double* vy, double*
     }
 }
 
+// Snapshot in the reference's file layout (write_data_to_binary_file, diagnostics.hpp:90-131, of
+// the Grid after fillGhostPeriodic + computePrimitives, Grid.hpp:64-136): out[0..8] = nx, ny, ng,
+// snapshot_rate, dx, dy, dt, divB rms, divB max (divb[0..1]), then the padded (nx+2ng) x (ny+2ng)
+// planes rho (floored), E, p, vx, vy, bxc, byc. The reference's ghost fill makes every ghost cell
+// the periodic image of a physical one (bxc, byc included: they are wrapped after computeCellB),
+// so each padded cell is computed from its image.
+static __global__ void __launch_bounds__(256)
+k_snapshot_pack(Domain D, CPlanes u, int ng, double rate, double dt, const double* divb,
+                double* out) {
+    const int nx = D.nx, ny = D.ny;
+    const int nxt = nx + 2 * ng, nyt = ny + 2 * ng;
+    const size_t plane = (size_t)nxt * nyt;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        out[0] = (double)nx;
+        out[1] = (double)ny;
+        out[2] = (double)ng;
+        out[3] = rate;
+        out[4] = D.dx;
+        out[5] = D.dy;
+        out[6] = dt;
+        out[7] = divb[0];
+        out[8] = divb[1];
+    }
+    double* const pl = out + 9;
+    for (int J = blockIdx.y; J < nyt; J += gridDim.y) {
+        const int j = wrap(J - ng, ny);
+        const size_t row = (size_t)j * nx, row_up = (size_t)wrap(j + 1, ny) * nx;
+        for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nxt; I += gridDim.x * blockDim.x) {
+            const int i = wrap(I - ng, nx);
+            const size_t g = row + i;
+            const double bx = (u.f[4][g] + u.f[4][row + wrap(i + 1, nx)]) / 2.0;
+            const double by = (u.f[5][g] + u.f[5][row_up + i]) / 2.0;
+            double rho = u.f[0][g], vx, vy;
+            const double E = u.f[3][g];
+            const double p = primitives(rho, u.f[1][g], u.f[2][g], E, bx, by, vx, vy);
+            const size_t o = (size_t)J * nxt + I;
+            pl[o] = rho;
+            pl[plane + o] = E;
+            pl[2 * plane + o] = p;
+            pl[3 * plane + o] = vx;
+            pl[4 * plane + o] = vy;
+            pl[5 * plane + o] = bx;
+            pl[6 * plane + o] = by;
+        }
+    }
+}
+
 // Rate of the face field from a corner field E (solvers.hpp:472-488): bx' = -(E(i,j+1) - E(i,j))/dy,
 // by' = (E(i+1,j) - E(i,j))/dx. With E == nullptr the corner field is eta*J_z(bxf, byf) itself
 // (the explicit resistive term, solvers.hpp:450-463 and :470).

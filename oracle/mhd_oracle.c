@@ -50,6 +50,44 @@ void orc_primitives(const orc_params* P, const double* const s[6], double* rho_f
         }
 }
 
+/* diagnostics.hpp:90-131 (header, then the 7 planes in the order written at :121-127). The ghost
+ * fill (Grid.hpp:64-80, 143-161) copies every field periodically -- bxc/byc after computeCellB --
+ * and computePrimitives then runs over the whole padded grid, so each padded cell holds the
+ * primitives of its periodic image. */
+void orc_snapshot(const orc_params* P, const double* const s[6], int ng, int snapshot_rate,
+                  double dt, double* out) {
+    const int nx = P->nx, ny = P->ny;
+    const int nxt = nx + 2 * ng, nyt = ny + 2 * ng;
+    const size_t n = (size_t)nx * ny, plane = (size_t)nxt * nyt;
+    double rms, maxabs;
+    orc_divb(P, s[ORC_BX], s[ORC_BY], &rms, &maxabs);
+    out[0] = nx;
+    out[1] = ny;
+    out[2] = ng;
+    out[3] = snapshot_rate;
+    out[4] = P->dx;
+    out[5] = P->dy;
+    out[6] = dt;
+    out[7] = rms;
+    out[8] = maxabs;
+    double* prim = (double*)malloc(6 * n * sizeof(double));
+    double* rho_f = prim;
+    double* vx = prim + n;
+    double* vy = prim + 2 * n;
+    double* p = prim + 3 * n;
+    double* bxc = prim + 4 * n;
+    double* byc = prim + 5 * n;
+    orc_primitives(P, s, rho_f, vx, vy, p, bxc, byc);
+    const double* src[7] = {rho_f, s[ORC_E], p, vx, vy, bxc, byc};
+    for (int q = 0; q < 7; ++q)
+        for (int J = 0; J < nyt; ++J)
+            for (int I = 0; I < nxt; ++I) {
+                const int i = ((I - ng) % nx + nx) % nx, j = ((J - ng) % ny + ny) % ny;
+                out[9 + q * plane + (size_t)J * nxt + I] = src[q][(size_t)j * nx + i];
+            }
+    free(prim);
+}
+
 /* ---------------------------------------------------------------- MUSCL (MUSCL.hpp) */
 
 /* MUSCL.hpp:11-17 */

@@ -65,6 +65,13 @@ double orc_cfl_dt(const orc_params* P, const double* const state[6], double cour
 /* diagnostics.hpp:15-42: RMS and max |div B| over physical cells. */
 void orc_divb(const orc_params* P, const double* bxf, const double* byf, double* rms, double* maxabs);
 
+/* diagnostics.hpp:90-131 write_data_to_binary_file of the Grid after fillGhostPeriodic +
+ * computePrimitives (Grid.hpp:64-136), as the driver calls it (integrator_main.cpp:106-108): into
+ * out, 9 doubles [nx, ny, ng, snapshot_rate, dx, dy, dt, divB rms, divB max], then the padded
+ * (nx+2ng)*(ny+2ng) planes rho (floored), E, p, vx, vy, bxc, byc with periodic ghost layers. */
+void orc_snapshot(const orc_params* P, const double* const state[6], int ng, int snapshot_rate,
+                  double dt, double* out);
+
 /* benchmarks.hpp:15-76 Orszag-Tang vortex (face B from Az at corners, E from face B). */
 void orc_init_orszag_tang(const orc_params* P, double* const state[6]);
 

@@ -76,6 +76,7 @@ def oracle_lib():
         lib.orc_cfl_dt.argtypes = [P, pa, ctypes.c_double, ctypes.c_double]
         lib.orc_cfl_dt.restype = ctypes.c_double
         lib.orc_divb.argtypes = [P, _dp, _dp, _dp, _dp]
+        lib.orc_snapshot.argtypes = [P, pa, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp]
         lib.orc_init_orszag_tang.argtypes = [P, pa]
         lib.orc_init_sine_wave.argtypes = [P, pa, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         lib.orc_cg_solve.argtypes = [P, ctypes.c_double, _dp, _dp, ctypes.POINTER(ctypes.c_long)]
@@ -140,6 +141,12 @@ class Oracle:
                           ctypes.byref(rms), ctypes.byref(mx))
         return rms.value, mx.value
 
+    def snapshot(self, ng=2, snapshot_rate=1, dt=0.0):
+        """orc_snapshot: the snapshot file's doubles (header + 7 padded planes)."""
+        out = np.zeros(9 + 7 * (self.p.nx + 2 * ng) * (self.p.ny + 2 * ng))
+        self.lib.orc_snapshot(ctypes.byref(self.p), _ptr_array(self.state), ng, snapshot_rate, dt, _ptr(out))
+        return out
+
     def cg_solve(self, alpha, rhs):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         x = np.zeros_like(rhs)
@@ -188,6 +195,7 @@ def ref_lib():
         lib.ref_set_alpha.argtypes = [vp, ctypes.c_double]
         lib.ref_step.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_long)]
         lib.ref_divb.argtypes = [vp, _dp, _dp]
+        lib.ref_write_snapshot.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         lib.ref_explicit_rhs.argtypes = [vp] + [_dp] * 6
         lib.ref_implicit_rate.argtypes = [vp, _dp, _dp, _dp]
         lib.ref_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, _dp, _dp, ctypes.POINTER(ctypes.c_long)]
@@ -256,6 +264,19 @@ class Reference:
         rms, mx = ctypes.c_double(), ctypes.c_double()
         self.lib.ref_divb(self.h, ctypes.byref(rms), ctypes.byref(mx))
         return rms.value, mx.value
+
+    def write_snapshot(self, workdir, frame_index, snapshot_rate, dt):
+        """integrator_main.cpp:106-108: the reference writes workdir/output/snapshot_NNNNNN.dat
+        (its path is relative to the working directory); returns the file's bytes."""
+        os.makedirs(os.path.join(workdir, "output"), exist_ok=True)
+        cwd = os.getcwd()
+        os.chdir(workdir)
+        try:
+            self.lib.ref_write_snapshot(self.h, frame_index, snapshot_rate, dt)
+        finally:
+            os.chdir(cwd)
+        with open(os.path.join(workdir, "output", "snapshot_%06d.dat" % frame_index), "rb") as f:
+            return f.read()
 
     def run(self, nsteps, dt_fixed=0.0, dts=None):
         """Driver loop of integrator_main.cpp:76-112; returns (dts, cg_products[nsteps, 2])."""

@@ -16,6 +16,8 @@
 //   ref_divb              diagnostics.hpp:15-42
 //   ref_explicit_rhs      solvers.hpp:393-402 (on a copy of the state)
 //   ref_run               integrator_main.cpp:76-112 (dt loop, matrix regeneration rule)
+//   ref_write_snapshot    integrator_main.cpp:106-108 (ghost fill, primitives,
+//                         write_data_to_binary_file into output/ of the working directory)
 #include <iostream>
 #include <fstream>
 #include <vector>
@@ -144,6 +146,13 @@ void ref_step(void* h, double dt, long* cg_products2) {
         cg_products2[0] = s->solver.product_log.size() > 0 ? static_cast<long>(s->solver.product_log[0]) : -1;
         cg_products2[1] = s->solver.product_log.size() > 1 ? static_cast<long>(s->solver.product_log[1]) : -1;
     }
+}
+
+void ref_write_snapshot(void* h, int frame_index, int snapshot_rate, double dt) {
+    RefSim* s = static_cast<RefSim*>(h);
+    s->state.fillGhostPeriodic();
+    s->state.computePrimitives();
+    write_data_to_binary_file(s->state, frame_index, snapshot_rate, dt);
 }
 
 void ref_divb(void* h, double* rms, double* maxabs) {

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import os
 import sys
+import tempfile
 
 import numpy as np
 
@@ -149,6 +150,21 @@ def main():
     out.update(pack("f1", f1))
     out.update(pack("final", ref.get_state()))
     np.savez(os.path.join(OUT, "upwind32_ref.npz"), **out)
+
+    # 7. Snapshot file (diagnostics.hpp:90-131) of a random smooth state on a 20x14 grid with
+    #    dx != dy after 2 reference steps: the exact bytes the reference writes, ng = 2
+    nx, ny = 20, 14
+    dx, dy = 2 * PI_REF / nx, 1.25 * PI_REF / ny
+    eta = 1e-2
+    ref = Reference(nx, ny, dx, dy, eta)
+    ref.set_state(smooth_random_state(nx, ny, dx, dy, seed=4321))
+    dts, _ = ref.run(2)
+    with tempfile.TemporaryDirectory() as tmp:
+        raw = ref.write_snapshot(tmp, 3, 5, float(dts[-1]))
+    out = dict(nx=nx, ny=ny, dx=dx, dy=dy, eta=eta, ng=2, snapshot_rate=5, frame_index=3,
+               dt=float(dts[-1]), snapshot=np.frombuffer(raw, dtype=np.float64))
+    out.update(pack("state", ref.get_state()))
+    np.savez(os.path.join(OUT, "snapshot20x14_ref.npz"), **out)
 
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

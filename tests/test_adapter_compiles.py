@@ -1,0 +1,46 @@
+"""CPU check of the reference-shaped C++ adapter (include/mhd_b200_imex.hpp): it compiles and its
+templates instantiate against a type with the members of the reference's Grid (Grid.hpp:9-26), as
+src/integrator_main.cpp would use them."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+PROGRAM = r"""
+#include <vector>
+#include "mhd_b200_imex.hpp"
+
+struct Grid {  // the members of the reference's Grid that the adapter uses
+    int nx = 8, ny = 8, ng = 2;
+    double cell_width = 0.5, cell_height = 0.5, resistivity = 1e-3;
+    std::vector<double> rho, mx, my, E, bxf, byf, bxc, byc, vx, vy, p;
+};
+struct Workspace {};
+struct Reconstruction {};
+struct Tableau {};
+struct Solver {};
+
+void driver_step(Grid& g, Grid& g1, Grid& g2, Workspace& w, Reconstruction& rv, Tableau& t,
+                 Solver& s, int frame) {
+    const double dt = mhd_b200::CFL_condition_checker(g);
+    mhd_b200::generate_A_matrix(g, w, dt * g.resistivity * 0.2928932188134524);
+    mhd_b200::IMEX(g, g1, g2, w, rv, t, s, dt);
+    mhd_b200::write_data_to_binary_file(g, frame, 10, dt);
+}
+"""
+
+
+def test_adapter_instantiates(tmp_path):
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "driver.cpp"
+    src.write_text(PROGRAM)
+    cuda_inc = "/usr/local/cuda/include"
+    cmd = [cxx, "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-I", cuda_inc, str(src)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -138,3 +138,21 @@ def test_cg_solves_system():
     lap = (np.roll(x, 1, 0) + np.roll(x, -1, 0) + np.roll(x, 1, 1) + np.roll(x, -1, 1) - 4 * x) / dx2
     assert np.max(np.abs(x - alpha * lap - b)) <= 1e-13 * np.max(np.abs(b))
     assert 0 < prods < 2 * n * n
+
+
+def test_snapshot_matches_reference_writer():
+    """orc_snapshot against the file the reference's write_data_to_binary_file wrote
+    (diagnostics.hpp:90-131, after fillGhostPeriodic + computePrimitives) for the same state."""
+    d = load_golden("snapshot20x14_ref.npz")
+    o = _oracle_for(d)
+    o.set_state(fields(d, "state"))
+    ng = int(d["ng"])
+    got = o.snapshot(ng, int(d["snapshot_rate"]), float(d["dt"]))
+    want = d["snapshot"]
+    assert got.shape == want.shape
+    assert np.array_equal(got[:7], want[:7])  # nx, ny, ng, snapshot_rate, dx, dy, dt
+    assert list(want[:4]) == [d["nx"], d["ny"], ng, d["snapshot_rate"]]
+    assert abs(got[7] - want[7]) <= 1e-13 and abs(got[8] - want[8]) <= 1e-13  # div B: rounding level
+    nxt, nyt = int(d["nx"]) + 2 * ng, int(d["ny"]) + 2 * ng
+    g, w = got[9:].reshape(7, nyt, nxt), want[9:].reshape(7, nyt, nxt)
+    _check(list(g), list(w), tol=1e-13)
