@@ -20,7 +20,9 @@ state (4 random Fourier modes, velocity amplitude 0.05, Az amplitude 0.1, rho = 
 100 fixed steps of dt = 1e-3, checkpoint every 10 steps, loss = 1/2 |rho(T) - rho_target|^2 with the
 target from the forward solver at eta = 4e-3: forward and backward device times per step (the
 backward recomputes each segment's explicit stages from its checkpoint) and central-difference
-checks of dL/deta and of the derivative along a smooth perturbation of Az.
+checks of dL/deta and of the derivative along a smooth perturbation of Az; and "snapshot": the
+headline run for 100 steps with a snapshot file in the reference's format (941 MB at 4096^2) written
+every 50 steps by the asynchronous writer, against the same steps without files.
 Multi-GPU: replicas only (independent simulations per rank, no collective on the data path).
 """
 from __future__ import annotations
@@ -353,6 +355,9 @@ def run_gpu_arm(args):
     adjoint = None
     if not args.no_adjoint:
         adjoint = measure_adjoint(torch, m)
+    snapshot = None
+    if not args.no_snapshot and rank == 0:
+        snapshot = measure_snapshots(torch, m, ctx)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -370,6 +375,7 @@ def run_gpu_arm(args):
         "status": [status, status2],
         "batched": batched,
         "adjoint": adjoint,
+        "snapshot": snapshot,
     }
     ctx.close()
     if dist is not None:
@@ -381,6 +387,49 @@ def run_gpu_arm(args):
 
 
 BATCH_WORKLOAD = "mixed64_sizes256-1024_seed2024_eta1e-4..1e-2_cfl0.5"
+
+
+def measure_snapshots(torch, m, ctx, steps=100, every=50):
+    """Snapshot files in the reference's format (mhd_snapshot_write) every `every` steps of the
+    headline run, against the same steps without them: device time of the steps on the context's
+    stream, and wall time until the files are on disk. One snapshot is written first, so that the
+    writer's buffers exist before the timed region. Files go to a temporary directory. At 4096^2 a
+    file is 941 MB, a few tenths of a second of disk writing: the interval leaves the disk time to
+    keep up (a shorter one makes the writer's two slots, and so the stepping, wait for the disk)."""
+    import tempfile
+
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    nchunks = max(1, steps // every)
+
+    def timed(folder):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for k in range(nchunks):
+            ctx.run(every, record=False)
+            if folder:
+                ctx.snapshot_write(os.path.join(folder, f"snapshot_{k:06d}.dat"), 2, every, 0.0)
+        e1.record(stream)
+        e1.synchronize()
+        if folder:
+            ctx.snapshot_wait()
+        return e0.elapsed_time(e1), time.perf_counter() - t0
+
+    with tempfile.TemporaryDirectory() as folder:
+        ctx.snapshot_write(os.path.join(folder, "warmup.dat"), 2, every, 0.0)
+        ctx.snapshot_wait()
+        plain_ms, _ = timed(None)
+        snap_ms, wall_s = timed(folder)
+    nbytes = ctx.snapshot_bytes(2)
+    return {
+        "what": f"{nchunks} snapshot files (ng = 2) written every {every} steps while stepping",
+        "bytes_per_snapshot": nbytes,
+        "ms_per_step_plain": plain_ms / (nchunks * every),
+        "ms_per_step_with_snapshots": snap_ms / (nchunks * every),
+        "files_on_disk_s": wall_s,
+        "file_write_GBps": nchunks * nbytes / wall_s / 1e9,
+    }
 
 
 def measure_batched(torch, m, steps):
@@ -548,6 +597,60 @@ def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
     }
 
 
+def run_profile_case(args):
+    """Small fixed cases for profilers (nothing is timed or printed as a result):
+    batched  the mixed 64-instance batch of the "batched" section, two CFL steps at a fixed
+             decomposition (stage rows 128, tail 32, solver tiles of 32 rows), no autotuning;
+    adjoint  the 1024^2 state of the "adjoint" section, one 10-step trajectory (one checkpoint
+             segment): forward, then backward."""
+    import torch
+
+    import magnetohydrodynamics_simulator_b200 as m
+
+    torch.cuda.set_device(0)
+    if args.profile_case == "batched":
+        specs, ics = [], []
+        for n, e, seed in m.problems.mixed_batch(64):
+            fields, h = m.problems.random_instance(n, seed)
+            specs.append(dict(nx=n, ny=n, dx=h, dy=h, eta=e))
+            ics.append(fields)
+        b = m.Batch(specs)
+        for i, f in enumerate(ics):
+            b.set_state(i, f)
+        b.set_tuning(128, 32, 1, 32)
+        for _ in range(2):
+            b.step()
+        worst, _ = b.synchronize_status()
+        b.close()
+        return 0 if worst == 0 else 1
+    from magnetohydrodynamics_simulator_b200.autograd import state_from_potential
+
+    n, nsteps = 1024, 10
+    dx = 2 * np.pi / n
+    rng = np.random.default_rng(5)
+    X, Y = np.meshgrid(np.arange(n) * dx, np.arange(n) * dx)
+
+    def modes(amp, shift):
+        f = np.zeros((n, n))
+        for _ in range(4):
+            kx, ky = rng.integers(-4, 5, size=2)
+            f += amp * rng.uniform(0.5, 1.0) * np.sin(kx * (X + shift) + ky * (Y + shift) + rng.uniform(0, 2 * np.pi))
+        return torch.tensor(f, device="cuda")
+
+    vx, vy, az = modes(0.05, dx / 2), modes(0.05, dx / 2), modes(0.1, 0.0)
+    one = torch.ones(n, n, dtype=torch.float64, device="cuda")
+    u0 = state_from_potential(az, one, vx, vy, one, dx, dx).contiguous()
+    adj = m.Adjoint(n, n, dx, dx, 5e-3, 1e-3, nsteps, checkpoint_every=nsteps)
+    uT, g0, gT = torch.empty_like(u0), torch.empty_like(u0), torch.randn_like(u0)
+    ptr = lambda t: [t[k].data_ptr() for k in range(6)]  # noqa: E731
+    torch.cuda.synchronize()
+    adj.forward(ptr(u0), ptr(uT))
+    adj.backward(ptr(gT), ptr(g0))
+    torch.cuda.synchronize()
+    adj.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -560,7 +663,12 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-snapshot", action="store_true")
+    ap.add_argument("--profile-case", choices=("batched", "adjoint"), default=None,
+                    help="run a small fixed case for a profiler and exit (no measurement)")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)
