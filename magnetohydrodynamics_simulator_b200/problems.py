@@ -2,7 +2,9 @@
 
 Orszag-Tang and the decaying magnetic sine wave follow the reference's initial-condition
 functions (include/benchmarks.hpp:15-76 and :352-417): face B from a vector potential sampled at
-cell corners, total energy from the face values. The mixed-size batch generator builds the
+cell corners, total energy from the face values. The other five (Alfven wave, Gaussian density
+pulse, acoustic wave, sausage and kink pinches, benchmarks.hpp:78-350) set face B from cell-centre
+formulas, as the reference does. The mixed-size batch generator builds the
 synthetic ensemble of independent periodic runs (smoothed random density, Fourier-mode velocity
 and vector potential). Fields are returned as dense (ny, nx) float64 arrays in the order rho, mx,
 my, E, bxf, byf.
@@ -55,6 +57,89 @@ def sine_wave_config(n: int, b0: float = 1e-3, k: float = 1.0):
     """The configured decaying wave: Az = (B0/k) sin(kx x) sin(ky y), kx = ky = k on [0, 2pi)^2."""
     dx = grid_spacing(n)
     return sine_wave(n, n, dx, dx, b0 / k, k, k, use_sin=True), dx
+
+
+# ------------------------------------------------------------------ benchmarks.hpp:78-350
+# The reference's other five initial conditions set every field at cell centres of the padded
+# grid, face B included (each has B_x constant and B_y a function of x only, so div B = 0), and
+# convert with ConservedState::fromPrimitive (HLL.hpp:31-47). Only the physical cells are returned
+# (the driver's ghost fill overwrites the rest, integrator_main.cpp:52). The reference's pi literal
+# and its sampling positions are kept, quirks included.
+
+
+def _centres(nx, ny, dx, dy, offset=0.5):
+    x = (np.arange(nx) + offset) * dx
+    y = (np.arange(ny) + offset) * dy
+    return np.meshgrid(x, y)
+
+
+def _conserved(rho, vx, vy, p, bx, by):
+    """HLL.hpp:31-47 fromPrimitive (bx, by go to the face planes unchanged)."""
+    rho, vx, vy, p, bx, by = np.broadcast_arrays(rho, vx, vy, p, bx, by)
+    E = p / (GAMMA_GAS - 1.0) + 0.5 * rho * (vx * vx + vy * vy) + 0.5 * (bx * bx + by * by)
+    return [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, rho * vx, rho * vy, E, bx, by)]
+
+
+def alfven_wave(nx: int, ny: int, dx: float, dy: float):
+    """benchmarks.hpp:78-125: B_x = 1, B_y = 1e-3 sin(kx x), v_y = -B_y/sqrt(rho), rho = p = 1."""
+    X, _ = _centres(nx, ny, dx, dy)
+    kx = 2.0 * PI_REF / (nx * dx)
+    by = 1e-3 * np.sin(kx * X)
+    vy = -by / np.sqrt(1.0)
+    return _conserved(1.0, 0.0, vy, 1.0, 1.0, by)
+
+
+def gaussian_pulse(nx: int, ny: int, dx: float, dy: float):
+    """benchmarks.hpp:127-172: rho = 1 + exp(-5 r^2 / 4) around the centre, v = (1, 1), p = 1,
+    B = 0. The centre's y uses nx (y_mid = 0.5 nx dy, :140), as the reference writes it."""
+    X, Y = _centres(nx, ny, dx, dy)
+    x_mid, y_mid = 0.5 * nx * dx, 0.5 * nx * dy
+    d2 = (X - x_mid) * (X - x_mid) + (Y - y_mid) * (Y - y_mid)
+    rho = 1.0 + np.exp(-5 * d2 / (2.0 * 2.0))
+    return _conserved(rho, 1.0, 1.0, 1.0, 0.0, 0.0)
+
+
+def acoustic_wave(nx: int, ny: int, dx: float, dy: float):
+    """benchmarks.hpp:174-231: a right-moving sound wave of amplitude 1e-4 and wavenumber 4 pi / L
+    sampled at cell corners (x = i dx, :210), p0 = 1/gamma, B = 0."""
+    X, _ = _centres(nx, ny, dx, dy, offset=0.0)
+    p_bg = 1.0 / GAMMA_GAS
+    c = np.sqrt(GAMMA_GAS * p_bg / 1.0)
+    s = 1e-4 * np.sin(4 * PI_REF * X / (dx * nx))
+    return _conserved(1.0 + s + 0.0, (c / 1.0) * s, (c / 1.0) * 0.0, p_bg + (c * c) * (s + 0.0), 0.0, 0.0)
+
+
+def _channel_centre(nx, dx, ng=2):
+    # x_mid = 0.5 * nxt * dx (benchmarks.hpp:252, :305): half the PADDED width, i.e. ng cells right
+    # of the physical centre
+    return 0.5 * (nx + 2 * ng) * dx
+
+
+def sausage(nx: int, ny: int, dx: float, dy: float, ng: int = 2):
+    """benchmarks.hpp:233-287: low-beta pinch (B_y = 5 (r/0.2) exp(-r^2/0.04), p = 0.1 exp(.) +
+    0.1, rho = exp(.) + 0.1) with an m = 0 modulation 1 - 0.15 cos(2 pi y / H) of the channel."""
+    X, Y = _centres(nx, ny, dx, dy)
+    r = X - _channel_centre(nx, dx, ng)
+    H = ny * dy
+    pert = 1.0 - 0.15 * np.cos((2.0 * PI_REF / H) * Y)
+    rho = np.maximum(1.0 * np.exp(-(r * r) / (0.04 * pert)) + 0.1, 1e-4)
+    p = np.maximum(0.1 * np.exp(-(r * r) / (0.04 * pert)) + 0.1, 1e-4)
+    by = 5.0 * (r / np.sqrt(0.04)) * np.exp(-(r * r) / 0.04)
+    return _conserved(rho, 0.0, 0.0, p, 0.0, by)
+
+
+def kink(nx: int, ny: int, dx: float, dy: float, ng: int = 2):
+    """benchmarks.hpp:289-350: a current channel B_y = exp(-r^2/0.04), rho = p = exp(.) + 0.1,
+    seeded by v_x = 0.05 sin(2 pi y) exp(-r^2/0.04)."""
+    X, Y = _centres(nx, ny, dx, dy)
+    r = X - _channel_centre(nx, dx, ng)
+    env = np.exp(-(r * r) / 0.04)
+    vx = 0.05 * np.sin((2.0 * PI_REF) * Y) * env
+    return _conserved(1.0 * env + 0.1, vx, 0.0, 1.0 * env + 0.1, 0.0, 1.0 * env)
+
+
+FIXTURES = {"alfven_wave": alfven_wave, "gaussian_pulse": gaussian_pulse,
+            "acoustic_wave": acoustic_wave, "sausage": sausage, "kink": kink}
 
 
 def _fourier_modes(rng, X, Y, Lx, Ly, n_modes, amp_lo, amp_hi, kmax=4):

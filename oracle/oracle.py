@@ -187,6 +187,8 @@ def ref_lib():
         lib.ref_destroy.argtypes = [vp]
         lib.ref_init_orszag_tang.argtypes = [vp]
         lib.ref_init_dsw.argtypes = [vp]
+        lib.ref_init_fixture.argtypes = [vp, ctypes.c_int]
+        lib.ref_init_fixture.restype = ctypes.c_int
         lib.ref_set_state.argtypes = [vp] + [_dp] * 6
         lib.ref_get_state.argtypes = [vp] + [_dp] * 6
         lib.ref_get_primitives.argtypes = [vp] + [_dp] * 5
@@ -222,6 +224,12 @@ class Reference:
 
     def init_dsw(self):
         self.lib.ref_init_dsw(self.h)
+
+    FIXTURES = ("alfven_wave", "gaussian_pulse", "acoustic_wave", "sausage", "kink")
+
+    def init_fixture(self, name):
+        """benchmarks.hpp:78-350, by name (FIXTURES)."""
+        assert self.lib.ref_init_fixture(self.h, self.FIXTURES.index(name)) == 0
 
     def set_state(self, fields):
         fs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]

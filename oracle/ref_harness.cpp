@@ -10,6 +10,8 @@
 //   ref_create            src/integrator_main.cpp:34-48   (grids, workspace, tableau, solver)
 //   ref_init_orszag_tang  benchmarks.hpp:15-76 + integrator_main.cpp:52-53
 //   ref_init_dsw          benchmarks.hpp:352-417 + integrator_main.cpp:52-53
+//   ref_init_fixture      benchmarks.hpp:78-350 (Alfven wave, Gaussian pulse, acoustic wave,
+//                         sausage, kink) + integrator_main.cpp:52-53
 //   ref_set_alpha         integrator_main.cpp:58-60 / :87-95 (generate_A_matrix + compute)
 //   ref_step              integrator_main.cpp:99 (IMEX, solvers.hpp:491-613)
 //   ref_cfl               diagnostics.hpp:44-88
@@ -87,6 +89,21 @@ void ref_init_dsw(void* h) {
     RefSim* s = static_cast<RefSim*>(h);
     decaying_magnetic_sine_wave_initial_conditions(s->state, s->mem);
     finish_setup(s);
+}
+
+// which: 0 Alfven wave, 1 Gaussian density pulse, 2 acoustic wave, 3 sausage, 4 kink.
+int ref_init_fixture(void* h, int which) {
+    RefSim* s = static_cast<RefSim*>(h);
+    switch (which) {
+        case 0: alfven_wave_test_initial_values(s->state); break;
+        case 1: gaussian_density_pulse_test_initial_values(s->state); break;
+        case 2: acoustic_wave_test_initial_values(s->state); break;
+        case 3: sausage_instability_initial_conditions(s->state); break;
+        case 4: kink_instability_initial_conditions(s->state); break;
+        default: return -1;
+    }
+    finish_setup(s);
+    return 0;
 }
 
 // Dense row-major (j*nx + i) physical arrays -> padded Grid, then ghosts + primitives.

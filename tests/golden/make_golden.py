@@ -166,6 +166,22 @@ def main():
     out.update(pack("state", ref.get_state()))
     np.savez(os.path.join(OUT, "snapshot20x14_ref.npz"), **out)
 
+    # 8. The reference's five other initial conditions (benchmarks.hpp:78-350) on a 32x24 grid with
+    #    dx != dy, and 5 steps of the reference driver loop from each (dynamic CFL, eta = 5e-3)
+    nx, ny = 32, 24
+    dx, dy = 2 * PI_REF / nx, 1.5 * PI_REF / ny
+    eta = 5e-3
+    out = dict(nx=nx, ny=ny, dx=dx, dy=dy, eta=eta, steps=5, names=np.array(Reference.FIXTURES))
+    for name in Reference.FIXTURES:
+        ref = Reference(nx, ny, dx, dy, eta)
+        ref.init_fixture(name)
+        out.update(pack(f"{name}_ic", ref.get_state()))
+        dts, prods = ref.run(5)
+        out[f"{name}_dts"] = dts
+        out[f"{name}_cg_products"] = prods
+        out.update(pack(f"{name}_final", ref.get_state()))
+    np.savez(os.path.join(OUT, "fixtures32x24_ref.npz"), **out)
+
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
