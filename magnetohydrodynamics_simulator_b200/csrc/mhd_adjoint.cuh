@@ -31,7 +31,6 @@ struct PrimAdj {
     double rho, vx, vy, p, bx, by;
 };
 
-constexpr double kInvGm1 = 1.0 / (kGammaGas - 1.0);  // d E / d p of the ideal-gas energy
 
 // fast_speed (HLL.hpp:107-122): given the adjoint of c_f, accumulate into w's adjoint and bn's.
 __device__ __forceinline__ void fast_speed_vjp(const Prim& w, double bn, double ac, PrimAdj& aw,
@@ -69,7 +68,7 @@ __device__ __forceinline__ void phys_flux_vjp(const Prim& w, const Flux& aF, Pri
     const double b2 = w.bx * w.bx + w.by * w.by;
     const double pt = w.p + 0.5 * b2;
     const double vb = w.vx * w.bx + w.vy * w.by;
-    const double E = w.p / (kGammaGas - 1.0) + 0.5 * (w.rho * v2 + b2);
+    const double E = w.p * kInvGm1 + 0.5 * (w.rho * v2 + b2);
     double apt, aE, avb;
     if (DIR == 0) {
         // rho vx | rho vx vx + pt - bx bx | rho vx vy - bx by | (E + pt) vx - bx vb | vx by - vy bx

@@ -282,7 +282,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
                 Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
             }
             Dn.by = Up.by = slot(c + 1)[5 * 32 + lane];  // byf of row c+1
-            fy = hll<1>(Dn, Up);
+            fy = hll<1, MODE == 1>(Dn, Up);
         }
         // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of
         //      i+1. With kXReuse every lane limits its own column's slope once and hands its lower
@@ -308,7 +308,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
             xrecon(Pp[1], L.p, R.p);
             xrecon(Pbyc[0], L.by, R.by);
             L.bx = R.bx = shdn(slot(c)[4 * 32 + lane], 1);  // bxf(i+1, c)
-            fx = hll<0>(L, R);
+            fx = hll<0, MODE == 1>(L, R);
         }
         // ---- CORNER (i, c): eN = -Fx^By(i-1, c), eS = -Fx^By(i-1, c-1), eE = Fy^Bx(i, c-1),
         //      eW = Fy^Bx(i-1, c-1); corner velocity = mean of the 4 cells
