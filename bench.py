@@ -10,7 +10,9 @@ Lines printed (rank 0, one JSON line):
                       copied host->device and back every step; roofline of the dominant kernel;
                       cpu_baseline = the reference's own IMEX step (compiled here) on 1 host core.
   --impl reference    the reference's CPU implementation (oracle/_ref, compiled from the
-                      reference's headers) on the same workload, a bounded sample per step.
+                      reference's headers) on the same workload, a bounded sample per step, as
+                      independent single-threaded replicas on the host's cores (the reference has
+                      no threads of its own); value = all replicas' zone-updates/s.
 The default line also carries "batched": 64 independent periodic runs of seeded sizes from
 {256, 384, 512, 768, 1024}^2 (random smooth states, eta log-uniform in [1e-4, 1e-2], CFL dt per
 instance), stepped as one batch (one launch per stage, CUDA graph, autotuned decomposition) and,
@@ -174,6 +176,58 @@ def cpu_reference_step_rate(n, steps, warmup=0):
     return n * n * steps / sec, sec
 
 
+# Host memory of one reference simulation (grids, workspace, reconstruction, sparse matrix),
+# measured at 512^2: about 1.1 kB per zone.
+REF_BYTES_PER_ZONE = 1200
+
+
+def max_over_ranks(dist, value, device="cpu"):
+    """The largest of every rank's value: multi-rank times are the slowest rank's."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _reference_replica(core, n, steps, warmup, conn):
+    """One reference simulation in its own process, pinned to one host core."""
+    try:
+        if core is not None:
+            os.sched_setaffinity(0, {core})
+        conn.send(cpu_reference_step_rate(n, steps, warmup))
+    except Exception as e:  # reported, not raised: the parent decides
+        conn.send(repr(e))
+    conn.close()
+
+
+def reference_replicas(n, steps, warmup, procs):
+    """`procs` independent reference simulations at once, one per host core (the reference is
+    single-threaded, so replicas are how it uses the host's cores). Returns the whole-job
+    zone-updates/s (procs * n^2 * steps / the slowest replica's time) and that time."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    cores = sorted(os.sched_getaffinity(0))
+    jobs = []
+    for k in range(procs):
+        a, b = ctx.Pipe(duplex=False)
+        p = ctx.Process(target=_reference_replica, args=(cores[k % len(cores)], n, steps, warmup, b))
+        p.start()
+        jobs.append((p, a))
+    results = []
+    for p, a in jobs:
+        results.append(a.recv())
+        p.join()
+    bad = [r for r in results if not isinstance(r, tuple)]
+    if bad:
+        raise RuntimeError(f"reference replica failed: {bad[0]}")
+    sec = max(r[1] for r in results)
+    return procs * n * n * steps / sec, sec
+
+
 def run_reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -185,18 +239,29 @@ def run_reference_arm(args):
                           "(the reference sources were absent when __graft_entry__.build() ran)"}))
         return 0
     # Each step is a bounded sample of the workload: one IMEX step of the same Orszag-Tang
-    # problem on the largest grid (<= 4096^2) whose K + 1 steps fit in ~150 s on one core,
-    # sized from a timed 512^2 probe step.
+    # problem on the largest grid (<= 4096^2) whose K + 1 steps fit in ~60 s of one core (sized
+    # from a timed 512^2 probe step), run as independent replicas on as many host cores as the
+    # host memory holds.
     probe_rate, _ = cpu_reference_step_rate(512, 1)
-    budget = 150.0
+    budget = 60.0
     n = 4096
     while n > 256 and (args.steps + 1) * n * n / probe_rate > budget:
         n //= 2
-    rate, sec = cpu_reference_step_rate(n, args.steps, warmup=min(args.warmup, 1))
+    try:
+        import psutil
+
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 8 << 30
+    cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, int(0.5 * avail // (REF_BYTES_PER_ZONE * n * n))))
+    warm = min(args.warmup, 1)
+    rate, sec = reference_replicas(n, args.steps, warm, procs)
     sample = (f"{args.steps} steps of the reference driver loop (its own CFL dt, matrix rebuilt "
               f"each step, IMEX) on the Orszag-Tang problem at {n}x{n}, eta 1e-4, after "
-              f"{min(args.warmup, 1)} untimed step; reference headers compiled -O3 -ffast-math, "
-              f"single thread")
+              f"{warm} untimed step, in each of {procs} concurrent single-threaded replicas pinned "
+              f"to {procs} of the host's {cores} cores (slowest replica's time); reference headers "
+              f"compiled -O3 -ffast-math")
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
@@ -204,7 +269,7 @@ def run_reference_arm(args):
         "impl": "reference",
         "config": {"workload": WORKLOAD, "grid": [N_GRID, N_GRID], "sampled_grid": [n, n],
                    "eta": ETA, "cfl": COURANT, "parallelism": f"replicas{args.gpus}"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -267,11 +332,7 @@ def run_gpu_arm(args):
     ctx.lib.mhd_kernel_times(ctx.h, kt, ctypes.byref(ksteps))
     ctx.lib.mhd_set_kernel_timing(ctx.h, 0)
     prods = ctx.last_cg_products()
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(dist, ms, "cuda")
     zones = float(n) * n
     value = world * zones * args.steps / (ms_max * 1e-3)
 
@@ -288,11 +349,7 @@ def run_gpu_arm(args):
         ctx.get_state_into(pinned)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
     e2e_value = world * zones * e2e_steps / (e2e_ms * 1e-3)
     status2 = ctx.synchronize_status()
 
