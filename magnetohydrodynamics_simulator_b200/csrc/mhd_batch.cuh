@@ -199,6 +199,7 @@ enum CgInstStatus : int { kCgActive = 0, kCgConverged = 1, kCgZero = 2, kCgBreak
 struct CgBInst {
     double cx, cy, diag, invdiag;  // matrix of this solve
     double alpha, beta;            // CG step scalars
+    double alpha_prev;             // alpha of the previous iteration (paired updates of x)
     double bb, absNew, thr, rr, pAp;
     long long products;
     int status;
@@ -234,7 +235,7 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     return g;
 }
 
-// Prefix sum over the chunk's instances of the work units of those with pick(status) (thread 0),
+// Prefix sum over the chunk's instances of the work units of those with pick(instance) (thread 0),
 // then a block barrier. Every block computes the same prefix from the same statuses.
 template <class Pick>
 __device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long long* pref, Pick pick) {
@@ -242,7 +243,7 @@ __device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long lo
         long long s = 0;
         for (int li = 0; li < ninst; ++li) {
             pref[li] = s;
-            if (pick(sh[li].status)) s += sh[li].units;
+            if (pick(sh[li])) s += sh[li].units;
         }
         pref[ninst] = s;
     }
@@ -293,7 +294,7 @@ __device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst
 // One sweep over this warp's items: PH 0 the right-hand side (cg_rhs_segment), 1 the first
 // iteration, 2 a later one (cg_iter_segment); NV sums per instance. Ends with the block's partials
 // of every instance published in part_out.
-template <int PH, int NV>
+template <int PH, int NV, int XM = kXSkip>
 __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const long long* pref,
                                           double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
@@ -314,6 +315,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         s.invdiag = sh[li].invdiag;
         s.alpha = sh[li].alpha;
         s.beta = sh[li].beta;
+        s.alpha_prev = sh[li].alpha_prev;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if constexpr (PH == 0) {
             cg_rhs_segment(g, s, sx, r0, r1, dir, g.r[0], ring, acc);
@@ -322,7 +324,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
             double* rk1 = odd ? g.r[0] : g.r[1];
             const double* pkm1 = odd ? g.p[0] : g.p[1];
             double* pk = odd ? g.p[1] : g.p[0];
-            cg_iter_segment<PH == 1>(g, s, sx, r0, r1, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<PH == 1, XM>(g, s, sx, r0, r1, dir, rk, pkm1, rk1, pk, ring, acc);
         }
 #pragma unroll
         for (int c = 0; c < NV; ++c)
@@ -397,6 +399,7 @@ k_cg_batch(CgBatchArgs a) {
         S.diag = 1 + 2 * (S.cx + S.cy);
         S.invdiag = (S.diag == 0.0) ? 1.0 : 1.0 / S.diag;
         S.alpha = 0.0;
+        S.alpha_prev = 0.0;
         S.beta = 0.0;
         S.products = 0;
         S.rr = 0.0;
@@ -407,7 +410,7 @@ k_cg_batch(CgBatchArgs a) {
                   ((a.order == 0) ? I.D.ny : (I.D.ny + a.rows - 1) / a.rows);
     }
     __syncthreads();
-    auto is_active = [](int st) { return st == kCgActive; };
+    auto is_active = [](const CgBInst& S) { return S.status == kCgActive; };
 
     // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
     cgb_prefix(sh, a.ninst, pref, is_active);
@@ -436,8 +439,11 @@ k_cg_batch(CgBatchArgs a) {
     for (int k = 0;; ++k) {
         // ---- iteration k: p_k, q_k, x_{k+1}, r_{k+1}; r.r, r.z, z.Az, z.q_k
         cgb_prefix(sh, a.ninst, pref, is_active);
-        if (k == 0) cgb_phase<1, 4>(a, sh, pref, wsum, ring, k, dir, part(phase));
-        else cgb_phase<2, 4>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        // (all instances run iteration k together, so k's x mode is the same for all of them)
+        if (k == 0) cgb_phase<1, 4, kXSkip>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        else if (cg_xmode(k) == kXSkip) cgb_phase<2, 4, kXSkip>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        else if (cg_xmode(k) == kXPairFirst) cgb_phase<2, 4, kXPairFirst>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        else cgb_phase<2, 4, kXPair>(a, sh, pref, wsum, ring, k, dir, part(phase));
         if (!barrier_or_quit()) return;
         int active = 0;
         for (int li = wid; li < a.ninst; li += NW) {
@@ -459,6 +465,7 @@ k_cg_batch(CgBatchArgs a) {
                     if (!(S.pAp > 0.0)) {
                         S.status = kCgBreakdown;
                     } else {
+                        S.alpha_prev = S.alpha;
                         S.alpha = S.absNew / S.pAp;
                         active = 1;
                     }
@@ -471,13 +478,33 @@ k_cg_batch(CgBatchArgs a) {
     }
 
     // x = 0 for a vanished right-hand side (Eigen returns the zero vector) and on breakdown
-    cgb_prefix(sh, a.ninst, pref, [](int st) { return st == kCgZero || st == kCgBreakdown; });
+    cgb_prefix(sh, a.ninst, pref, [](const CgBInst& S) {
+        return S.status == kCgZero || S.status == kCgBreakdown || (S.status == kCgCapped && S.products == 0);
+    });
     cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const int nx = I.D.nx;
         const int i = sx * CG_W - CG_HALO + lane;
         if (lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx)
             for (int j = r0; j < r1; ++j) I.x[(size_t)j * nx + i] = 0.0;
+    });
+    // solutions whose last iteration was even (an odd number of products) still lack that
+    // iteration's alpha_k p_k (x moves every second iteration, see mhd_cg_sweep.cuh)
+    __syncthreads();  // every warp is done with the prefix above
+    cgb_prefix(sh, a.ninst, pref, [](const CgBInst& S) {
+        return (S.status == kCgConverged || S.status == kCgCapped) && (S.products & 1) == 1;
+    });
+    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+        const BatchInst& I = a.insts[a.inst0 + li];
+        const CgBInst& S = sh[li];
+        const double* pl = ((S.products - 1) & 1) ? I.p[1] : I.p[0];
+        const int nx = I.D.nx;
+        const int i = sx * CG_W - CG_HALO + lane;
+        if (lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx)
+            for (int j = r0; j < r1; ++j) {
+                const size_t g = (size_t)j * nx + i;
+                I.x[g] = (S.products == 1) ? S.alpha * pl[g] : fma(S.alpha, pl[g], I.x[g]);
+            }
     });
     if (blockIdx.x == 0) {
         for (int li = tid; li < a.ninst; li += CGS_NT) {

@@ -7,9 +7,13 @@
 // strip and two halo columns on each side. 5-point products are formed from register windows over
 // rows (y neighbours) and shuffles (x neighbours); rows are prefetched into a per-warp shared-memory
 // ring with cp.async. One sweep per iteration (after the right-hand-side sweep):
-//   p_k = z_k + beta_k p_{k-1}; q_k = A p_k; x_{k+1} = x_k + alpha_k p_k;
-//   r_{k+1} = r_k - alpha_k q_k; z_{k+1} = r_{k+1}/d; partials r.r, r.z, z.Az, z.q_k
-//   (reads r_k, p_{k-1}, x_k; writes x_{k+1}, r_{k+1}, p_k)
+//   p_k = z_k + beta_k p_{k-1}; q_k = A p_k; r_{k+1} = r_k - alpha_k q_k; z_{k+1} = r_{k+1}/d;
+//   partials r.r, r.z, z.Az, z.q_k (reads r_k, p_{k-1}; writes r_{k+1}, p_k).
+// The solution moves every second iteration: odd k also forms
+//   x_{k+1} = (x_{k-1} + alpha_{k-1} p_{k-1}) + alpha_k p_k
+// from the p_{k-1} the sweep reads anyway -- the two updates of a one-per-iteration CG, in the same
+// order -- so even iterations neither read nor write x (32 instead of 48 bytes per cell). A solve
+// that stops after an even iteration adds its last alpha_k p_k in one elementwise pass.
 // The next step length needs p_{k+1}.A p_{k+1}; with p_{k+1} = z_{k+1} + beta p_k and A symmetric
 // it is z.Az + 2 beta z.q_k + beta^2 p_k.q_k, all known after this sweep, so no second sweep over
 // the vectors is needed. In exact arithmetic these are Eigen's iterates; the step lengths differ
@@ -52,7 +56,18 @@ struct CgSweepArgs {
 struct CgScal {
     double invdiag, beta, alpha;
     double cx, cy, diag;
+    double alpha_prev;  // alpha_{k-1} (odd iterations fold its update of x into theirs)
 };
+
+// How an iteration's sweep treats the solution x (see the header comment).
+enum CgXMode : int {
+    kXSkip = 0,      // even k: x neither read nor written
+    kXPairFirst = 1, // k = 1: x_2 = alpha_0 p_0 + alpha_1 p_1 (x_0 = 0 is not read)
+    kXPair = 2,      // odd k >= 3: x_{k+1} = (x_{k-1} + alpha_{k-1} p_{k-1}) + alpha_k p_k
+};
+__device__ __forceinline__ int cg_xmode(long long k) {
+    return (k & 1) == 0 ? kXSkip : (k == 1 ? kXPairFirst : kXPair);
+}
 
 // (A p) at a corner from its column window and x neighbours, summed in increasing column order
 // for interior rows (bottom, left, centre, right, top) as the reference's compressed product.
@@ -166,12 +181,11 @@ __device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgSca
 }
 
 // One CG iteration k over rows [r0w, r1w) of column strip sx (the sweep of the header comment).
-// FIRST: k = 0,
-// p_0 = z_0 and x_0 = 0 (p_{-1} and x are not read). acc[0..3] receive r.r, r.z, z.Az, z.q_k of
+// FIRST: k = 0, p_0 = z_0 (p_{-1} is not read). XM: the iteration's CgXMode. acc[0..3] receive r.r, r.z, z.Az, z.q_k of
 // the owned cells. Sweep row t holds grid row jfirst + (t - 2) dir, t = 0 .. nrows + 3; at sweep
 // row t the warp forms p_k of row t, q_k, r_{k+1}, z_{k+1} of row t-1 and A z_{k+1} and the outputs
 // of row t-2. Row t is copied into slot t % CG_RING by the end of sweep row t - 6.
-template <bool FIRST>
+template <bool FIRST, int XM>
 __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
                                                 int r1w, int dir, const double* rk, const double* pkm1,
                                                 double* rk1, double* pk, double* ring,
@@ -191,10 +205,8 @@ __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgSc
             double* sl = slot(t);
             const size_t rp = (size_t)wrap(jfirst + (t - 2) * dir, ny) * nx + iw;
             cp_async8(&sl[lane], &rk[rp]);
-            if constexpr (!FIRST) {
-                cp_async8(&sl[32 + lane], &pkm1[rp]);
-                cp_async8(&sl[64 + lane], &a.x[rp]);
-            }
+            if constexpr (!FIRST) cp_async8(&sl[32 + lane], &pkm1[rp]);
+            if constexpr (XM == kXPair) cp_async8(&sl[64 + lane], &a.x[rp]);
         }
         cp_async_commit();
     };
@@ -231,10 +243,13 @@ __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgSc
             const double z_hi = (dir > 0) ? z_b : z_a;
             const double az = stencil(z_lo, zl, z_o, zr, z_hi, s);
             if (owner) {
-                double xv;
-                if constexpr (FIRST) xv = s.alpha * p_a;
-                else xv = slot(t - 2)[64 + lane] + s.alpha * p_a;
-                a.x[g] = xv;
+                if constexpr (XM != kXSkip) {
+                    const double* so = slot(t - 2);  // p_{k-1} (and x_{k-1}) of the output row
+                    const double xm = (XM == kXPairFirst)
+                                          ? s.alpha_prev * so[32 + lane]
+                                          : fma(s.alpha_prev, so[32 + lane], so[64 + lane]);
+                    a.x[g] = fma(s.alpha, p_a, xm);
+                }
                 rk1[g] = r_o;
                 pk[g] = p_a;
                 acc[0] += r_o * r_o;
@@ -298,6 +313,7 @@ k_cg_sweep(CgSweepArgs a) {
     s.invdiag = (s.diag == 0.0) ? 1.0 : 1.0 / s.diag;
     s.beta = 0.0;
     s.alpha = 0.0;
+    s.alpha_prev = 0.0;
     unsigned long long target = 0;
     const unsigned long long deadline =
         global_timer_ns() + (unsigned long long)(a.timeout_s * 1e9);
@@ -338,10 +354,14 @@ k_cg_sweep(CgSweepArgs a) {
     bool breakdown = !isfinite(bb);
     bool converged = zero_solution;
     double rr_final = 0.0;
+    long long k_last = -1;     // the last iteration swept
+    double alpha_last = 0.0;   // its step length
 
     if (!zero_solution && !breakdown) {
         s.alpha = absNew / pAp;
         for (long long k = 0; k < a.max_iters; ++k) {
+            k_last = k;
+            alpha_last = s.alpha;
             const bool odd = (k & 1) != 0;
             const double* rk = odd ? a.r[1] : a.r[0];
             double* rk1 = odd ? a.r[0] : a.r[1];
@@ -352,8 +372,19 @@ k_cg_sweep(CgSweepArgs a) {
                 for (int w = wfirst; w < a.nwarps; w += wstride) {
                     const int sx = w % a.strips_x, r0w = (w / a.strips_x) * a.seg_h;
                     const int r1w = min(r0w + a.seg_h, a.D.ny);
-                    if (k == 0) cg_iter_segment<true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
-                    else cg_iter_segment<false>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    switch (cg_xmode(k)) {
+                        case kXSkip:
+                            if (k == 0)
+                                cg_iter_segment<true, kXSkip>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                            else
+                                cg_iter_segment<false, kXSkip>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                            break;
+                        case kXPairFirst:
+                            cg_iter_segment<false, kXPairFirst>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                            break;
+                        default:
+                            cg_iter_segment<false, kXPair>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+                    }
                 }
                 publish<4>(acc, part(phase) + (size_t)blockIdx.x * 4, red);
             }
@@ -373,11 +404,20 @@ k_cg_sweep(CgSweepArgs a) {
             s.beta = absNew / absOld;
             pAp = v[2] + 2.0 * s.beta * v[3] + s.beta * s.beta * pAp;
             if (!(pAp > 0.0)) { breakdown = true; break; }
+            s.alpha_prev = s.alpha;
             s.alpha = absNew / pAp;
         }
     }
-    if (zero_solution || breakdown) {
-        // x = 0 (Eigen returns the zero vector when b == 0); on breakdown the status says so
+    if (!zero_solution && !breakdown && k_last >= 0 && cg_xmode(k_last) == kXSkip) {
+        // the last iteration was even: add its alpha_k p_k (x_0 = 0 when it was the first)
+        const double* pl = (k_last & 1) ? a.p[1] : a.p[0];
+        const size_t n = (size_t)a.D.nx * a.D.ny;
+        for (size_t g = (size_t)blockIdx.x * CGS_NT + tid; g < n; g += (size_t)G * CGS_NT)
+            a.x[g] = (k_last == 0) ? alpha_last * pl[g] : fma(alpha_last, pl[g], a.x[g]);
+    }
+    if (zero_solution || breakdown || k_last < 0) {
+        // x = 0 (Eigen returns the zero vector when b == 0, and x0 = 0 when no iteration may run);
+        // on breakdown the status says so
         const int nx = a.D.nx, ny = a.D.ny;
         const size_t n = (size_t)nx * ny;
         for (size_t g = (size_t)blockIdx.x * CGS_NT + tid; g < n; g += (size_t)G * CGS_NT) a.x[g] = 0.0;
