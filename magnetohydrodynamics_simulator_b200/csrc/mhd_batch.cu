@@ -199,7 +199,7 @@ mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
     b->stage_grid[0] = grid_for(b->stage_occ[0], b->num_sms, b->n_stage_items, SW_WARPS);
     b->stage_grid[1] = grid_for(b->stage_occ[1], b->num_sms, b->n_stage_items, SW_WARPS);
     b->fin_grid = grid_for(b->fin_occ, b->num_sms, b->n_fin_items, FS_WARPS);
-    b->cg_grid = grid_for(b->cg_occ, b->num_sms, cg_warps, CGS_NT / 32);
+    b->cg_grid = grid_for(b->cg_occ, b->num_sms, cg_warps, CGB_NW);
     b->tuning.stage_rows = t.stage_rows;
     b->tuning.cg_rows = t.cg_rows;
     b->tuning.cg_order = t.cg_order;
@@ -223,8 +223,8 @@ mhd_status launch_cg_chunks(mhd_batch* b, const BatchInst* insts, int solve, boo
         a.timeout_s = b->timeout_s;
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(b->cg_grid);
-        cfg.blockDim = dim3(CGS_NT);
-        cfg.dynamicSmemBytes = kCgRingBytes;
+        cfg.blockDim = dim3(CGB_NT);
+        cfg.dynamicSmemBytes = kCgbSmemBytes;
         cfg.stream = b->stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
@@ -360,8 +360,8 @@ mhd_status mhd_batch_create(const mhd_params* params, int count, void* stream, m
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->fin_occ, k_finalize_batch, 32 * FS_WARPS,
                                                       0) != cudaSuccess ||
         cudaFuncSetAttribute(k_cg_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kCgRingBytes) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->cg_occ, k_cg_batch, CGS_NT, kCgRingBytes) !=
+                             (int)kCgbSmemBytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->cg_occ, k_cg_batch, CGB_NT, kCgbSmemBytes) !=
             cudaSuccess ||
         b->stage_occ[0] < 1 || b->stage_occ[1] < 1 || b->fin_occ < 1 || b->cg_occ < 1) {
         cudaGetLastError();

@@ -193,6 +193,16 @@ k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restric
 // is active.
 
 constexpr int CGB_MAX_INST = 64;
+// Threads per block of the batched solver (its own size: the per-warp partial sums of 64 instances
+// live in dynamic shared memory beside the rows' rings).
+#ifndef MHD_CGB_NT
+#define MHD_CGB_NT 512
+#endif
+constexpr int CGB_NT = MHD_CGB_NT;
+constexpr int CGB_NW = CGB_NT / 32;
+// dynamic shared memory of a k_cg_batch block: the warps' row rings, then wsum[CGB_NW][64][4]
+constexpr size_t kCgbRingBytes = (size_t)CGB_NW * CG_RING * CG_SLOT * sizeof(double);
+constexpr size_t kCgbSmemBytes = kCgbRingBytes + (size_t)CGB_NW * CGB_MAX_INST * 4 * sizeof(double);
 
 enum CgInstStatus : int { kCgActive = 0, kCgConverged = 1, kCgZero = 2, kCgBreakdown = 3, kCgCapped = 4 };
 
@@ -254,7 +264,7 @@ __device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long lo
 template <class F>
 __device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst* sh,
                                              const long long* pref, F&& f) {
-    constexpr int NW = CGS_NT / 32;
+    constexpr int NW = CGB_NW;
     const long long nw = (long long)gridDim.x * NW;
     const long long g = (long long)blockIdx.x * NW + (threadIdx.x >> 5);
     const long long T = pref[a.ninst];
@@ -298,7 +308,7 @@ template <int PH, int NV, int XM = kXSkip>
 __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const long long* pref,
                                           double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
-    constexpr int NW = CGS_NT / 32;
+    constexpr int NW = CGB_NW;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int li = lane; li < a.ninst; li += 32)
 #pragma unroll
@@ -336,7 +346,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         __syncwarp();
     });
     __syncthreads();
-    for (int q = threadIdx.x; q < a.ninst * NV; q += CGS_NT) {
+    for (int q = threadIdx.x; q < a.ninst * NV; q += CGB_NT) {
         const int li = q / NV, c = q - li * NV;
         double v = 0.0;
         for (int w2 = 0; w2 < NW; ++w2) v += wsum[w2][li][c];
@@ -360,20 +370,21 @@ __device__ __forceinline__ void cgb_span_sum(const double* part, int li, double 
         for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
 }
 
-static __global__ void __launch_bounds__(CGS_NT, MHD_CG_MIN_BLOCKS)
+static __global__ void __launch_bounds__(CGB_NT, MHD_CG_MIN_BLOCKS)
 k_cg_batch(CgBatchArgs a) {
-    constexpr int NW = CGS_NT / 32;
+    constexpr int NW = CGB_NW;
     __shared__ CgBInst sh[CGB_MAX_INST];
-    __shared__ double wsum[NW][CGB_MAX_INST][4];
     __shared__ long long pref[CGB_MAX_INST + 1];
     __shared__ int sflag;
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double cg_ring_mem[];
 #else
-    static double cg_ring_mem[(CGS_NT / 32) * CG_RING * CG_SLOT];
+    static double cg_ring_mem[kCgbSmemBytes / sizeof(double)];
 #endif
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     double* const ring = cg_ring_mem + (size_t)wid * CG_RING * CG_SLOT;
+    double (*const wsum)[CGB_MAX_INST][4] =
+        reinterpret_cast<double (*)[CGB_MAX_INST][4]>(cg_ring_mem + kCgbRingBytes / sizeof(double));
     unsigned long long target = 0;
     const unsigned long long deadline = global_timer_ns() + (unsigned long long)(a.timeout_s * 1e9);
     double* const part0 = a.partials;
@@ -390,7 +401,7 @@ k_cg_batch(CgBatchArgs a) {
     };
 
     // matrix of each instance's solve (the coefficient was set by this step's coefficients)
-    for (int li = tid; li < a.ninst; li += CGS_NT) {
+    for (int li = tid; li < a.ninst; li += CGB_NT) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const double am = I.C->alpha;
         CgBInst& S = sh[li];
@@ -507,7 +518,7 @@ k_cg_batch(CgBatchArgs a) {
             }
     });
     if (blockIdx.x == 0) {
-        for (int li = tid; li < a.ninst; li += CGS_NT) {
+        for (int li = tid; li < a.ninst; li += CGB_NT) {
             const BatchInst& I = a.insts[a.inst0 + li];
             const CgBInst& S = sh[li];
             I.st->cg_products[a.solve_index] = S.products;

@@ -29,7 +29,10 @@
 
 namespace mhd {
 
-constexpr int CGS_NT = 512;  // threads per block (16 warps)
+#ifndef MHD_CGS_NT
+#define MHD_CGS_NT 512
+#endif
+constexpr int CGS_NT = MHD_CGS_NT;  // threads per block (16 warps)
 #ifndef MHD_CG_MIN_BLOCKS
 #define MHD_CG_MIN_BLOCKS 1      // blocks per SM (the prefetch lives in shared memory)
 #endif
