@@ -219,7 +219,11 @@ def reference_replicas(n, steps, warmup, procs):
         jobs.append((p, a))
     results = []
     for p, a in jobs:
-        results.append(a.recv())
+        try:
+            results.append(a.recv())
+        except EOFError:  # the process died without an answer (killed, out of memory, ...)
+            p.join()
+            results.append(f"replica process ended without a result (exit code {p.exitcode})")
         p.join()
     bad = [r for r in results if not isinstance(r, tuple)]
     if bad:
