@@ -245,17 +245,30 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     return g;
 }
 
-// Prefix sum over the chunk's instances of the work units of those with pick(instance) (thread 0),
-// then a block barrier. Every block computes the same prefix from the same statuses.
+// Prefix sum over the chunk's instances (at most 64) of the work units of those with
+// pick(instance), by a scan in the first warp (lane l: instances l and l + 32), then a block
+// barrier. Every block computes the same prefix from the same statuses.
 template <class Pick>
 __device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long long* pref, Pick pick) {
-    if (threadIdx.x == 0) {
-        long long s = 0;
-        for (int li = 0; li < ninst; ++li) {
-            pref[li] = s;
-            if (pick(sh[li])) s += sh[li].units;
+    static_assert(CGB_MAX_INST <= 64, "two instances per lane");
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        const long long u0 = (l < ninst && pick(sh[l])) ? sh[l].units : 0;
+        const long long u1 = (l + 32 < ninst && pick(sh[l + 32])) ? sh[l + 32].units : 0;
+        long long s0 = u0, s1 = u1;  // inclusive scans over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y0 = __shfl_up_sync(0xffffffffu, s0, o);
+            const long long y1 = __shfl_up_sync(0xffffffffu, s1, o);
+            if (l >= o) {
+                s0 += y0;
+                s1 += y1;
+            }
         }
-        pref[ninst] = s;
+        const long long first = __shfl_sync(0xffffffffu, s0, 31);  // instances 0 .. 31
+        if (l < ninst) pref[l] = s0 - u0;
+        if (l + 32 < ninst) pref[l + 32] = first + s1 - u1;
+        if (l == 31) pref[ninst] = first + s1;
     }
     __syncthreads();
 }
@@ -357,14 +370,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
 // Sum of instance li's block partials (all blocks, fixed order); identical in every lane.
 template <int NV>
 __device__ __forceinline__ void cgb_span_sum(const double* part, int li, double (&v)[NV]) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int c = 0; c < NV; ++c) v[c] = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) {
-        const double* p = part + ((size_t)li * gridDim.x + b) * 4;
-#pragma unroll
-        for (int c = 0; c < NV; ++c) v[c] += __ldcg(&p[c]);
-    }
+    lane_partial_sum<NV>(part + (size_t)li * gridDim.x * 4, (int)gridDim.x, v);
 #pragma unroll
     for (int c = 0; c < NV; ++c)
         for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);

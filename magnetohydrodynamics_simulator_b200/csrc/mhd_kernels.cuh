@@ -205,6 +205,31 @@ __device__ __forceinline__ bool grid_barrier(CgSync* sync, unsigned long long& t
     return *sflag != 0;
 }
 
+// This lane's sum of K consecutive doubles of the 4-double partials of blocks lane, lane + 32, ...
+// (< nblocks), in that order. The loads of four blocks are issued before they are added, so a lane
+// waits for one round trip per four blocks instead of one per block; the sum is the same.
+template <int K>
+__device__ __forceinline__ void lane_partial_sum(const double* base, int nblocks, double (&v)[K]) {
+    const int l = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    for (int b0 = l; b0 < nblocks; b0 += 128) {
+        double t[4][K];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int b = b0 + 32 * u;
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[u][k] = (b < nblocks) ? __ldcg(&base[(size_t)b * 4 + k]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (b0 + 32 * u < nblocks) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) v[k] += t[u][k];
+            }
+    }
+}
+
 // Sum the K partial slots of every block in a fixed order (all blocks get identical sums).
 template <int K>
 __device__ __forceinline__ void reduce_partials(const double* part, int nblocks, double* out,
@@ -212,12 +237,7 @@ __device__ __forceinline__ void reduce_partials(const double* part, int nblocks,
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
         double v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) v[k] = 0.0;
-        for (int b = l; b < nblocks; b += 32) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) v[k] += __ldcg(&part[(size_t)b * 4 + k]);
-        }
+        lane_partial_sum<K>(part, nblocks, v);
 #pragma unroll
         for (int k = 0; k < K; ++k)
             for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
