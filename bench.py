@@ -318,6 +318,7 @@ def run_gpu_arm(args):
 
     # ---- timed region: K steps, device-resident inputs, CFL dt on the device
     ctx.lib.mhd_set_kernel_timing(ctx.h, 1)
+    sum0 = ctx.cg_products_sum()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     with ClockSampler(local) as clocks:
@@ -329,6 +330,8 @@ def run_gpu_arm(args):
     barrier()
     status = ctx.synchronize_status()
     ms = start.elapsed_time(stop)
+    sum1 = ctx.cg_products_sum()
+    divb_after = ctx.divb()  # |div B| of the state the timed steps left (outside the timing)
     import ctypes
 
     kt = (ctypes.c_double * 5)()
@@ -361,8 +364,9 @@ def run_gpu_arm(args):
     peak, peak_kind = load_peaks()
     ksum = dict(zip(KERNELS, list(kt)))
     steps_rec = max(1, ksteps.value)
-    k1, k2 = prods  # CG products of the last step (reported)
-    # average products over the timed steps are not recorded per step by mhd_step; use the last
+    # mean products of each solve over the timed steps (device-side running sums read around it)
+    k1 = (sum1[0] - sum0[0]) / args.steps
+    k2 = (sum1[1] - sum0[1]) / args.steps
     per_kernel = {}
     for name in KERNELS:
         avg_ms = ksum[name] / steps_rec
@@ -375,7 +379,16 @@ def run_gpu_arm(args):
         gbs = alg * zones / (avg_ms * 1e-3) / 1e9
         per_kernel[name] = {"ms": avg_ms, "alg_bytes_per_zone": alg, "achieved_gbs": gbs,
                             "frac": gbs / peak}
-    dominant = max(KERNELS, key=lambda k: per_kernel[k]["ms"])
+    # the solver kernel (k_cg_sweep) runs twice per step: its share of the step is both launches
+    solver_ms = per_kernel["cg1"]["ms"] + per_kernel["cg2"]["ms"]
+    solver_gbs = ALG_BYTES["cg_per_iter"] * (k1 + k2) * zones / (solver_ms * 1e-3) / 1e9
+    step_kernels_ms = sum(per_kernel[k]["ms"] for k in KERNELS)
+    shares = {"k_stage_sweep<1>": per_kernel["stage1"]["ms"] / step_kernels_ms,
+              "k_cg_sweep": solver_ms / step_kernels_ms,
+              "k_stage_sweep<2>": per_kernel["stage2"]["ms"] / step_kernels_ms,
+              "k_finalize_sweep": per_kernel["finalize"]["ms"] / step_kernels_ms}
+    longest = max(KERNELS, key=lambda k: per_kernel[k]["ms"])
+    dominant = longest
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "dram_bytes_per_zone.json")
     if os.path.exists(tr_path):
@@ -396,20 +409,24 @@ def run_gpu_arm(args):
         "achieved": per_kernel[dominant]["achieved_gbs"], "peak": peak, "unit": "GB/s",
         "frac": per_kernel[dominant]["achieved_gbs"] / peak,
         "traffic": traffic, "peak_source": peak_kind,
+        "kernel_is": "the longest single launch of the step",
+        "largest_share": {"kernel": "k_cg_sweep", "launches_per_step": 2,
+                          "share_of_step": shares["k_cg_sweep"], "ms_per_step": solver_ms,
+                          "alg_bytes_per_zone": ALG_BYTES["cg_per_iter"] * (k1 + k2),
+                          "achieved": solver_gbs, "frac": solver_gbs / peak},
+        "shares": shares,
         "step": {"alg_bytes_per_zone": 384.0 + 48.0 * (k1 + k2),
                  "achieved": step_alg / (step_ms * 1e-3) / 1e9,
                  "frac": step_alg / (step_ms * 1e-3) / 1e9 / peak},
         "kernels": per_kernel,
     }
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference_step_rate(n, 1)
-        if r is not None:
-            cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": f"1 step of the reference driver loop (CFL dt, matrix build, IMEX) "
-                             f"on the same {n}x{n} Orszag-Tang state; reference headers compiled "
-                             f"-O3 -ffast-math, single thread, {r[1]:.1f} s"}
+        cpu, parity = headline_parity(ctx, state, n, dx)
+    if parity is not None:
+        parity["divb_after_timed_steps"] = {"steps": args.warmup + args.steps, "rms": divb_after[0],
+                                            "max": divb_after[1]}
     clk = clocks.summary()
     batched = None
     if not args.no_batch:
@@ -427,11 +444,13 @@ def run_gpu_arm(args):
         "config": {"workload": WORKLOAD if n == N_GRID else f"orszag_tang_{n}x{n}_eta1e-4_cfl0.4",
                    "grid": [n, n], "eta": ETA, "cfl": COURANT,
                    "parallelism": f"replicas{world}", "l2": "inputs exceed L2 (805 MB state)",
-                   "cg_products_last_step": [k1, k2]},
+                   "cg_products_last_step": list(prods),
+                   "cg_products_mean_per_step": [k1, k2]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
                 "d2h_bytes_per_step": int(6 * zones * 8), "steps": e2e_steps},
         "roofline": roofline,
         "cpu_baseline": cpu,
+        "parity": parity,
         "clocks": clk,
         "gpu_launches": args.steps * ctx.launches_per_step,
         "status": [status, status2],
@@ -446,6 +465,47 @@ def run_gpu_arm(args):
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def headline_parity(ctx, state, n, dx):
+    """One step of the headline problem from its initial state, on the GPU (the context, dt = its
+    CFL step) and in the reference's own code (oracle/_ref, the reference driver loop given the
+    same dt: CFL evaluation, matrix build, IMEX), compared field by field. The reference step is
+    timed too: it is the CPU baseline (1 host core; the reference is single-threaded). Returns
+    (cpu_baseline, parity)."""
+    from oracle.oracle import Reference, reference_available, rel_linf
+
+    if not reference_available():
+        return None, None
+    ctx.set_state(state)
+    dt = ctx.cfl_dt()
+    ctx.step(dt)
+    st = ctx.synchronize_status()
+    got = ctx.get_state()
+    g_rms, g_max = ctx.divb()
+    prods = ctx.last_cg_products()
+    ref = Reference(n, n, dx, dx, ETA)
+    ref.set_state(state)
+    t0 = time.perf_counter()
+    ref.cfl_dt()
+    _, rprods = ref.run(1, dts=np.array([dt]))
+    sec = time.perf_counter() - t0
+    want = ref.get_state()
+    r_rms, r_max = ref.divb()
+    names = ("rho", "mx", "my", "E", "bxf", "byf")
+    errs = {k: rel_linf(g, w) for k, g, w in zip(names, got, want)}
+    del ref
+    cpu = {"value": n * n / sec, "unit": UNIT, "cores": 1, "kind": "reference",
+           "sample": f"1 step of the reference driver loop (CFL evaluation, matrix build, IMEX) on "
+                     f"the {n}x{n} Orszag-Tang initial state with the GPU's dt; reference headers "
+                     f"compiled -O3 -ffast-math, single thread, {sec:.1f} s"}
+    parity = {"what": f"one step from the {n}x{n} Orszag-Tang initial state, dt = {dt!r} (the GPU's "
+                      f"CFL 0.4 step), GPU against the reference's own IMEX (oracle/_ref)",
+              "rel_linf_per_field": errs, "max_rel_linf": max(errs.values()), "bar": 1e-10,
+              "divb_max": {"gpu": g_max, "reference": r_max}, "divb_rms": {"gpu": g_rms, "reference": r_rms},
+              "cg_products": {"gpu": list(prods), "reference": [int(x) for x in rprods[0]]},
+              "status": st}
+    return cpu, parity
 
 
 BATCH_WORKLOAD = "mixed64_sizes256-1024_seed2024_eta1e-4..1e-2_cfl0.5"

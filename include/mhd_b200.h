@@ -128,8 +128,11 @@ mhd_status mhd_resistive_rate(mhd_context* ctx, int solve_implicitly, double alp
  * address (cudaGetSymbolAddress) and sets up the solver kernel; make that first call before any
  * stream capture. All calls share the one array: calls that overlap on the GPU (other streams,
  * other threads) race on it, so serialise them. stream: a cudaStream_t (NULL = legacy default).
- * cg_products (host, may be NULL) receives the matrix-vector products; the call waits for the
- * result and returns the solve's device status. */
+ * With solve_implicitly != 0 the call always waits for the solve and returns its device status
+ * (MHD_ERR_NONFINITE, MHD_ERR_CG_NOT_CONVERGED, MHD_ERR_TIMEOUT or MHD_OK), whether or not
+ * cg_products (host, may be NULL) is given to receive the matrix-vector products; the solver runs
+ * with the same geometry as a context's, so its result equals mhd_resistive_rate's bit for bit.
+ * With solve_implicitly == 0 (no solve) the call only enqueues the rate kernel and returns. */
 #define MHD_NOALLOC_MAX_CELLS 65536
 mhd_status mhd_resistive_rate_noalloc(const mhd_params* p, int solve_implicitly, double alpha,
                                       const double* bxf, const double* byf, double* bx_rate,
@@ -147,6 +150,10 @@ mhd_status mhd_synchronize(mhd_context* ctx);
 
 /* Matrix-vector products of the last step's two implicit solves (after mhd_synchronize). */
 mhd_status mhd_last_cg_products(mhd_context* ctx, long long out[2]);
+/* Matrix-vector products of the first (out[0]) and second (out[1]) implicit solve of every step
+ * since the context was created, summed (for per-step averages over a timed run; no counterpart
+ * in the reference). Synchronises. */
+mhd_status mhd_cg_products_sum(mhd_context* ctx, long long out[2]);
 
 /* Device planes of the current state (dense nx*ny, valid until the next step). */
 mhd_status mhd_state_device_pointers(mhd_context* ctx, double* out[6]);
@@ -265,6 +272,16 @@ typedef struct mhd_adjoint mhd_adjoint;
  * dt > 0 the fixed step; nsteps >= 1; checkpoint_every >= 1. */
 mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkpoint_every,
                           void* stream, mhd_adjoint** out);
+/* Memory mode of mhd_adj_create_ex. By default the forward pass keeps the two implicit solutions
+ * of every step (2 * nsteps planes) and the backward pass recomputes only each segment's explicit
+ * stages. MHD_ADJ_RECOMPUTE_SOLVES keeps the solutions of one segment (2 * checkpoint_every planes)
+ * and re-solves each segment in the backward pass: device memory of O(nsteps / checkpoint_every +
+ * checkpoint_every) planes for two more solves per step; the gradients are bit-identical. */
+#define MHD_ADJ_RECOMPUTE_SOLVES 1
+mhd_status mhd_adj_create_ex(const mhd_params* p, double dt, int nsteps, int checkpoint_every,
+                             int flags, void* stream, mhd_adjoint** out);
+/* Device memory the adjoint object holds for its planes, in bytes. */
+size_t mhd_adj_device_bytes(mhd_adjoint* a);
 mhd_status mhd_adj_destroy(mhd_adjoint* a);
 /* Resistivity of the following passes (the matrix coefficient follows: alpha = dt*eta*g). */
 mhd_status mhd_adj_set_eta(mhd_adjoint* a, double eta);

@@ -19,6 +19,15 @@ from .capi import Adjoint
 GAMMA = 5.0 / 3.0
 
 
+def _after_current_stream(adj: Adjoint, device: torch.device) -> None:
+    """Order the library's stream after the work torch has queued on its current stream (that
+    produced the inputs): an event, not a device-wide synchronisation. The library's calls return
+    only when their own stream is done, so torch's later work needs no further ordering."""
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(device))
+    torch.cuda.ExternalStream(adj.stream, device=device).wait_event(ev)
+
+
 def _ptrs(t: torch.Tensor):
     if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.dim() != 3 or t.shape[0] != 6:
         raise ValueError("states must be contiguous float64 CUDA tensors of shape (6, ny, nx)")
@@ -31,7 +40,7 @@ class _Trajectory(torch.autograd.Function):
         u0c = u0.detach().contiguous()
         adj.set_eta(float(eta))
         uT = torch.empty_like(u0c)
-        torch.cuda.synchronize(u0c.device)  # the library runs on its own stream
+        _after_current_stream(adj, u0c.device)  # the library runs on its own stream
         adj.forward(_ptrs(u0c), _ptrs(uT))
         adj._generation = getattr(adj, "_generation", 0) + 1
         ctx.adj = adj
@@ -47,7 +56,7 @@ class _Trajectory(torch.autograd.Function):
                                "use one Adjoint per trajectory in flight")
         g = grad_uT.detach().contiguous()
         gu0 = torch.empty_like(g)
-        torch.cuda.synchronize(g.device)
+        _after_current_stream(adj, g.device)
         geta = adj.backward(_ptrs(g), _ptrs(gu0))
         return gu0, torch.tensor(geta, dtype=torch.float64, device=g.device).reshape(ctx.eta_shape), None
 

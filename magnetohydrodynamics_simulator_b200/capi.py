@@ -109,6 +109,7 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_snapshot_pack.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp]
     lib.mhd_synchronize.argtypes = [vp]
     lib.mhd_last_cg_products.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.mhd_cg_products_sum.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.mhd_state_device_pointers.argtypes = [vp, P6]
     lib.mhd_stream.argtypes = [vp]
     lib.mhd_stream.restype = vp
@@ -143,6 +144,10 @@ def load_library() -> ctypes.CDLL:
                                                vp, vp, vp, vp, llp, vp]
     lib.mhd_adj_create.argtypes = [ctypes.POINTER(Params), ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                    vp, ctypes.POINTER(vp)]
+    lib.mhd_adj_create_ex.argtypes = [ctypes.POINTER(Params), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, vp, ctypes.POINTER(vp)]
+    lib.mhd_adj_device_bytes.argtypes = [vp]
+    lib.mhd_adj_device_bytes.restype = ctypes.c_size_t
     lib.mhd_adj_destroy.argtypes = [vp]
     lib.mhd_adj_set_eta.argtypes = [vp, ctypes.c_double]
     lib.mhd_adj_forward.argtypes = [vp, P6, P6]
@@ -280,6 +285,12 @@ class Context:
     def last_cg_products(self):
         out = (ctypes.c_longlong * 2)()
         _check(self.lib.mhd_last_cg_products(self.h, out), "mhd_last_cg_products")
+        return int(out[0]), int(out[1])
+
+    def cg_products_sum(self):
+        """Products of the first and of the second solve of every step so far, summed."""
+        out = (ctypes.c_longlong * 2)()
+        _check(self.lib.mhd_cg_products_sum(self.h, out), "mhd_cg_products_sum")
         return int(out[0]), int(out[1])
 
     def resistive_rate(self, bxf: int, byf: int, bx_rate: int, by_rate: int, *,
@@ -478,12 +489,14 @@ class Batch:
 class Adjoint:
     """Differentiable fixed-dt trajectory of `nsteps` IMEX steps of one grid (the mhd_adj_* ABI):
     forward keeps every `checkpoint_every`-th state, backward recomputes each segment and runs the
-    hand-written adjoint steps. State arguments are lists of six device addresses (dense planes
+    hand-written adjoint steps. recompute_solves: keep one segment's implicit solutions instead of
+    every step's and re-solve in the backward pass (memory O(nsteps/k + k) planes). State arguments are lists of six device addresses (dense planes
     rho, mx, my, E, bxf, byf). Calls are synchronous on the object's own stream."""
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, eta: float, dt: float, nsteps: int,
                  checkpoint_every: int = 10, *, ct_mode: int = 0, cg_tol: float = 0.0,
-                 cg_max_iters: int = 0, cg_timeout_s: float = 30.0, stream: int | None = None):
+                 cg_max_iters: int = 0, cg_timeout_s: float = 30.0, stream: int | None = None,
+                 recompute_solves: bool = False):
         self.lib = load_library()
         self.nx, self.ny, self.dt, self.nsteps = int(nx), int(ny), float(dt), int(nsteps)
         self.checkpoint_every = int(checkpoint_every)
@@ -496,10 +509,16 @@ class Adjoint:
         self.params = p
         self.eta = float(eta)
         h = ctypes.c_void_p()
-        _check(self.lib.mhd_adj_create(ctypes.byref(p), dt, nsteps, checkpoint_every,
-                                       ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)),
-               "mhd_adj_create")
+        _check(self.lib.mhd_adj_create_ex(ctypes.byref(p), dt, nsteps, checkpoint_every,
+                                          1 if recompute_solves else 0,
+                                          ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)),
+               "mhd_adj_create_ex")
         self.h = h
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory of the object's planes (checkpoints, segment slots, solutions, scratch)."""
+        return int(self.lib.mhd_adj_device_bytes(self.h))
 
     def close(self):
         if getattr(self, "h", None):

@@ -8,7 +8,10 @@
 // for the whole trajectory (2 planes per step). A forward pass alternates two slots and copies every
 // checkpoint_every-th state out; the backward pass recomputes the explicit stages of a segment of
 // steps into one slot per step (the stored solutions stand in for the solves) and then runs the
-// adjoint steps backwards over it.
+// adjoint steps backwards over it. With MHD_ADJ_RECOMPUTE_SOLVES the solutions are kept for one
+// segment only (2 * checkpoint_every planes): the backward pass recomputes each segment's steps
+// with their solves (bit-identical: the solver is deterministic), so device memory grows with
+// nsteps / checkpoint_every + checkpoint_every planes instead of 2 * nsteps.
 //
 // Adjoint of one step (U^{n+1} = Phi(U^n); notation of mhd_adjoint.cuh, cg = dt*g, cd = dt*d,
 // c1md = dt*(1-d), c1mg = dt*(1-g), S the implicit rate, R the explicit resistive rate):
@@ -77,6 +80,7 @@ struct mhd_adjoint {
     size_t n = 0;
     double dt = 0.0, eta = 0.0;
     int nsteps = 0, every = 1, nseg = 0, nslots = 0;
+    bool recompute_solves = false;  // keep one segment's solutions, re-solve in the backward pass
     double g = 0.0, d = 0.0;
     double* pool = nullptr;
     std::vector<double*> ckpt;  // nseg * 6 planes
@@ -333,13 +337,26 @@ mhd_status read_status(mhd_adjoint* a) {
     return MHD_OK;
 }
 
+// The solution planes of step `step` (x1, x2): the trajectory's own, or the segment's when the
+// solves are recomputed.
+double* xs_of(mhd_adjoint* a, int step, int which) {
+    const size_t k = a->recompute_solves ? (size_t)(step % a->every) : (size_t)step;
+    return a->xs[2 * k + which];
+}
+
 }  // namespace
 
 extern "C" {
 
 mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkpoint_every,
                           void* stream, mhd_adjoint** out) {
-    if (!p || !out || !(dt > 0) || !std::isfinite(dt) || nsteps < 1 || checkpoint_every < 1)
+    return mhd_adj_create_ex(p, dt, nsteps, checkpoint_every, 0, stream, out);
+}
+
+mhd_status mhd_adj_create_ex(const mhd_params* p, double dt, int nsteps, int checkpoint_every,
+                             int flags, void* stream, mhd_adjoint** out) {
+    if (!p || !out || !(dt > 0) || !std::isfinite(dt) || nsteps < 1 || checkpoint_every < 1 ||
+        (flags & ~MHD_ADJ_RECOMPUTE_SOLVES) != 0)
         return MHD_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     if (p->nx < 2 || p->ny < 2 || !(p->dx > 0) || !(p->dy > 0) || !(p->eta >= 0) ||
@@ -365,6 +382,7 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
     a->eta = p->eta;
     a->nsteps = nsteps;
     a->every = std::min(checkpoint_every, nsteps);
+    a->recompute_solves = (flags & MHD_ADJ_RECOMPUTE_SOLVES) != 0;
     a->nseg = (nsteps + a->every - 1) / a->every;
     a->nslots = std::max(2, a->every);
     a->g = (2.0 - sqrt(2.0)) / 2.0;     // solvers.hpp:41
@@ -430,8 +448,9 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
     a->ew_blocks = std::max(1, std::min((int)((a->n + 255) / 256), a->num_sms * 8));
     a->dot_blocks = std::max(1, std::min((int)((a->n + 255) / 256), a->num_sms * 2));
     // memory: checkpoints, slots, scratch
-    const size_t planes = (size_t)a->nseg * 6 + (size_t)a->nslots * kSlotPlanes +
-                          2 * (size_t)a->nsteps + kScratchPlanes;
+    const size_t xplanes = 2 * (size_t)(a->recompute_solves ? a->every : a->nsteps);
+    const size_t planes = (size_t)a->nseg * 6 + (size_t)a->nslots * kSlotPlanes + xplanes +
+                          kScratchPlanes;
     if (cudaMalloc(&a->pool, planes * a->n * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&a->coeffs, sizeof(StepCoeffs)) != cudaSuccess ||
         cudaMalloc(&a->status, sizeof(DeviceStatus)) != cudaSuccess ||
@@ -458,7 +477,7 @@ mhd_status mhd_adj_create(const mhd_params* p, double dt, int nsteps, int checkp
         sl.Bn[0] = take();
         sl.Bn[1] = take();
     }
-    a->xs.resize(2 * (size_t)a->nsteps);
+    a->xs.resize(xplanes);
     for (auto& x : a->xs) x = take();
     AdjScratch& s = a->s;
     for (int k = 0; k < 6; ++k) s.lam[k] = take();
@@ -530,7 +549,7 @@ mhd_status mhd_adj_forward(mhd_adjoint* a, const double* const u0[6], double* co
             for (int k = 0; k < 6; ++k) U[k] = ck[k];
         }
         const Slot& sl = a->slots[step % 2];
-        if ((s = forward_step(a, U, sl, a->xs[2 * step], a->xs[2 * step + 1], true)) != MHD_OK) return s;
+        if ((s = forward_step(a, U, sl, xs_of(a, step, 0), xs_of(a, step, 1), true)) != MHD_OK) return s;
         next_state(sl, U);
     }
     if ((s = copy_planes(a, uT, U)) != MHD_OK) return s;
@@ -551,12 +570,14 @@ mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6], doub
     for (int seg = a->nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * a->every, s1 = std::min(a->nsteps, s0 + a->every);
         const double* const* ck = &a->ckpt[(size_t)seg * 6];
-        // recompute the explicit stages of the segment, keeping every step's intermediates
+        // recompute the explicit stages of the segment (and, with recompute_solves, its solves),
+        // keeping every step's intermediates
         const double* U[6];
         for (int k = 0; k < 6; ++k) U[k] = ck[k];
         for (int step = s0; step < s1; ++step) {
             const Slot& sl = a->slots[step - s0];
-            if ((s = forward_step(a, U, sl, a->xs[2 * step], a->xs[2 * step + 1], false)) != MHD_OK)
+            if ((s = forward_step(a, U, sl, xs_of(a, step, 0), xs_of(a, step, 1), a->recompute_solves)) !=
+                MHD_OK)
                 return s;
             next_state(sl, U);
         }
@@ -567,7 +588,7 @@ mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6], doub
             } else {
                 next_state(a->slots[step - s0 - 1], Us);
             }
-            if ((s = adjoint_step(a, Us, a->slots[step - s0], a->xs[2 * step], a->xs[2 * step + 1])) !=
+            if ((s = adjoint_step(a, Us, a->slots[step - s0], xs_of(a, step, 0), xs_of(a, step, 1))) !=
                 MHD_OK)
                 return s;
         }
@@ -614,6 +635,14 @@ mhd_status mhd_adj_rate_vjp(mhd_adjoint* a, const double* const u[6], const doub
 
 void* mhd_adj_stream(mhd_adjoint* a) { return a ? (void*)a->stream : nullptr; }
 
+size_t mhd_adj_device_bytes(mhd_adjoint* a) {
+    if (!a) return 0;
+    const size_t xplanes = 2 * (size_t)(a->recompute_solves ? a->every : a->nsteps);
+    const size_t planes = (size_t)a->nseg * 6 + (size_t)a->nslots * kSlotPlanes + xplanes +
+                          kScratchPlanes;
+    return planes * a->n * sizeof(double);
+}
+
 mhd_status mhd_adj_launch_counts(mhd_adjoint* a, int* forward_step, int* adjoint_step) {
     if (!a) return MHD_ERR_INVALID_ARGUMENT;
     // forward: stage 1, solve, stage 2, solve, finalize
@@ -621,7 +650,7 @@ mhd_status mhd_adj_launch_counts(mhd_adjoint* a, int* forward_step, int* adjoint
     // adjoint: 4 corner currents, 4 dot products (2 launches each), 5 curls, 2 solves,
     // 2 explicit-rate VJPs (4 kernels + primitives each), 2 plane combinations; plus the
     // recomputation of the step's explicit stages (stage 1, stage 2, finalize)
-    if (adjoint_step) *adjoint_step = 4 + 8 + 5 + 2 + 10 + 2 + 3;
+    if (adjoint_step) *adjoint_step = 4 + 8 + 5 + 2 + 10 + 2 + 3 + (a->recompute_solves ? 2 : 0);
     return MHD_OK;
 }
 

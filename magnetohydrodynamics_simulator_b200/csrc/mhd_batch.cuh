@@ -528,7 +528,7 @@ k_cg_batch(CgBatchArgs a) {
             const BatchInst& I = a.insts[a.inst0 + li];
             const CgBInst& S = sh[li];
             I.st->cg_products[a.solve_index] = S.products;
-            I.st->cg_products_total += S.products;
+            I.st->cg_products_sum[a.solve_index] += S.products;
             I.st->cg_last_rr[a.solve_index] = (S.bb > 0.0) ? S.rr / S.bb : 0.0;
             if (a.prods_rec)
                 a.prods_rec[((size_t)(a.inst0 + li) * a.rec_stride + I.C->cur) * 2 + a.solve_index] =

@@ -844,6 +844,20 @@ mhd_status mhd_last_cg_products(mhd_context* c, long long out[2]) {
     return MHD_OK;
 }
 
+mhd_status mhd_cg_products_sum(mhd_context* c, long long out[2]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!out) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
+                            c->stream));
+    MHD_TRY(cudaStreamSynchronize(c->stream));
+    DeviceStatus st;
+    memcpy(&st, c->host_pinned, sizeof(st));
+    out[0] = st.cg_products_sum[0];
+    out[1] = st.cg_products_sum[1];
+    return MHD_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
@@ -892,7 +906,8 @@ mhd_status noalloc_setup(int dev, NoAllocDevice** out) {
         MHD_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if (occ < 1) return MHD_ERR_CUDA;
         d.scratch = static_cast<double*>(addr);
-        d.grid = std::max(1, std::min(occ * sms, kNoAllocMaxBlocks));
+        // one block per SM, as a context launches the solver
+        d.grid = std::max(1, std::min(sms, kNoAllocMaxBlocks));
         d.ready = true;
     }
     *out = &d;
@@ -948,9 +963,13 @@ extern "C" mhd_status mhd_resistive_rate_noalloc(const mhd_params* p, int solve_
     MHD_TRY(cudaMemsetAsync(ctrl, 0, 8 * kNoAllocControlDoubles, stream));
     k_set_alpha<<<1, 1, 0, stream>>>(coeffs, alpha);
     MHD_TRY(cudaGetLastError());
-    // solver geometry as for a context (strips of CG_W columns, one wave of warps)
-    const int grid = std::max(1, std::min(nd->grid, (int)std::max<size_t>(1, (n + 63) / 64)));
+    // solver geometry exactly as a context's (mhd_create): strips of CG_W columns, no more blocks
+    // than rows of work for their warps, so both entry points reduce in the same order
     const int strips_x = (p->nx + CG_W - 1) / CG_W;
+    const long long rows_total = (long long)strips_x * p->ny;
+    const long long max_blocks =
+        std::max(1LL, (rows_total + (CGS_NT / 32) * 4 - 1) / ((CGS_NT / 32) * 4));
+    const int grid = (int)std::max(1LL, std::min((long long)nd->grid, max_blocks));
     const long long warps = (long long)grid * (CGS_NT / 32);
     const int segs = (int)std::max(1LL, warps / strips_x);
     const int seg_h = std::max(4, (p->ny + segs - 1) / segs);
@@ -988,12 +1007,11 @@ extern "C" mhd_status mhd_resistive_rate_noalloc(const mhd_params* p, int solve_
     MHD_TRY(cudaLaunchKernelEx(&cfg, k_cg_sweep, a));
     k_corner_rates<<<blocks, 256, 0, stream>>>(D, x, nullptr, nullptr, bx_rate, by_rate);
     MHD_TRY(cudaGetLastError());
-    if (cg_products) {
-        DeviceStatus hs;
-        MHD_TRY(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, stream));
-        MHD_TRY(cudaStreamSynchronize(stream));
-        *cg_products = hs.cg_products[0];
-        return status_from_flags(hs.flags);
-    }
-    return MHD_OK;
+    // The solve's status lives only in the shared array, where the next call clears it, so it is
+    // read back here on every call: the implicit path always waits for its result.
+    DeviceStatus hs;
+    MHD_TRY(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+    MHD_TRY(cudaStreamSynchronize(stream));
+    if (cg_products) *cg_products = hs.cg_products[0];
+    return status_from_flags(hs.flags);
 }

@@ -427,7 +427,7 @@ k_cg_sweep(CgSweepArgs a) {
     }
     if (blockIdx.x == 0 && tid == 0) {
         a.st->cg_products[a.solve_index] = products;
-        a.st->cg_products_total += products;
+        a.st->cg_products_sum[a.solve_index] += products;
         a.st->cg_last_rr[a.solve_index] = (bb > 0.0) ? rr_final / bb : 0.0;
         if (a.prods_out) a.prods_out[2 * a.C->cur + a.solve_index] = products;
         if (breakdown) atomicOr(&a.st->flags, (unsigned)(kStatusCgBreakdown | kStatusNonFinite));

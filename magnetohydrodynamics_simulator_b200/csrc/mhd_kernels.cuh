@@ -73,7 +73,7 @@ struct DeviceStatus {
     unsigned int pad;
     unsigned long long smax_bits;  // max CFL signal speed of the current state (as double bits)
     long long cg_products[2];      // matrix-vector products of the last step's two solves
-    long long cg_products_total;
+    long long cg_products_sum[2];  // products of each of the step's two solves, summed over steps
     double cg_last_rr[2];          // final recursive |r|^2 / |b|^2 of each solve
 };
 

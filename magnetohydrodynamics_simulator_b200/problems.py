@@ -168,8 +168,8 @@ def _smooth_periodic(rng, nx, ny, width_cells):
 
 def random_instance(n: int, seed: int, v_modes: int = 8, az_modes: int = 8, rho_floor: float = 0.2):
     """One member of the mixed-size batch: rho = 1 + 0.2 * smoothed N(0,1) (clamped at rho_floor),
-    p = 1, v and Az sums of Fourier modes with |k| <= 4 and per-mode amplitudes in [0.1, 1]; each
-    sum is scaled by 1/sqrt(modes) so the field's RMS is that of a single mode."""
+    p = 1, v and Az sums of Fourier modes with |k| <= 4 and per-mode amplitudes in [0.1, 1] (the
+    sums are not normalised: |v| reaches ~4-5 and |B| ~5-7, supersonic and low-beta)."""
     rng = np.random.default_rng(seed)
     dx = grid_spacing(n)
     L = n * dx
@@ -178,9 +178,9 @@ def random_instance(n: int, seed: int, v_modes: int = 8, az_modes: int = 8, rho_
     xc = np.arange(n + 1) * dx
     XC, YC = np.meshgrid(xc, xc)
     rho = np.maximum(1.0 + 0.2 * _smooth_periodic(rng, n, n, width_cells=n / 32), rho_floor)
-    vx = _fourier_modes(rng, X, Y, L, L, v_modes, 0.1, 1.0) / np.sqrt(v_modes)
-    vy = _fourier_modes(rng, X, Y, L, L, v_modes, 0.1, 1.0) / np.sqrt(v_modes)
-    az = _fourier_modes(rng, XC, YC, L, L, az_modes, 0.1, 1.0) / np.sqrt(az_modes)
+    vx = _fourier_modes(rng, X, Y, L, L, v_modes, 0.1, 1.0)
+    vy = _fourier_modes(rng, X, Y, L, L, v_modes, 0.1, 1.0)
+    az = _fourier_modes(rng, XC, YC, L, L, az_modes, 0.1, 1.0)
     bxf = (az[1:, :-1] - az[:-1, :-1]) / dx
     byf = -(az[:-1, 1:] - az[:-1, :-1]) / dx
     bxc = 0.5 * (bxf + np.roll(bxf, -1, axis=1))

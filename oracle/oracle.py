@@ -22,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmhdref.so")
-REF_SRC = "/root/reference"
+REF_SRC = os.environ.get("MHD_REFERENCE_DIR", "/root/reference")  # the reference sources (build only)
 
 FIELDS = ("rho", "mx", "my", "E", "bxf", "byf")
 PI_REF = 3.14159265359  # the reference driver's pi literal (src/integrator_main.cpp:36)

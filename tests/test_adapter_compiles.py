@@ -44,3 +44,25 @@ def test_adapter_instantiates(tmp_path):
            "-I", cuda_inc, str(src)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_reference_driver_compiles_against_adapter():
+    """The reference's own src/integrator_main.cpp with the integration guide's diff applied
+    (oracle/dropin.py), against the reference's real include/*.hpp (Grid.hpp:6-62 included) and
+    the Eigen subset: it compiles. Needs the reference sources ($MHD_REFERENCE_DIR, else
+    /root/reference); skipped where they are absent."""
+    ref = os.environ.get("MHD_REFERENCE_DIR", "/root/reference")
+    if not os.path.exists(os.path.join(ref, "src", "integrator_main.cpp")):
+        pytest.skip("reference sources absent")
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    import sys
+
+    src = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "dropin.py"), ref, "b200"],
+                         capture_output=True, text=True, check=True).stdout
+    assert "mhd_b200::IMEX(global_state," in src and "matrix_solver.compute" not in src
+    cmd = [cxx, "-std=c++17", "-fsyntax-only", "-w", "-I", os.path.join(ROOT, "oracle", "eigen_subset"),
+           "-I", os.path.join(ref, "include"), "-I", os.path.join(ROOT, "include"), "-x", "c++", "-"]
+    r = subprocess.run(cmd, input=src, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]

@@ -185,3 +185,85 @@ def test_gradients_match_central_differences(m):
         fd_dir = float((((rp - rm) / (2 * s)) * w).sum())
     assert abs(g_eta - fd_eta) <= 1e-6 * abs(fd_eta), (g_eta, fd_eta)
     assert abs(g_dir - fd_dir) <= 5e-6 * abs(fd_dir), (g_dir, fd_dir)
+
+
+def _configured_setup(m, recompute_solves=False):
+    """The configured differentiable workload: 1024^2, 4 random Fourier modes (velocity amplitude
+    0.05, Az amplitude 0.1, rho = p = 1), eta = 5e-3, 100 fixed steps of 1e-3, checkpoint every 10;
+    loss 1/2 |rho(T) - rho_target|^2 with the target from the forward solver at eta = 4e-3."""
+    from magnetohydrodynamics_simulator_b200.autograd import state_from_potential, trajectory
+
+    n, nsteps, every, dt, eta = 1024, 100, 10, 1e-3, 5e-3
+    dx = 2 * np.pi / n
+    rng = np.random.default_rng(5)
+    X, Y = np.meshgrid(np.arange(n) * dx, np.arange(n) * dx)
+
+    def modes(amp, shift):
+        f = np.zeros((n, n))
+        for _ in range(4):
+            kx, ky = rng.integers(-4, 5, size=2)
+            f += amp * rng.uniform(0.5, 1.0) * np.sin(kx * (X + shift) + ky * (Y + shift) + rng.uniform(0, 2 * np.pi))
+        return torch.tensor(f, device="cuda")
+
+    vx, vy = modes(0.05, dx / 2), modes(0.05, dx / 2)
+    az0, daz = modes(0.1, 0.0), modes(0.1, 0.0)
+    one = torch.ones(n, n, dtype=torch.float64, device="cuda")
+    adj = m.Adjoint(n, n, dx, dx, eta, dt, nsteps, checkpoint_every=every, recompute_solves=recompute_solves)
+
+    def u0_of(az):
+        return state_from_potential(az, one, vx, vy, one, dx, dx).contiguous()
+
+    with torch.no_grad():
+        target = trajectory(u0_of(az0), torch.tensor(0.8 * eta, dtype=torch.float64, device="cuda"), adj)[0].clone()
+    return adj, u0_of, az0, daz, eta, target
+
+
+def test_configured_loss_gradients_match_central_differences(m):
+    """The configured loss's gradient along the initial Az and in eta against central differences
+    of the GPU forward, <= 1e-6 relative. The differences are taken on the final density (two
+    trajectories, contracted with the loss's derivative afterwards), steps 3e-7 (Az) and 1e-3 eta."""
+    from magnetohydrodynamics_simulator_b200.autograd import trajectory
+
+    adj, u0_of, az0, daz, eta, target = _configured_setup(m)
+    az = az0.clone().requires_grad_(True)
+    eta_t = torch.tensor(eta, dtype=torch.float64, device="cuda", requires_grad=True)
+    uT = trajectory(u0_of(az), eta_t, adj)
+    (0.5 * ((uT[0] - target) ** 2).sum()).backward()
+    g_dir, g_eta = float((az.grad * daz).sum()), float(eta_t.grad)
+    e0 = torch.tensor(eta, dtype=torch.float64, device="cuda")
+    with torch.no_grad():
+        s = 3e-7
+        rp = trajectory(u0_of(az0 + s * daz), e0, adj)[0]
+        rm = trajectory(u0_of(az0 - s * daz), e0, adj)[0]
+        fd_dir = float((((rp - rm) / (2 * s)) * ((rp + rm) / 2 - target)).sum())
+        h = 1e-3 * eta
+        rp = trajectory(u0_of(az0), e0 + h, adj)[0]
+        rm = trajectory(u0_of(az0), e0 - h, adj)[0]
+        fd_eta = float((((rp - rm) / (2 * h)) * ((rp + rm) / 2 - target)).sum())
+    adj.close()
+    assert abs(g_dir - fd_dir) <= 1e-6 * abs(fd_dir), (g_dir, fd_dir)
+    assert abs(g_eta - fd_eta) <= 1e-6 * abs(fd_eta), (g_eta, fd_eta)
+
+
+def test_recomputed_solves_give_identical_gradients(m):
+    """MHD_ADJ_RECOMPUTE_SOLVES (one segment's solutions kept, each segment re-solved in the
+    backward pass) gives bit-identical gradients with fewer planes."""
+    nx, ny = 40, 36
+    dx, dy, U = _setup(nx, ny, 11)
+    eta, dt, nsteps, every = 2e-2, 2e-3, 9, 3
+    u_d = U.cuda().contiguous()
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    gT = torch.randn(u_d.shape, generator=gen, dtype=torch.float64, device="cuda")
+    outs = []
+    for recompute in (False, True):
+        adj = m.Adjoint(nx, ny, dx, dy, eta, dt, nsteps, checkpoint_every=every, recompute_solves=recompute)
+        uT, g0 = torch.empty_like(u_d), torch.empty_like(u_d)
+        torch.cuda.synchronize()
+        adj.forward(_ptrs(u_d), _ptrs(uT))
+        geta = adj.backward(_ptrs(gT), _ptrs(g0))
+        outs.append((uT.cpu(), g0.cpu(), geta, adj.device_bytes))
+        adj.close()
+    (uA, gA, eA, bA), (uB, gB, eB, bB) = outs
+    assert torch.equal(uA, uB) and torch.equal(gA, gB) and eA == eB
+    # 2 * nsteps solution planes against 2 * every
+    assert bA - bB == 2 * (nsteps - every) * nx * ny * 8, (bA, bB)

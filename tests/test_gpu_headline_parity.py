@@ -1,0 +1,127 @@
+"""Parity at the sizes the benchmark measures, against the reference's own code (oracle/_ref: the
+reference's include/*.hpp compiled here, driven through ref_harness.cpp).
+
+* Orszag-Tang 4096^2 (the headline problem, eta = 1e-4): one IMEX step from the initial state with
+  the GPU's CFL 0.4 dt, against the reference's IMEX given the same dt;
+* Orszag-Tang 2048^2: five steps of the device driver loop (mhd_run: CFL dt and the matrix rule on
+  the device) against the reference's driver loop (integrator_main.cpp:76-112, its own CFL dt);
+* the mixed-size batch of the batched benchmark (64 members, 256^2 to 1024^2): the whole batch
+  steps twice with per-member CFL dts, and members of each size class are compared with the
+  reference's driver loop run on their own.
+
+Tolerances: 1e-12 relative L-infinity per field (one to five steps), dts to 1e-12, CG products
+within 1, |div B|_inf <= 1e-12 on the GPU. (|div B|_inf is a rounding residue that grows by about
+eps |B| / dx per step in both codes -- ~7e-14 per step at 2048^2 -- so the two maxima are of the same
+size but not equal.)
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Reference, reference_available, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def m():
+    import torch
+
+    assert torch.cuda.is_available()
+    import magnetohydrodynamics_simulator_b200 as mod
+
+    assert mod.device_available(), "libmhd_b200.so has no kernels for this device"
+    assert reference_available(), "oracle/_ref/libmhdref.so was not built (oracle/Makefile ref)"
+    return mod
+
+
+def _errs(got, want, floor=0.0):
+    return [rel_linf(g, w, floor) for g, w in zip(got, want)]
+
+
+def test_orszag_tang_4096_one_step_matches_reference(m):
+    n, eta = 4096, 1e-4
+    dx = m.problems.grid_spacing(n)
+    ic = m.problems.orszag_tang(n, n, dx, dx)
+    ctx = m.Context(n, n, dx, dx, eta, courant=0.4)
+    ctx.set_state(ic)
+    dt = ctx.cfl_dt()
+    ctx.step(dt)
+    ctx.synchronize()
+    got = ctx.get_state()
+    g_rms, g_max = ctx.divb()
+    prods = ctx.last_cg_products()
+    ctx.close()
+    ref = Reference(n, n, dx, dx, eta)
+    ref.set_state(ic)
+    del ic
+    _, r_prods = ref.run(1, dts=np.array([dt]))
+    want = ref.get_state()
+    r_rms, r_max = ref.divb()
+    del ref
+    errs = _errs(got, want)
+    assert max(errs) <= STEP_TOL, errs
+    assert all(abs(a - b) <= 1 for a, b in zip(prods, r_prods[0])), (prods, r_prods)
+    assert g_max <= 1e-12, (g_max, r_max)
+
+
+def test_orszag_tang_2048_five_steps_driver_loop_matches_reference(m):
+    n, eta, steps = 2048, 1e-4, 5
+    dx = m.problems.grid_spacing(n)
+    ic = m.problems.orszag_tang(n, n, dx, dx)
+    ctx = m.Context(n, n, dx, dx, eta)  # CFL 0.5 and safety 0.9, as diagnostics.hpp:82-84
+    ctx.set_state(ic)
+    dts, prods = ctx.run(steps)
+    ctx.synchronize()
+    got = ctx.get_state()
+    g_max = ctx.divb()[1]
+    ctx.close()
+    ref = Reference(n, n, dx, dx, eta)
+    ref.set_state(ic)
+    r_dts, r_prods = ref.run(steps)
+    want = ref.get_state()
+    r_max = ref.divb()[1]
+    del ref
+    assert np.max(np.abs(dts - r_dts) / r_dts) <= 1e-12, (dts, r_dts)
+    assert np.max(np.abs(prods - r_prods)) <= 1, (prods, r_prods)
+    errs = _errs(got, want)
+    assert max(errs) <= STEP_TOL, errs
+    assert g_max <= 1e-12, (g_max, r_max)
+
+
+def test_mixed_batch_members_match_reference(m):
+    """The benchmarked batch itself: all 64 members step together; the first member of each
+    size class (256^2 ... 1024^2) is checked against the reference's driver loop."""
+    specs = m.problems.mixed_batch(64)
+    insts, ics = [], []
+    for n_i, eta_i, seed_i in specs:
+        f, h = m.problems.random_instance(n_i, seed_i)
+        insts.append(dict(nx=n_i, ny=n_i, dx=h, dy=h, eta=eta_i))
+        ics.append(f)
+    b = m.Batch(insts)
+    for i, f in enumerate(ics):
+        b.set_state(i, f)
+    b.autotune()
+    steps = 2
+    dts, prods = b.run(steps)
+    worst, _ = b.synchronize_status()
+    assert worst == 0
+    checked = {}
+    for i, (n_i, _, _) in enumerate(specs):
+        if n_i not in checked:
+            checked[n_i] = i
+    assert sorted(checked) == [256, 384, 512, 768, 1024]
+    for n_i, i in sorted(checked.items()):
+        s = insts[i]
+        ref = Reference(n_i, n_i, s["dx"], s["dy"], s["eta"])
+        ref.set_state(ics[i])
+        r_dts, r_prods = ref.run(steps)
+        want = ref.get_state()
+        del ref
+        assert np.max(np.abs(dts[i] - r_dts) / r_dts) <= 1e-12, (n_i, dts[i], r_dts)
+        assert np.max(np.abs(prods[i] - r_prods)) <= 1, (n_i, prods[i], r_prods)
+        errs = _errs(b.get_state(i), want, floor=1.0)
+        assert max(errs) <= STEP_TOL, (n_i, errs)
+        assert b.divb(i)[1] <= 1e-11  # |B| ~ 5-7 at dx ~ 6e-3 here: rounding level ~1e-12
+    b.close()
