@@ -304,6 +304,72 @@ mhd_status mhd_adj_launch_counts(mhd_adjoint* a, int* forward_step, int* adjoint
 /* The stream the adjoint object enqueues on (a cudaStream_t). */
 void* mhd_adj_stream(mhd_adjoint* a);
 
+/* ---------------------------------------------------------------------------------------------
+ * Domain decomposition (no counterpart in the reference, which grows one Grid on one thread:
+ * src/integrator_main.cpp:29-30). A grid is split into P x Q subdomains, one mhd_subdomain each
+ * (one per GPU; several may share a GPU). A subdomain keeps its nx x ny interior cells inside
+ * extended planes with a ring of MHD_SUB_HALO cells on every side; the explicit kernels run on the
+ * extended planes, and the caller (the decomposition driver) refreshes the rings between kernels
+ * by packing strips of each interior into buffers (mhd_sub_pack), moving them to the neighbours
+ * (device copies, or NCCL between GPUs) and unpacking them into the neighbours' rings
+ * (mhd_sub_unpack): west/east first, then south/north, whose strips span the extended width and so
+ * also fill the corners. The implicit solve is a conjugate gradient on the interior corners with
+ * one call per phase; calls that return partial sums wait for them, and the driver adds the
+ * subdomains' partials in a fixed order and takes Eigen's decisions (x0 = 0, Jacobi scaling, stop
+ * at |r|^2 < max(tol^2 |b|^2, DBL_MIN)). One step, with exchanges (set, ring width):
+ *   set_step(dt, alpha); stage(1); exchange(PREDICTOR, H); solve on T_B; exchange(SOLUTION, H);
+ *   stage(2); exchange(ACCUMULATOR_B, H); solve on A_B; exchange(SOLUTION, H); finalize();
+ *   exchange(STATE, H)
+ * where a solve is cg_rhs, then per product exchange(DIRECTION, 1), cg_matvec, cg_update and
+ * cg_direction. dt comes from the largest interior CFL speed (mhd_sub_cfl_speed) of all
+ * subdomains, by the formula of diagnostics.hpp:82-84. */
+#define MHD_SUB_HALO 4
+enum { MHD_SUB_WEST = 0, MHD_SUB_EAST = 1, MHD_SUB_SOUTH = 2, MHD_SUB_NORTH = 3 };
+enum {
+    MHD_SUB_SET_STATE = 0,          /* rho, mx, my, E, bxf, byf */
+    MHD_SUB_SET_PREDICTOR = 1,      /* U1* (6 planes) */
+    MHD_SUB_SET_ACCUMULATOR_B = 2,  /* the face fields of U2* (2 planes) */
+    MHD_SUB_SET_SOLUTION = 3,       /* the corner field of the last solve */
+    MHD_SUB_SET_DIRECTION = 4       /* the CG direction p */
+};
+typedef struct mhd_subdomain mhd_subdomain;
+int mhd_sub_halo(void);
+/* p: the interior (nx, ny >= MHD_SUB_HALO), spacing, eta, ct_mode. stream: a cudaStream_t or NULL. */
+mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out);
+mhd_status mhd_sub_destroy(mhd_subdomain* s);
+void* mhd_sub_stream(mhd_subdomain* s);
+/* Interior state from / to dense nx*ny planes (host or device pointers). Synchronous. */
+mhd_status mhd_sub_set_state(mhd_subdomain* s, const double* const fields[6]);
+mhd_status mhd_sub_get_state(mhd_subdomain* s, double* const fields[6]);
+/* Doubles of the strip that `side` exchanges for `set` with a ring of `width` (1..MHD_SUB_HALO):
+ * planes x width x ny (west/east) or planes x (nx + 2 MHD_SUB_HALO) x width (south/north). */
+size_t mhd_sub_strip_doubles(mhd_subdomain* s, int set, int side, int width);
+/* Pack the strip of the interior next to `side` into the device buffer buf; unpack a neighbour's
+ * strip into the ring beyond `side` (the strip the neighbour packed for its opposite side).
+ * Asynchronous on the subdomain's stream. */
+mhd_status mhd_sub_pack(mhd_subdomain* s, int set, int side, int width, double* buf);
+mhd_status mhd_sub_unpack(mhd_subdomain* s, int set, int side, int width, const double* buf);
+/* Largest CFL signal speed over the interior of the state (diagnostics.hpp:60-78), and whether a
+ * value is not finite. Synchronous. */
+mhd_status mhd_sub_cfl_speed(mhd_subdomain* s, double* smax, int* nonfinite);
+/* Coefficients of the next step: dt and the implicit matrix coefficient alpha. */
+mhd_status mhd_sub_set_step(mhd_subdomain* s, double dt, double alpha);
+/* Explicit stage 1 or 2 (solvers.hpp:509-517, 522-566) and the finalize (:571-611). */
+mhd_status mhd_sub_stage(mhd_subdomain* s, int stage);
+mhd_status mhd_sub_finalize(mhd_subdomain* s);
+/* CG phases on the interior corners. cg_rhs: b = eta J_z(B*) of the predictor's (solve 0) or the
+ * accumulator's (solve 1) faces, r = b, p = z = b/d, x = 0; out = partial |b|^2, r.z. cg_matvec:
+ * q = (I - alpha L) p, *pq = partial p.q. cg_update: x += alpha p, r -= alpha q, z = r/d;
+ * out = partial |r|^2, r.z. cg_direction: p = z + beta p. cg_zero_solution: x = 0. */
+mhd_status mhd_sub_cg_rhs(mhd_subdomain* s, int solve_index, double out[2]);
+mhd_status mhd_sub_cg_matvec(mhd_subdomain* s, double* pq);
+mhd_status mhd_sub_cg_update(mhd_subdomain* s, double alpha, double out[2]);
+mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta);
+mhd_status mhd_sub_cg_zero_solution(mhd_subdomain* s);
+/* Interior div B partials (diagnostics.hpp:15-42): out[0] = sum of div^2, out[1] = max |div|. */
+mhd_status mhd_sub_divb_sums(mhd_subdomain* s, double out[2]);
+mhd_status mhd_sub_synchronize(mhd_subdomain* s);
+
 const char* mhd_status_string(mhd_status s);
 
 /* 1 when a device this library was built for is present, else 0. */

@@ -1,0 +1,469 @@
+"""Domain decomposition of one periodic grid into P x Q subdomains (the mhd_sub_* C ABI).
+
+The reference grows one Grid on one thread (src/integrator_main.cpp:29-30); past one GPU's memory
+the grid is split. Each subdomain is an ``mhd_subdomain`` on some GPU: its interior plus a ring of
+``HALO`` cells. This module is the driver around them: the partition, the ring exchanges between
+kernels, and the global reductions of the implicit solve and the CFL step.
+
+* ``Partition``: subdomain sizes and offsets (the remainder of nx / P and ny / Q goes to the first
+  columns / rows of subdomains) and the periodic neighbours; subdomain index = q * P + p.
+* Transports move the rings and add the partial sums:
+  - ``LocalTransport``: every subdomain in this process (one GPU, or a CPU stand-in in the tests):
+    strips go from one subdomain's buffer into its neighbour's ring directly;
+  - ``DistTransport``: one subdomain per rank of a ``torch.distributed`` process group (NCCL for
+    GPU buffers, gloo for CPU ones): a ring exchange is two shifts per axis (each rank sends one
+    strip and receives one), and partial sums are all-gathered and added in rank order, so every
+    rank takes the same decisions.
+* ``DecomposedRun``: one ARS(2,2,2) step over the subdomains (solvers.hpp:491-613): the explicit
+  kernels on the extended planes, ring exchanges between them, and the implicit solves as a
+  conjugate gradient with Eigen's rules (x0 = 0, Jacobi scaling, stop when
+  |r|^2 < max(tol^2 |b|^2, DBL_MIN), at most 2 n products) whose dot products are sums of the
+  subdomains' partials in a fixed order. dt is the CFL step of diagnostics.hpp:82-84 from the
+  largest interior signal speed of all subdomains.
+
+A subdomain object needs: set_state, get_state, pack(set, side, width) -> buffer,
+unpack(set, side, width, buffer), synchronize, cfl_speed, set_step, stage(1|2), finalize,
+cg_rhs, cg_matvec, cg_update, cg_direction, cg_zero_solution, divb_sums. ``GpuSubdomain`` is the
+one over the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import List, Sequence
+
+import numpy as np
+
+from .capi import MHDError, Params, _check, load_library
+
+HALO = 4
+WEST, EAST, SOUTH, NORTH = 0, 1, 2, 3
+OPPOSITE = {WEST: EAST, EAST: WEST, SOUTH: NORTH, NORTH: SOUTH}
+SET_STATE, SET_PREDICTOR, SET_ACCUMULATOR_B, SET_SOLUTION, SET_DIRECTION = 0, 1, 2, 3, 4
+DBL_MIN = 2.2250738585072014e-308
+EPS = 2.220446049250313e-16
+ARS_G = (2.0 - math.sqrt(2.0)) / 2.0  # solvers.hpp:41
+
+
+class Partition:
+    """P x Q blocks of an nx x ny periodic grid."""
+
+    def __init__(self, nx: int, ny: int, P: int, Q: int):
+        if P < 1 or Q < 1 or nx // P < HALO or ny // Q < HALO:
+            raise ValueError(f"every subdomain needs at least {HALO} x {HALO} cells")
+        self.nx, self.ny, self.P, self.Q = nx, ny, P, Q
+
+        def split(n, k):
+            sizes = [n // k + (1 if i < n % k else 0) for i in range(k)]
+            offs = [sum(sizes[:i]) for i in range(k)]
+            return sizes, offs
+
+        self.xs, self.x0 = split(nx, P)
+        self.ys, self.y0 = split(ny, Q)
+
+    @property
+    def count(self) -> int:
+        return self.P * self.Q
+
+    def coords(self, idx: int):
+        return idx % self.P, idx // self.P
+
+    def shape(self, idx: int):
+        p, q = self.coords(idx)
+        return self.xs[p], self.ys[q]  # (nx, ny) of the interior
+
+    def window(self, idx: int):
+        """(row slice, column slice) of the subdomain's interior in the global arrays."""
+        p, q = self.coords(idx)
+        return slice(self.y0[q], self.y0[q] + self.ys[q]), slice(self.x0[p], self.x0[p] + self.xs[p])
+
+    def neighbour(self, idx: int, side: int) -> int:
+        p, q = self.coords(idx)
+        if side == WEST:
+            p = (p - 1) % self.P
+        elif side == EAST:
+            p = (p + 1) % self.P
+        elif side == SOUTH:
+            q = (q - 1) % self.Q
+        else:
+            q = (q + 1) % self.Q
+        return q * self.P + p
+
+
+class GpuSubdomain:
+    """One subdomain on the current CUDA device (mhd_sub_* of the C ABI)."""
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, eta: float, *, ct_mode: int = 0,
+                 stream: int | None = None):
+        import torch
+
+        self.torch = torch
+        self.lib = _bind(load_library())
+        self.nx, self.ny = int(nx), int(ny)
+        p = Params()
+        _check(self.lib.mhd_default_params(ctypes.byref(p), nx, ny, dx, dy, eta), "mhd_default_params")
+        p.ct_mode = ct_mode
+        h = ctypes.c_void_p()
+        _check(self.lib.mhd_sub_create(ctypes.byref(p), ctypes.c_void_p(stream) if stream else None,
+                                       ctypes.byref(h)), "mhd_sub_create")
+        self.h = h
+        self._bufs = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_sub_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mhd_sub_stream(self.h) or 0
+
+    def set_state(self, fields: Sequence[np.ndarray]):
+        fs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+        arr = (ctypes.c_void_p * 6)(*[f.ctypes.data for f in fs])
+        _check(self.lib.mhd_sub_set_state(self.h, arr), "mhd_sub_set_state")
+
+    def get_state(self):
+        out = [np.empty((self.ny, self.nx)) for _ in range(6)]
+        arr = (ctypes.c_void_p * 6)(*[f.ctypes.data for f in out])
+        _check(self.lib.mhd_sub_get_state(self.h, arr), "mhd_sub_get_state")
+        return out
+
+    def _buffer(self, key, n):
+        b = self._bufs.get(key)
+        if b is None or b.numel() != n:
+            b = self.torch.empty(n, dtype=self.torch.float64, device="cuda")
+            self._bufs[key] = b
+        return b
+
+    def pack(self, set_: int, side: int, width: int):
+        n = self.lib.mhd_sub_strip_doubles(self.h, set_, side, width)
+        buf = self._buffer((set_, side, width), n)
+        _check(self.lib.mhd_sub_pack(self.h, set_, side, width, ctypes.c_void_p(buf.data_ptr())), "mhd_sub_pack")
+        return buf
+
+    def recv_buffer(self, set_: int, side: int, width: int):
+        n = self.lib.mhd_sub_strip_doubles(self.h, set_, side, width)
+        return self._buffer(("recv", set_, side, width), n)
+
+    def unpack(self, set_: int, side: int, width: int, buf):
+        _check(self.lib.mhd_sub_unpack(self.h, set_, side, width, ctypes.c_void_p(buf.data_ptr())),
+               "mhd_sub_unpack")
+
+    def synchronize(self):
+        _check(self.lib.mhd_sub_synchronize(self.h), "mhd_sub_synchronize")
+
+    def cfl_speed(self):
+        v, bad = ctypes.c_double(), ctypes.c_int()
+        _check(self.lib.mhd_sub_cfl_speed(self.h, ctypes.byref(v), ctypes.byref(bad)), "mhd_sub_cfl_speed")
+        return v.value, bool(bad.value)
+
+    def set_step(self, dt: float, alpha: float):
+        _check(self.lib.mhd_sub_set_step(self.h, dt, alpha), "mhd_sub_set_step")
+
+    def stage(self, k: int):
+        _check(self.lib.mhd_sub_stage(self.h, k), "mhd_sub_stage")
+
+    def finalize(self):
+        _check(self.lib.mhd_sub_finalize(self.h), "mhd_sub_finalize")
+
+    def cg_rhs(self, solve_index: int):
+        out = (ctypes.c_double * 2)()
+        _check(self.lib.mhd_sub_cg_rhs(self.h, solve_index, out), "mhd_sub_cg_rhs")
+        return [out[0], out[1]]
+
+    def cg_matvec(self):
+        v = ctypes.c_double()
+        _check(self.lib.mhd_sub_cg_matvec(self.h, ctypes.byref(v)), "mhd_sub_cg_matvec")
+        return [v.value]
+
+    def cg_update(self, alpha: float):
+        out = (ctypes.c_double * 2)()
+        _check(self.lib.mhd_sub_cg_update(self.h, alpha, out), "mhd_sub_cg_update")
+        return [out[0], out[1]]
+
+    def cg_direction(self, beta: float):
+        _check(self.lib.mhd_sub_cg_direction(self.h, beta), "mhd_sub_cg_direction")
+
+    def cg_zero_solution(self):
+        _check(self.lib.mhd_sub_cg_zero_solution(self.h), "mhd_sub_cg_zero_solution")
+
+    def divb_sums(self):
+        out = (ctypes.c_double * 2)()
+        _check(self.lib.mhd_sub_divb_sums(self.h, out), "mhd_sub_divb_sums")
+        return [out[0], out[1]]
+
+
+_bound = set()
+
+
+def _bind(lib):
+    if id(lib) in _bound:
+        return lib
+    vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.c_int
+    lib.mhd_sub_halo.restype = ip
+    lib.mhd_sub_create.argtypes = [ctypes.POINTER(Params), vp, ctypes.POINTER(vp)]
+    lib.mhd_sub_destroy.argtypes = [vp]
+    lib.mhd_sub_stream.argtypes = [vp]
+    lib.mhd_sub_stream.restype = vp
+    lib.mhd_sub_set_state.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.mhd_sub_get_state.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.mhd_sub_strip_doubles.argtypes = [vp, ip, ip, ip]
+    lib.mhd_sub_strip_doubles.restype = ctypes.c_size_t
+    lib.mhd_sub_pack.argtypes = [vp, ip, ip, ip, vp]
+    lib.mhd_sub_unpack.argtypes = [vp, ip, ip, ip, vp]
+    lib.mhd_sub_cfl_speed.argtypes = [vp, dp, ctypes.POINTER(ip)]
+    lib.mhd_sub_set_step.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    lib.mhd_sub_stage.argtypes = [vp, ip]
+    lib.mhd_sub_finalize.argtypes = [vp]
+    lib.mhd_sub_cg_rhs.argtypes = [vp, ip, dp]
+    lib.mhd_sub_cg_matvec.argtypes = [vp, dp]
+    lib.mhd_sub_cg_update.argtypes = [vp, ctypes.c_double, dp]
+    lib.mhd_sub_cg_direction.argtypes = [vp, ctypes.c_double]
+    lib.mhd_sub_cg_zero_solution.argtypes = [vp]
+    lib.mhd_sub_divb_sums.argtypes = [vp, dp]
+    lib.mhd_sub_synchronize.argtypes = [vp]
+    assert lib.mhd_sub_halo() == HALO
+    _bound.add(id(lib))
+    return lib
+
+
+def _ordered_sum(rows) -> List[float]:
+    """Add equal-length lists of partial sums in the given order (subdomain / rank order)."""
+    out = [0.0] * len(rows[0])
+    for r in rows:
+        for k, v in enumerate(r):
+            out[k] += float(v)
+    return out
+
+
+class LocalTransport:
+    """Every subdomain in this process; `subs[i]` is subdomain i of the partition."""
+
+    def __init__(self, part: Partition, subs: Sequence):
+        assert len(subs) == part.count
+        self.part = part
+        self.subs = list(subs)
+
+    @property
+    def own(self):
+        return self.subs
+
+    def exchange(self, set_: int, width: int):
+        for axis in ((EAST, WEST), (NORTH, SOUTH)):
+            bufs = {}
+            for i, s in enumerate(self.subs):
+                for side in axis:
+                    bufs[(i, side)] = s.pack(set_, side, width)
+            for s in self.subs:
+                s.synchronize()
+            for i, s in enumerate(self.subs):
+                for side in axis:
+                    nb = self.part.neighbour(i, side)
+                    s.unpack(set_, side, width, bufs[(nb, OPPOSITE[side])])
+            for s in self.subs:
+                s.synchronize()
+
+    def sum(self, rows) -> List[float]:
+        return _ordered_sum(rows)
+
+    def max(self, values) -> float:
+        return max(values)
+
+    def any(self, flags) -> bool:
+        return any(flags)
+
+
+class DistTransport:
+    """One subdomain per rank of the default torch.distributed group (rank = subdomain index).
+    GPU subdomains exchange CUDA tensors (NCCL); CPU stand-ins exchange CPU tensors (gloo)."""
+
+    def __init__(self, part: Partition, sub, device=None):
+        import torch
+        import torch.distributed as dist
+
+        self.torch, self.dist = torch, dist
+        self.part = part
+        self.rank = dist.get_rank()
+        assert dist.get_world_size() == part.count
+        self.sub = sub
+        self.device = device if device is not None else torch.device("cpu")
+
+    @property
+    def own(self):
+        return [self.sub]
+
+    def _as_tensor(self, buf):
+        if isinstance(buf, np.ndarray):
+            return self.torch.from_numpy(np.ascontiguousarray(buf))
+        return buf
+
+    def exchange(self, set_: int, width: int):
+        for axis in ((EAST, WEST), (NORTH, SOUTH)):
+            for side in axis:
+                # shift toward `side`: send this side's strip to that neighbour, receive the strip
+                # the opposite neighbour sent toward `side` into the opposite ring
+                send = self.sub.pack(set_, side, width)
+                self.sub.synchronize()
+                dst = self.part.neighbour(self.rank, side)
+                src = self.part.neighbour(self.rank, OPPOSITE[side])
+                if dst == self.rank:
+                    self.sub.unpack(set_, OPPOSITE[side], width, send)
+                    continue
+                st = self._as_tensor(send)
+                rt = self.torch.empty_like(st)
+                ops = [self.dist.P2POp(self.dist.isend, st, dst), self.dist.P2POp(self.dist.irecv, rt, src)]
+                for req in self.dist.batch_isend_irecv(ops):
+                    req.wait()
+                self.sub.unpack(set_, OPPOSITE[side], width, rt.numpy() if isinstance(send, np.ndarray) else rt)
+            self.sub.synchronize()
+
+    def _gather(self, values) -> np.ndarray:
+        t = self.torch.tensor(values, dtype=self.torch.float64, device=self.device)
+        out = self.torch.empty(self.part.count * t.numel(), dtype=self.torch.float64, device=self.device)
+        self.dist.all_gather_into_tensor(out, t)
+        return out.cpu().numpy().reshape(self.part.count, -1)
+
+    def sum(self, rows) -> List[float]:
+        (mine,) = rows
+        return _ordered_sum(list(self._gather(list(mine))))
+
+    def max(self, values) -> float:
+        (mine,) = values
+        return float(np.max(self._gather([mine])))
+
+    def any(self, flags) -> bool:
+        (mine,) = flags
+        return bool(np.any(self._gather([1.0 if mine else 0.0])))
+
+
+class DecomposedRun:
+    """ARS(2,2,2) steps of one nx x ny periodic grid split over the transport's subdomains."""
+
+    def __init__(self, part: Partition, transport, dx: float, dy: float, eta: float, *,
+                 courant: float = 0.5, safety: float = 0.9, cg_tol: float = 0.0, cg_max_iters: int = 0):
+        self.part, self.tr = part, transport
+        self.dx, self.dy, self.eta = dx, dy, eta
+        self.courant, self.safety = courant, safety
+        self.tol = cg_tol if cg_tol > 0 else EPS
+        self.max_iters = cg_max_iters if cg_max_iters > 0 else 2 * part.nx * part.ny
+        self.status = "ok"
+        self.last_products = (0, 0)
+
+    def _own_indices(self):
+        if isinstance(self.tr, LocalTransport):
+            return list(range(self.part.count))
+        return [self.tr.rank]
+
+    def set_state(self, fields: Sequence[np.ndarray]):
+        """Global dense (ny, nx) planes; each subdomain takes its window, then the rings fill."""
+        for i, s in zip(self._own_indices(), self.tr.own):
+            rs, cs = self.part.window(i)
+            s.set_state([np.ascontiguousarray(f[rs, cs]) for f in fields])
+        self.tr.exchange(SET_STATE, HALO)
+
+    def get_state(self):
+        """Global dense planes (every rank's interiors; with DistTransport gathered to all)."""
+        out = [np.zeros((self.part.ny, self.part.nx)) for _ in range(6)]
+        if isinstance(self.tr, LocalTransport):
+            for i, s in enumerate(self.tr.subs):
+                rs, cs = self.part.window(i)
+                for k, f in enumerate(s.get_state()):
+                    out[k][rs, cs] = f
+            return out
+        mine = np.stack(self.tr.sub.get_state())
+        pieces = [None] * self.part.count
+        self.tr.dist.all_gather_object(pieces, mine)
+        for i, st in enumerate(pieces):
+            rs, cs = self.part.window(i)
+            for k in range(6):
+                out[k][rs, cs] = st[k]
+        return out
+
+    def cfl_dt(self) -> float:
+        """diagnostics.hpp:82-84 from the largest interior signal speed (the device formula)."""
+        speeds, bad = zip(*[s.cfl_speed() for s in self.tr.own])
+        if self.tr.any(list(bad)):
+            self.status = "nonfinite"
+        smaxv = max(self.tr.max(list(speeds)), 1e-8)
+        hmin = min(self.dx, self.dy)
+        dt_res = math.inf if self.eta == 0.0 else hmin * hmin / (4.0 * self.eta)
+        dt_hyp = self.courant * hmin / smaxv
+        return (dt_res if dt_res < dt_hyp else dt_hyp) * self.safety
+
+    def _solve(self, index: int) -> int:
+        own = self.tr.own
+        bb, abs_new = self.tr.sum([s.cg_rhs(index) for s in own])
+        threshold = max(self.tol * self.tol * bb, DBL_MIN)
+        if not math.isfinite(bb):
+            self.status = "nonfinite"
+            return 0
+        if bb == 0.0 or bb < threshold:
+            return 0  # x = 0 (cg_rhs zeroed it)
+        products = 0
+        converged = False
+        for _ in range(self.max_iters):
+            self.tr.exchange(SET_DIRECTION, 1)
+            (pq,) = self.tr.sum([s.cg_matvec() for s in own])
+            alpha = abs_new / pq
+            rr, rz = self.tr.sum([s.cg_update(alpha) for s in own])
+            products += 1
+            if not (math.isfinite(rr) and math.isfinite(alpha)):
+                self.status = "nonfinite"
+                for s in own:
+                    s.cg_zero_solution()
+                return products
+            if rr < threshold:
+                converged = True
+                break
+            beta = rz / abs_new
+            abs_new = rz
+            for s in own:
+                s.cg_direction(beta)
+        if not converged:
+            self.status = "cg_not_converged"
+        return products
+
+    def step(self, dt: float = 0.0, alpha: float | None = None):
+        """One IMEX step; dt <= 0 takes the CFL step. alpha defaults to (dt * eta) * g (the matrix
+        the reference driver builds for this dt). Returns (dt, (products of the two solves))."""
+        if dt <= 0.0:
+            dt = self.cfl_dt()
+        if alpha is None:
+            alpha = (dt * self.eta) * ARS_G
+        own = self.tr.own
+        for s in own:
+            s.set_step(dt, alpha)
+        for s in own:
+            s.stage(1)
+        self.tr.exchange(SET_PREDICTOR, HALO)
+        k1 = self._solve(0)
+        self.tr.exchange(SET_SOLUTION, HALO)
+        for s in own:
+            s.stage(2)
+        self.tr.exchange(SET_ACCUMULATOR_B, HALO)
+        k2 = self._solve(1)
+        self.tr.exchange(SET_SOLUTION, HALO)
+        for s in own:
+            s.finalize()
+        self.tr.exchange(SET_STATE, HALO)
+        self.last_products = (k1, k2)
+        return dt, (k1, k2)
+
+    def divb(self):
+        """calculate_current_div_B (diagnostics.hpp:15-42) over the whole grid: (rms, max)."""
+        rows = [s.divb_sums() for s in self.tr.own]
+        (sq,) = self.tr.sum([[r[0]] for r in rows])
+        mx = self.tr.max([max(r[1] for r in rows)])
+        return math.sqrt(sq / (self.part.nx * self.part.ny)), mx
+
+
+__all__ = ["Partition", "GpuSubdomain", "LocalTransport", "DistTransport", "DecomposedRun", "HALO",
+           "MHDError"]
