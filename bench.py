@@ -715,8 +715,32 @@ def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
         rm = trajectory(u0_of(az0 - s_ * daz), e0, adj)[0]
         fd_dir = float((((rp - rm) / (2 * s_)) * w).sum())
         fd_dir_loss = float((((rp - rm) / (2 * s_)) * ((rp + rm) / 2 - target)).sum())
+        # the same difference at half the step, and their Richardson combination (4 D(s/2) - D(s)) / 3,
+        # which removes an O(s^2) error term where the scheme is smooth
+        rp2 = trajectory(u0_of(az0 + 0.5 * s_ * daz), e0, adj)[0]
+        rm2 = trajectory(u0_of(az0 - 0.5 * s_ * daz), e0, adj)[0]
+        fd_dir_half = float((((rp2 - rm2) / s_) * w).sum())
+        fd_dir_rich = (4.0 * fd_dir_half - fd_dir) / 3.0
     f_launch, a_launch = adj.launch_counts()
+    mem_default = adj.device_bytes
     adj.close()
+    # the memory-bounded mode: one segment's solutions kept, each segment re-solved backwards
+    adj2 = m.Adjoint(n, n, dx, dx, eta, dt, nsteps, checkpoint_every=every, recompute_solves=True)
+    a2stream = torch.cuda.ExternalStream(adj2.stream)
+    g0b = torch.empty_like(u0)
+    adj2.set_eta(eta)
+    torch.cuda.synchronize()
+    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev2[0].record(a2stream)
+    adj2.forward(ptr(u0), ptr(uT))
+    ev2[1].record(a2stream)
+    adj2.backward(ptr(gT), ptr(g0b))
+    ev2[2].record(a2stream)
+    ev2[2].synchronize()
+    rec_fwd_ms, rec_bwd_ms = ev2[0].elapsed_time(ev2[1]), ev2[1].elapsed_time(ev2[2])
+    mem_recompute = adj2.device_bytes
+    same = bool(torch.equal(g0, g0b))
+    adj2.close()
     return {
         "workload": ADJ_WORKLOAD, "grid": [n, n], "steps": nsteps, "checkpoint_every": every,
         "forward_ms_per_step": fwd_ms / nsteps, "backward_ms_per_step": bwd_ms / nsteps,
@@ -724,6 +748,12 @@ def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
         "backward_includes": "recomputation of each segment's explicit stages from its checkpoint "
                              "(the implicit solutions of every step are kept by the forward pass)",
         "launches_per_step": {"forward": f_launch, "backward": a_launch},
+        "device_bytes": mem_default,
+        "recompute_solves": {"device_bytes": mem_recompute,
+                             "forward_ms_per_step": rec_fwd_ms / nsteps,
+                             "backward_ms_per_step": rec_bwd_ms / nsteps,
+                             "adjoint_over_forward": rec_bwd_ms / rec_fwd_ms,
+                             "gradient_bit_identical": same},
         "gradient_check": {
             "method": "central differences of the final state (two trajectories), contracted after",
             "d_eta": {"loss": "1/2|rho(T) - rho_target|^2", "adjoint": g_eta,
@@ -731,7 +761,11 @@ def measure_adjoint(torch, m, n=1024, nsteps=100, every=10, dt=1e-3, eta=5e-3):
                       "rel_err": abs(g_eta - fd_eta) / abs(fd_eta)},
             "d_az_direction": {"loss": "<w, rho(T)>, w ~ N(0,1)", "adjoint": g_dir,
                                "central_difference": fd_dir, "step": 3e-7,
-                               "rel_err": abs(g_dir - fd_dir) / abs(fd_dir)},
+                               "rel_err": abs(g_dir - fd_dir) / abs(fd_dir),
+                               "central_difference_half_step": fd_dir_half,
+                               "rel_err_half_step": abs(g_dir - fd_dir_half) / abs(fd_dir_half),
+                               "richardson": fd_dir_rich,
+                               "rel_err_richardson": abs(g_dir - fd_dir_rich) / abs(fd_dir_rich)},
             "d_az_direction_density_loss": {"loss": "1/2|rho(T) - rho_target|^2", "adjoint": g_dir_loss,
                                             "central_difference": fd_dir_loss, "step": 3e-7,
                                             "rel_err": abs(g_dir_loss - fd_dir_loss) / abs(fd_dir_loss)},
@@ -744,12 +778,24 @@ def run_profile_case(args):
     batched  the mixed 64-instance batch of the "batched" section, two CFL steps at a fixed
              decomposition (stage rows 128, tail 32, solver tiles of 32 rows), no autotuning;
     adjoint  the 1024^2 state of the "adjoint" section, one 10-step trajectory (one checkpoint
-             segment): forward, then backward."""
+             segment): forward, then backward;
+    snapshot the Orszag-Tang state at 2048^2 (201 MB, above the L2), one step, then one snapshot
+             packed on the device and copied to the host (mhd_snapshot_pack, 235 MB)."""
     import torch
 
     import magnetohydrodynamics_simulator_b200 as m
 
     torch.cuda.set_device(0)
+    if args.profile_case == "snapshot":
+        n = 2048
+        state, dx = make_state(n)
+        ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
+        ctx.set_state(state)
+        ctx.step(0.0)
+        buf = ctx.snapshot_pack(2, 50, 1e-3)
+        st = ctx.synchronize_status()
+        ctx.close()
+        return 0 if st == 0 and buf.size > 0 else 1
     if args.profile_case == "batched":
         specs, ics = [], []
         for n, e, seed in m.problems.mixed_batch(64):
@@ -806,7 +852,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
-    ap.add_argument("--profile-case", choices=("batched", "adjoint"), default=None,
+    ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot"), default=None,
                     help="run a small fixed case for a profiler and exit (no measurement)")
     args = ap.parse_args()
     if args.profile_case:

@@ -322,6 +322,10 @@ class DistTransport:
                 ops = [self.dist.P2POp(self.dist.isend, st, dst), self.dist.P2POp(self.dist.irecv, rt, src)]
                 for req in self.dist.batch_isend_irecv(ops):
                     req.wait()
+                if rt.is_cuda:
+                    # wait() orders torch's current stream after the transfer; the unpack runs on
+                    # the subdomain's own stream, so finish the transfer first
+                    self.torch.cuda.current_stream().synchronize()
                 self.sub.unpack(set_, OPPOSITE[side], width, rt.numpy() if isinstance(send, np.ndarray) else rt)
             self.sub.synchronize()
 

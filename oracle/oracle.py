@@ -274,7 +274,7 @@ class Reference:
         return rms.value, mx.value
 
     def write_snapshot(self, workdir, frame_index, snapshot_rate, dt):
-        """integrator_main.cpp:106-108: the reference writes workdir/output/snapshot_NNNNNN.dat
+        """integrator_main.cpp:107-109: the reference writes workdir/output/snapshot_NNNNNN.dat
         (its path is relative to the working directory); returns the file's bytes."""
         os.makedirs(os.path.join(workdir, "output"), exist_ok=True)
         cwd = os.getcwd()

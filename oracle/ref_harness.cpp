@@ -18,7 +18,7 @@
 //   ref_divb              diagnostics.hpp:15-42
 //   ref_explicit_rhs      solvers.hpp:393-402 (on a copy of the state)
 //   ref_run               integrator_main.cpp:76-112 (dt loop, matrix regeneration rule)
-//   ref_write_snapshot    integrator_main.cpp:106-108 (ghost fill, primitives,
+//   ref_write_snapshot    integrator_main.cpp:107-109 (ghost fill, primitives,
 //                         write_data_to_binary_file into output/ of the working directory)
 #include <iostream>
 #include <fstream>
