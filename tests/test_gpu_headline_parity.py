@@ -10,9 +10,10 @@ reference's include/*.hpp compiled here, driven through ref_harness.cpp).
   reference's driver loop run on their own.
 
 Tolerances: 1e-12 relative L-infinity per field (one to five steps), dts to 1e-12, CG products
-within 1, |div B|_inf <= 1e-12 on the GPU. (|div B|_inf is a rounding residue that grows by about
-eps |B| / dx per step in both codes -- ~7e-14 per step at 2048^2 -- so the two maxima are of the same
-size but not equal.)
+within 1, |div B|_inf <= 1e-12 on the GPU for Orszag-Tang. |div B|_inf is a rounding residue that
+grows by about eps |B| / dx per step in both codes -- ~7e-14 per step at 2048^2 -- so the two maxima
+are of the same size but not equal; the batch members (|B| up to ~7) are held to twice the
+reference's own value on the same run.
 """
 import numpy as np
 import pytest
@@ -118,10 +119,14 @@ def test_mixed_batch_members_match_reference(m):
         ref.set_state(ics[i])
         r_dts, r_prods = ref.run(steps)
         want = ref.get_state()
+        r_divb = ref.divb()[1]
         del ref
         assert np.max(np.abs(dts[i] - r_dts) / r_dts) <= 1e-12, (n_i, dts[i], r_dts)
         assert np.max(np.abs(prods[i] - r_prods)) <= 1, (n_i, prods[i], r_prods)
         errs = _errs(b.get_state(i), want, floor=1.0)
         assert max(errs) <= STEP_TOL, (n_i, errs)
-        assert b.divb(i)[1] <= 1e-11  # |B| ~ 5-7 at dx ~ 6e-3 here: rounding level ~1e-12
+        # |B| reaches 5-7 here and dx is as small as 6e-3, so the rounding residue of div B is
+        # ~1e-11 in the reference itself: the GPU's must be of the same size
+        g_divb = b.divb(i)[1]
+        assert g_divb <= max(1e-12, 2.0 * r_divb), (n_i, g_divb, r_divb)
     b.close()
