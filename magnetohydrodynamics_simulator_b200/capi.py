@@ -89,6 +89,9 @@ def load_library() -> ctypes.CDLL:
     lib.mhd_destroy.argtypes = [vp]
     lib.mhd_set_state.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
     lib.mhd_get_state.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
+    lib.mhd_set_state_async.argtypes = [vp, P6]
+    lib.mhd_get_state_async.argtypes = [vp, P6]
+    lib.mhd_transfers_wait.argtypes = [vp]
     lib.mhd_set_state_device.argtypes = [vp, P6]
     lib.mhd_get_state_device.argtypes = [vp, P6]
     lib.mhd_get_primitives.argtypes = [vp, P6, ctypes.c_int, ctypes.c_int]
@@ -243,6 +246,18 @@ class Context:
 
     def get_state_into(self, out: Sequence[np.ndarray], layout: int = LAYOUT_DENSE, ng: int = 2):
         _check(self.lib.mhd_get_state(self.h, _host_ptrs(out), layout, ng), "mhd_get_state")
+
+    def set_state_async(self, fields: Sequence[np.ndarray]):
+        """Pipelined upload of dense host planes (pinned for overlap); see mhd_set_state_async.
+        The arrays must stay alive and untouched until transfers_wait()."""
+        _check(self.lib.mhd_set_state_async(self.h, _host_ptrs(fields)), "mhd_set_state_async")
+
+    def get_state_async(self, out: Sequence[np.ndarray]):
+        """Pipelined read-back into dense host planes; ready after transfers_wait()."""
+        _check(self.lib.mhd_get_state_async(self.h, _host_ptrs(out)), "mhd_get_state_async")
+
+    def transfers_wait(self):
+        _check(self.lib.mhd_transfers_wait(self.h), "mhd_transfers_wait")
 
     def set_state_device(self, ptrs: Sequence[int]):
         _check(self.lib.mhd_set_state_device(self.h, _device_ptrs(ptrs)), "mhd_set_state_device")

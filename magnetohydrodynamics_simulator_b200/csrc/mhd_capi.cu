@@ -80,6 +80,12 @@ struct mhd_context {
     std::vector<cudaEvent_t> events;
     size_t events_used = 0;
     mhd_host::SnapshotWriter* snap = nullptr;  // created by the first mhd_snapshot_write
+    // pipelined host transfers (mhd_set_state_async / mhd_get_state_async), created on first use
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t ev_ctx = nullptr, ev_h2d = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_d2h[6]{};
+    bool d2h_pending[6]{};
+    bool join_pending = false;  // state planes still read by mhd_get_state_async's copies
 };
 
 namespace {
@@ -450,6 +456,8 @@ mhd_status mhd_destroy(mhd_context* c) {
     if (!c) return MHD_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->h2d) cudaStreamSynchronize(c->h2d);
+    if (c->d2h) cudaStreamSynchronize(c->d2h);
     delete c->snap;  // waits for the snapshots in flight
     cudaFree(c->pool);
     cudaFree(c->partials);
@@ -463,6 +471,12 @@ mhd_status mhd_destroy(mhd_context* c) {
     cudaFree(c->run.prods);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    for (cudaEvent_t e : {c->ev_ctx, c->ev_h2d, c->ev_join})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->ev_d2h)
+        if (e) cudaEventDestroy(e);
+    if (c->h2d) cudaStreamDestroy(c->h2d);
+    if (c->d2h) cudaStreamDestroy(c->d2h);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     cudaGetLastError();
     delete c;
@@ -476,9 +490,30 @@ int mhd_launches_per_step(mhd_context* c) {
     return 6;  // coefficients, stage 1, CG, stage 2, CG, finalize
 }
 
+// Work about to write the state planes waits for the copies of mhd_get_state_async.
+static mhd_status join_transfers(mhd_context* c) {
+    if (!c->join_pending) return MHD_OK;
+    MHD_TRY(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    c->join_pending = false;
+    return MHD_OK;
+}
+
+// Copy streams and events of the pipelined transfers (first use).
+static mhd_status ensure_transfer_streams(mhd_context* c) {
+    if (c->h2d) return MHD_OK;
+    MHD_TRY(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    MHD_TRY(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    MHD_TRY(cudaEventCreateWithFlags(&c->ev_ctx, cudaEventDisableTiming));
+    MHD_TRY(cudaEventCreateWithFlags(&c->ev_h2d, cudaEventDisableTiming));
+    MHD_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    for (cudaEvent_t& e : c->ev_d2h) MHD_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return MHD_OK;
+}
+
 mhd_status mhd_set_state(mhd_context* c, const double* const f[6], int layout, int ng) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
+    if ((s = join_transfers(c)) != MHD_OK) return s;
     if (!f || (layout != MHD_LAYOUT_DENSE && layout != MHD_LAYOUT_PADDED) ||
         (layout == MHD_LAYOUT_PADDED && ng < 0))
         return MHD_ERR_INVALID_ARGUMENT;
@@ -501,9 +536,67 @@ mhd_status mhd_set_state(mhd_context* c, const double* const f[6], int layout, i
     return refresh_cfl(c);
 }
 
+mhd_status mhd_set_state_async(mhd_context* c, const double* const f[6]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k)
+        if (!f[k]) return MHD_ERR_INVALID_ARGUMENT;
+    if ((s = ensure_transfer_streams(c)) != MHD_OK) return s;
+    // the planes are overwritten only after the work queued on the context so far
+    MHD_TRY(cudaEventRecord(c->ev_ctx, c->stream));
+    MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_ctx, 0));
+    for (int k = 0; k < 6; ++k) {
+        // plane k's host buffer (and device plane) may still be read by the previous
+        // mhd_get_state_async: its copy goes first, the other planes' copies overlap it
+        if (c->d2h_pending[k]) MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_d2h[k], 0));
+        MHD_TRY(cudaMemcpyAsync(c->S[k], f[k], c->n * sizeof(double), cudaMemcpyHostToDevice, c->h2d));
+    }
+    if (c->join_pending) {  // copies of planes the last mhd_get_state_async skipped
+        MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_join, 0));
+        c->join_pending = false;
+    }
+    MHD_TRY(cudaEventRecord(c->ev_h2d, c->h2d));
+    MHD_TRY(cudaStreamWaitEvent(c->stream, c->ev_h2d, 0));
+    c->have_state = true;
+    return refresh_cfl(c);
+}
+
+mhd_status mhd_get_state_async(mhd_context* c, double* const f[6]) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (!f) return MHD_ERR_INVALID_ARGUMENT;
+    if (!c->have_state) return MHD_ERR_NO_STATE;
+    if ((s = ensure_transfer_streams(c)) != MHD_OK) return s;
+    MHD_TRY(cudaEventRecord(c->ev_ctx, c->stream));
+    MHD_TRY(cudaStreamWaitEvent(c->d2h, c->ev_ctx, 0));
+    for (int k = 0; k < 6; ++k) {
+        if (!f[k]) continue;
+        MHD_TRY(cudaMemcpyAsync(f[k], c->S[k], c->n * sizeof(double), cudaMemcpyDeviceToHost, c->d2h));
+        MHD_TRY(cudaEventRecord(c->ev_d2h[k], c->d2h));
+        c->d2h_pending[k] = true;
+    }
+    // work that writes the state planes waits for these copies (join_transfers); a following
+    // mhd_set_state_async orders its own copies plane by plane instead, so the copies of two
+    // steps overlap
+    MHD_TRY(cudaEventRecord(c->ev_join, c->d2h));
+    c->join_pending = true;
+    return MHD_OK;
+}
+
+mhd_status mhd_transfers_wait(mhd_context* c) {
+    mhd_status s = check_ctx(c);
+    if (s != MHD_OK) return s;
+    if (c->h2d) MHD_TRY(cudaStreamSynchronize(c->h2d));
+    if (c->d2h) MHD_TRY(cudaStreamSynchronize(c->d2h));
+    for (bool& b : c->d2h_pending) b = false;
+    return MHD_OK;
+}
+
 mhd_status mhd_set_state_device(mhd_context* c, const double* const f[6]) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
+    if ((s = join_transfers(c)) != MHD_OK) return s;
     if (!f) return MHD_ERR_INVALID_ARGUMENT;
     for (int k = 0; k < 6; ++k) {
         if (!f[k]) return MHD_ERR_INVALID_ARGUMENT;
@@ -578,6 +671,7 @@ mhd_status mhd_set_implicit_coefficient(mhd_context* c, double alpha) {
 mhd_status mhd_step(mhd_context* c, double dt) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
+    if ((s = join_transfers(c)) != MHD_OK) return s;
     if (!c->have_state) return MHD_ERR_NO_STATE;
     if (!std::isfinite(dt)) return MHD_ERR_INVALID_ARGUMENT;
     s = launch_coeffs(c, dt, c->alpha_fixed ? 0 : 1, 0.0, nullptr);
@@ -589,6 +683,7 @@ mhd_status mhd_run(mhd_context* c, int nsteps, double dt_fixed, double t_end, do
                    long long* prods_out) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
+    if ((s = join_transfers(c)) != MHD_OK) return s;
     if (!c->have_state) return MHD_ERR_NO_STATE;
     if (nsteps < 0 || !std::isfinite(dt_fixed) || !std::isfinite(t_end)) return MHD_ERR_INVALID_ARGUMENT;
     if (nsteps == 0) return MHD_OK;
@@ -791,6 +886,7 @@ mhd_status mhd_divb(mhd_context* c, double* rms, double* maxabs) {
 mhd_status mhd_synchronize(mhd_context* c) {
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
+    if ((s = mhd_transfers_wait(c)) != MHD_OK) return s;
     MHD_TRY(cudaMemcpyAsync(c->host_pinned, c->status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost,
                             c->stream));
     MHD_TRY(cudaStreamSynchronize(c->stream));

@@ -397,3 +397,44 @@ def test_other_initial_conditions_match_reference(m, name):
     errs = _errs(ctx.get_state(), fields(d, f"{name}_final"), floor=1e-3)
     assert max(errs) <= STEP_TOL, errs
     assert ctx.divb()[1] <= 1e-12
+
+
+def test_pipelined_host_transfers_match_synchronous_calls(m):
+    """mhd_set_state_async / mhd_get_state_async (copies on two copy streams, a step's read-back
+    overlapping the next upload) round-trip every step's state through pinned host planes and give
+    the same states, bit for bit, as the synchronous set_state / get_state calls; the read-back
+    also holds the state when no upload follows it."""
+    import torch
+
+    n = 96
+    dx = m.problems.grid_spacing(n)
+    ic = m.problems.orszag_tang(n, n, dx, dx)
+    a = m.Context(n, n, dx, dx, 1e-2)
+    b = m.Context(n, n, dx, dx, 1e-2)
+    pinned = [torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy() for _ in range(6)]
+    for k in range(6):
+        pinned[k][...] = ic[k]
+    host = [f.copy() for f in ic]
+    for _ in range(4):
+        a.set_state_async(pinned)
+        a.step(0.0)
+        a.get_state_async(pinned)
+        b.set_state(host)
+        b.step(0.0)
+        host = b.get_state()
+    a.transfers_wait()
+    for x, y in zip(pinned, host):
+        assert np.array_equal(x, y)
+    # a read-back followed by more steps: the steps wait for the copies
+    a.get_state_async(pinned)
+    a.step(1e-3)
+    a.step(1e-3)
+    a.transfers_wait()
+    for x, y in zip(pinned, host):
+        assert np.array_equal(x, y)
+    b.step(1e-3)
+    b.step(1e-3)
+    a.synchronize()
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(x, y)
+    assert a.synchronize_status() == 0
