@@ -90,11 +90,13 @@ __device__ __forceinline__ int batch_next_item(int* queue) {
     return __shfl_sync(0xffffffffu, it, 0);
 }
 
-// Stage 2 of the batch forms its y slopes per face: the carried slopes (10 registers) push the
-// persistent kernel, which holds an item loop around the sweep, into spills (measured on B200:
-// 4096^2 explicit stages 0.169 -> 0.161 ns per zone, 16 x 1024^2 0.161 -> 0.151).
+// Stage 2 of the batch carries its y slopes in shared memory (as a single context's stage 2 does)
+// and keeps the branchy HLL: the persistent kernel holds an item loop around the sweep, which the
+// branch-free HLL pushes into spills. (Measured on B200 on the 64-instance mixed batch: with the
+// carried values in shared memory, per-face y slopes 7.18 -> 6.97 ms per step, carried slopes
+// 6.93 ms.)
 #ifndef MHD_BATCH_YREUSE_2
-#define MHD_BATCH_YREUSE_2 0
+#define MHD_BATCH_YREUSE_2 1
 #endif
 #ifndef MHD_BATCH_XREUSE_2
 #define MHD_BATCH_XREUSE_2 MHD_SWEEP_XREUSE_2
@@ -108,11 +110,11 @@ k_stage_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double sw_ring_mem[];
 #else
-    static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];
+    static double sw_ring_mem[SW_WARPS * (SW_RING * SW_SLOT + SW_CARRY)];
 #endif
     __shared__ SweepInstRec rec[SW_WARPS];
     const int wl = threadIdx.x >> 5;
-    double* const ring = sw_ring_mem + (size_t)wl * SW_RING * SW_SLOT;
+    double* const ring = sw_ring_mem + (size_t)wl * sweep_warp_doubles(MODE);
     const RecPlanes pl{base, &rec[wl]};
     for (;;) {
         const int it = batch_next_item(queue);
@@ -126,8 +128,8 @@ k_stage_batch(const BatchInst* __restrict__ insts, const SweepItem* __restrict__
         }
         __syncwarp();
         stage_sweep_warp<MODE, RecPlanes, MODE == 1 ? MHD_SWEEP_YREUSE_1 : MHD_BATCH_YREUSE_2,
-                         MODE == 1 ? MHD_SWEEP_XREUSE_1 : MHD_BATCH_XREUSE_2>(I.C, pl, e.sx, e.r0,
-                                                                              e.r1, ring);
+                         MODE == 1 ? MHD_SWEEP_XREUSE_1 : MHD_BATCH_XREUSE_2, MODE == 1>(
+            I.C, pl, e.sx, e.r0, e.r1, ring);
     }
 }
 

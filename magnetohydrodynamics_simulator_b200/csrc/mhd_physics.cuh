@@ -119,7 +119,8 @@ __device__ __forceinline__ Flux conserved(const Prim& w) {
 // HLL.hpp:126-172 (DIR = 0) and :177-218 (DIR = 1). L is the lower/left state. SELECT: form the
 // HLL average for every face and select the case afterwards instead of returning early (the same
 // values; straight-line code that schedules better where registers allow it, measured on B200:
-// stage 1 1.030 -> 1.010 ms at 4096^2, stage 2 slower through spills).
+// stage 1 1.030 -> 1.010 ms at 4096^2; stage 2 uses it once its carried values live in shared
+// memory, the batch's stage 2 does not, as it spills there).
 template <int DIR, bool SELECT = false>
 __device__ __forceinline__ Flux hll(const Prim& L, const Prim& R) {
     const Flux FL = phys_flux<DIR>(L);

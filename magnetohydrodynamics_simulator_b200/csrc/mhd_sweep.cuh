@@ -35,6 +35,13 @@ constexpr int SW_OUT = 28;       // output columns per warp
 constexpr int SW_RING = 8;       // row slots per warp (power of two): rows c-1 .. c+6
 constexpr int SW_E1 = 196;       // offset of E1 in a stage-2 slot
 constexpr int SW_SLOT = 230;     // doubles per slot (1840 bytes, 16-byte multiple)
+// Stage 2 keeps the values it carries from row to row -- the y slopes and the y-face fluxes of the
+// previous row, 10 per lane -- in shared memory after its ring, not in registers. The registers it
+// frees let stage 2 evaluate HLL branch-free as stage 1 does (measured on B200 at 4096^2: stage 2
+// 1.001 -> 0.954 ms; stage 1, whose carried values fit its registers, is 1.7% slower this way).
+constexpr int SW_CARRY = 10 * 32;
+// doubles of shared memory per warp of an explicit-stage kernel
+constexpr int sweep_warp_doubles(int mode) { return SW_RING * SW_SLOT + (mode == 2 ? SW_CARRY : 0); }
 // One warp (an independent strip segment) per block: blocks retire warp by warp, so the tail of
 // a launch and the persistent batch kernels balance at warp granularity (measured on B200 against
 // 4-warp blocks at the same registers: stage 1 1.29 -> 1.25 ms, stage 2 1.24 -> 1.15 ms at 4096^2).
@@ -129,7 +136,7 @@ struct RecPlanes {
 
 // The sweep of one warp over rows [r0, r1) of column strip sx of one grid.
 template <int MODE, class PL, bool kYReuse = (MODE == 1) ? MHD_SWEEP_YREUSE_1 : MHD_SWEEP_YREUSE_2,
-          bool kXReuse = (MODE == 1) ? MHD_SWEEP_XREUSE_1 : MHD_SWEEP_XREUSE_2>
+          bool kXReuse = (MODE == 1) ? MHD_SWEEP_XREUSE_1 : MHD_SWEEP_XREUSE_2, bool kSelect = true>
 __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ C, const PL& pl,
                                                  int sx, int r0, int r1, double* ring) {
     const int lane = threadIdx.x & 31;
@@ -155,15 +162,25 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
     // ---- windows (index 0 = oldest row)
     double Prho[4], Pvx[4], Pvy[4], Pp[4], Pbxc[4];  // rows c-1 .. c+2
     double Pbyc[3];                                   // rows c .. c+2
-    double Sy[5];                                     // y slopes of row c (when carried)
-    double fy_prev[5];                                // y-face flux of row c-1
+    // y slopes of row c (when carried) and the y-face flux of row c-1: registers in stage 1,
+    // shared memory after the ring in stage 2
+    double Sy_r[5], fy_r[5];
+    double* const carry = ring + SW_RING * SW_SLOT;
+    auto Sy = [&](int k) -> double& {
+        if constexpr (MODE == 2) return carry[(5 + k) * 32 + lane];
+        else return Sy_r[k];
+    };
+    auto fy_prev = [&](int k) -> double& {
+        if constexpr (MODE == 2) return carry[k * 32 + lane];
+        else return fy_r[k];
+    };
     double fxbt_prev = 0.0, ez_prev = 0.0, jz_prev = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) { Prho[k] = 1.0; Pvx[k] = 0.0; Pvy[k] = 0.0; Pp[k] = 1.0; Pbxc[k] = 0.0; }
 #pragma unroll
     for (int k = 0; k < 3; ++k) Pbyc[k] = 0.0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) { Sy[k] = 0.0; fy_prev[k] = 0.0; }
+    for (int k = 0; k < 5; ++k) { Sy(k) = 0.0; fy_prev(k) = 0.0; }
 
     const int cstart = r0 - SW_PRE;
     // The input rows live in the ring: sweep row r sits in slot (r - cstart + 1) % SW_RING; it is
@@ -259,17 +276,17 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
                 const double s_vy = minmod(Pvy[2] - Pvy[1], Pvy[3] - Pvy[2]);
                 const double s_p = minmod(Pp[2] - Pp[1], Pp[3] - Pp[2]);
                 const double s_bx = minmod(Pbxc[2] - Pbxc[1], Pbxc[3] - Pbxc[2]);
-                Dn.rho = Prho[1] + 0.5 * Sy[0];
-                Dn.vx = Pvx[1] + 0.5 * Sy[1];
-                Dn.vy = Pvy[1] + 0.5 * Sy[2];
-                Dn.p = Pp[1] + 0.5 * Sy[3];
-                Dn.bx = Pbxc[1] + 0.5 * Sy[4];
+                Dn.rho = Prho[1] + 0.5 * Sy(0);
+                Dn.vx = Pvx[1] + 0.5 * Sy(1);
+                Dn.vy = Pvy[1] + 0.5 * Sy(2);
+                Dn.p = Pp[1] + 0.5 * Sy(3);
+                Dn.bx = Pbxc[1] + 0.5 * Sy(4);
                 Up.rho = Prho[2] - 0.5 * s_rho;
                 Up.vx = Pvx[2] - 0.5 * s_vx;
                 Up.vy = Pvy[2] - 0.5 * s_vy;
                 Up.p = Pp[2] - 0.5 * s_p;
                 Up.bx = Pbxc[2] - 0.5 * s_bx;
-                Sy[0] = s_rho; Sy[1] = s_vx; Sy[2] = s_vy; Sy[3] = s_p; Sy[4] = s_bx;
+                Sy(0) = s_rho; Sy(1) = s_vx; Sy(2) = s_vy; Sy(3) = s_p; Sy(4) = s_bx;
             } else {
                 Dn.rho = recon_hi(Prho[0], Prho[1], Prho[2]);
                 Dn.vx = recon_hi(Pvx[0], Pvx[1], Pvx[2]);
@@ -283,7 +300,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
                 Up.bx = recon_lo(Pbxc[1], Pbxc[2], Pbxc[3]);
             }
             Dn.by = Up.by = slot(c + 1)[5 * 32 + lane];  // byf of row c+1
-            fy = hll<1, MODE == 1>(Dn, Up);
+            fy = hll<1, kSelect>(Dn, Up);
         }
         // ---- XFACE: right face of (i, c); L = upper x-extrapolation of column i, R = lower of
         //      i+1. With kXReuse every lane limits its own column's slope once and hands its lower
@@ -309,7 +326,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
             xrecon(Pp[1], L.p, R.p);
             xrecon(Pbyc[0], L.by, R.by);
             L.bx = R.bx = shdn(slot(c)[4 * 32 + lane], 1);  // bxf(i+1, c)
-            fx = hll<0, MODE == 1>(L, R);
+            fx = hll<0, kSelect>(L, R);
         }
         // ---- CORNER (i, c): eN = -Fx^By(i-1, c), eS = -Fx^By(i-1, c-1), eE = Fy^Bx(i, c-1),
         //      eW = Fy^Bx(i-1, c-1); corner velocity = mean of the 4 cells
@@ -317,8 +334,8 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
         {
             const double eN = -shup(fx.bt, 1);
             const double eS = -shup(fxbt_prev, 1);
-            const double eE = fy_prev[4];
-            const double eW = shup(fy_prev[4], 1);
+            const double eE = fy_prev(4);
+            const double eW = shup(fy_prev(4), 1);
             const double vxc = 0.25 * (Pvx[1] + shup(Pvx[1], 1) + Pvx[0] + shup(Pvx[0], 1));
             const double vyc = 0.25 * (Pvy[1] + shup(Pvy[1], 1) + Pvy[0] + shup(Pvy[0], 1));
             ez = corner_ez(eN, eS, eE, eW, vxc, vyc, pl.ct_mode());
@@ -333,10 +350,10 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
         // ---- hydro rates of row c
         {
             double f[4];
-            f[0] = -((fx.rho - shup(fx.rho, 1)) * idx + (fy.rho - fy_prev[0]) * idy);
-            f[1] = -((fx.mx - shup(fx.mx, 1)) * idx + (fy.mx - fy_prev[1]) * idy);
-            f[2] = -((fx.my - shup(fx.my, 1)) * idx + (fy.my - fy_prev[2]) * idy);
-            f[3] = -((fx.E - shup(fx.E, 1)) * idx + (fy.E - fy_prev[3]) * idy);
+            f[0] = -((fx.rho - shup(fx.rho, 1)) * idx + (fy.rho - fy_prev(0)) * idy);
+            f[1] = -((fx.mx - shup(fx.mx, 1)) * idx + (fy.mx - fy_prev(1)) * idy);
+            f[2] = -((fx.my - shup(fx.my, 1)) * idx + (fy.my - fy_prev(2)) * idy);
+            f[3] = -((fx.E - shup(fx.E, 1)) * idx + (fy.E - fy_prev(3)) * idy);
             if (out_lane && c >= r0 && c < r1) {
                 const size_t g = (size_t)c * pl.nx() + i;
                 if constexpr (MODE == 1) {
@@ -383,7 +400,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
             }
         }
         // ---- carry to the next row
-        fy_prev[0] = fy.rho; fy_prev[1] = fy.mx; fy_prev[2] = fy.my; fy_prev[3] = fy.E; fy_prev[4] = fy.bt;
+        fy_prev(0) = fy.rho; fy_prev(1) = fy.mx; fy_prev(2) = fy.my; fy_prev(3) = fy.E; fy_prev(4) = fy.bt;
         fxbt_prev = fx.bt;
         ez_prev = ez;
         jz_prev = jz;
@@ -394,7 +411,7 @@ __device__ __forceinline__ void stage_sweep_warp(const StepCoeffs* __restrict__ 
 
 // Dynamic shared memory of a block of the explicit-stage kernels (their warps' row rings).
 constexpr size_t sweep_smem_bytes(int mode) {
-    return (void)mode, (size_t)SW_WARPS * SW_RING * SW_SLOT * sizeof(double);
+    return (size_t)SW_WARPS * sweep_warp_doubles(mode) * sizeof(double);
 }
 
 template <int MODE>
@@ -404,9 +421,9 @@ k_stage_sweep(Domain D, const StepCoeffs* __restrict__ C, CPlanes in,
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double sw_ring_mem[];
 #else
-    static double sw_ring_mem[SW_WARPS * SW_RING * SW_SLOT];  // host compilation: one copy
+    static double sw_ring_mem[SW_WARPS * (SW_RING * SW_SLOT + SW_CARRY)];  // host compilation: one copy
 #endif
-    double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * SW_RING * SW_SLOT;
+    double* const ring = sw_ring_mem + (size_t)(threadIdx.x >> 5) * sweep_warp_doubles(MODE);
     const int w = blockIdx.x * SW_WARPS + (threadIdx.x >> 5);
     if (w >= G.nwarps) return;
     const ParamPlanes pl{in, xsolve, outA, outB, D};
