@@ -452,6 +452,9 @@ def run_gpu_arm(args):
     snapshot = None
     if not args.no_snapshot and rank == 0:
         snapshot = measure_snapshots(torch, m, ctx)
+    decomposed = None
+    if not args.no_decomposed and rank == 0:
+        decomposed = measure_decomposed(torch, m)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -477,6 +480,7 @@ def run_gpu_arm(args):
         "batched": batched,
         "adjoint": adjoint,
         "snapshot": snapshot,
+        "decomposed": decomposed,
     }
     ctx.close()
     if dist is not None:
@@ -572,6 +576,56 @@ def measure_snapshots(torch, m, ctx, steps=100, every=50):
         "files_on_disk_s": wall_s,
         "file_write_GBps": nchunks * nbytes / wall_s / 1e9,
     }
+
+
+def measure_decomposed(torch, m, n=2048, P=2, Q=2, steps=3):
+    """The domain decomposition on one GPU: Orszag-Tang n^2 split P x Q, subdomains exchanging
+    their rings through device buffers (the ranks of a multi-GPU run emulated in one process),
+    against a single context on the same steps; wall time per step (the decomposed solve waits on
+    the host for every product's sums) and the largest per-field difference."""
+    from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
+                                                                LocalTransport, Partition)
+
+    dx = m.problems.grid_spacing(n)
+    ic = m.problems.orszag_tang(n, n, dx, dx)
+    part = Partition(n, n, P, Q)
+    subs = [GpuSubdomain(*part.shape(i), dx, dx, ETA) for i in range(part.count)]
+    run = DecomposedRun(part, LocalTransport(part, subs), dx, dx, ETA, courant=COURANT)
+    run.set_state(ic)
+    run.step()  # warm-up
+    start = run.get_state()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dts, prods = [], []
+    for _ in range(steps):
+        dt, k = run.step()
+        dts.append(dt)
+        prods.append(k)
+    torch.cuda.synchronize()
+    dec = time.perf_counter() - t0
+    ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
+    ctx.set_state(start)
+    ctx.step(dts[0])  # warm-up of the single context, then the same steps again from the start
+    ctx.set_state(start)
+    ctx.synchronize()
+    t1 = time.perf_counter()
+    for dt in dts:
+        ctx.step(dt)
+    ctx.synchronize()
+    single = time.perf_counter() - t1
+    errs = [float(np.max(np.abs(g - w)) / max(float(np.max(np.abs(w))), 1.0))
+            for g, w in zip(run.get_state(), ctx.get_state())]
+    out = {"what": f"Orszag-Tang {n}x{n} split {P}x{Q} on one GPU (rings through device buffers), "
+                   f"{steps} CFL steps, against a single context stepped with the same dts",
+           "ms_per_step_decomposed": 1e3 * dec / steps,
+           "ms_per_step_single_context": 1e3 * single / steps,
+           "cg_products": prods, "max_rel_linf_vs_single": max(errs), "divb_max": run.divb()[1],
+           "status": run.status,
+           "note": "wall time; the decomposed solve reads each product's partial sums on the host"}
+    ctx.close()
+    for sd in subs:
+        sd.close()
+    return out
 
 
 def measure_batched(torch, m, steps):
@@ -872,6 +926,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
+    ap.add_argument("--no-decomposed", action="store_true")
     ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot"), default=None,
                     help="run a small fixed case for a profiler and exit (no measurement)")
     args = ap.parse_args()
