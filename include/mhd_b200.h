@@ -373,12 +373,16 @@ mhd_status mhd_sub_finalize(mhd_subdomain* s);
 /* CG phases on the interior corners. cg_rhs: b = eta J_z(B*) of the predictor's (solve 0) or the
  * accumulator's (solve 1) faces, r = b, p = z = b/d, x = 0; out = partial |b|^2, r.z. cg_matvec:
  * q = (I - alpha L) p, *pq = partial p.q. cg_update: x += alpha p, r -= alpha q, z = r/d;
- * out = partial |r|^2, r.z. cg_direction: p = z + beta p. cg_zero_solution: x = 0. */
+ * out = partial |r|^2, r.z. cg_direction: p = z + beta p. cg_zero_solution: x = 0.
+ * cg_rhs, cg_matvec and cg_update wait for their sums when given an output pointer; with NULL they
+ * only enqueue (several subdomains' phases then run together) and mhd_sub_sums(s, out, n) waits
+ * and returns the n sums of the last such phase. */
 mhd_status mhd_sub_cg_rhs(mhd_subdomain* s, int solve_index, double out[2]);
 mhd_status mhd_sub_cg_matvec(mhd_subdomain* s, double* pq);
 mhd_status mhd_sub_cg_update(mhd_subdomain* s, double alpha, double out[2]);
 mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta);
 mhd_status mhd_sub_cg_zero_solution(mhd_subdomain* s);
+mhd_status mhd_sub_sums(mhd_subdomain* s, double* out, int n);
 /* Interior div B partials (diagnostics.hpp:15-42): out[0] = sum of div^2, out[1] = max |div|. */
 mhd_status mhd_sub_divb_sums(mhd_subdomain* s, double out[2]);
 mhd_status mhd_sub_synchronize(mhd_subdomain* s);

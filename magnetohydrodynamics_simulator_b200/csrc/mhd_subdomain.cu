@@ -289,6 +289,7 @@ struct mhd_subdomain {
     SweepGeom sg[2]{}, fg{};
     int st_blocks[2]{}, fn_blocks = 0;
     int blocks = 0;     // grid of the per-cell interior kernels
+    int pending_sums = 0;  // sums enqueued by a CG phase without an output pointer
 };
 
 namespace {
@@ -368,6 +369,17 @@ mhd_status read_small(mhd_subdomain* s, int n, double* out) {
                             s->stream));
     MHD_TRY(cudaStreamSynchronize(s->stream));
     for (int k = 0; k < n; ++k) out[k] = s->host_out[k];
+    return MHD_OK;
+}
+
+// The CG phases' sums: with an output pointer, wait and return them; without, only enqueue their
+// copy to pinned host memory (mhd_sub_sums reads them), so that several subdomains' phases run at
+// the same time.
+mhd_status sums_out(mhd_subdomain* s, int n, double* out) {
+    if (out) return read_small(s, n, out);
+    MHD_TRY(cudaMemcpyAsync(s->host_out, s->dev_out, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                            s->stream));
+    s->pending_sums = n;
     return MHD_OK;
 }
 
@@ -630,7 +642,7 @@ mhd_status mhd_sub_finalize(mhd_subdomain* s) {
 mhd_status mhd_sub_cg_rhs(mhd_subdomain* s, int solve_index, double out[2]) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    if (!out || (solve_index != 0 && solve_index != 1)) return MHD_ERR_INVALID_ARGUMENT;
+    if (solve_index != 0 && solve_index != 1) return MHD_ERR_INVALID_ARGUMENT;
     const double* bx = solve_index == 0 ? s->T[4] : s->A[4];
     const double* by = solve_index == 0 ? s->T[5] : s->A[5];
     k_sub_cg_rhs<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->prm.eta, 1.0 / s->prm.dx, 1.0 / s->prm.dy,
@@ -638,29 +650,37 @@ mhd_status mhd_sub_cg_rhs(mhd_subdomain* s, int solve_index, double out[2]) {
     MHD_TRY(cudaGetLastError());
     k_sub_final<2><<<1, 32, 0, s->stream>>>(s->part, s->blocks, s->dev_out);
     MHD_TRY(cudaGetLastError());
-    return read_small(s, 2, out);
+    return sums_out(s, 2, out);
 }
 
 mhd_status mhd_sub_cg_matvec(mhd_subdomain* s, double* pq) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    if (!pq) return MHD_ERR_INVALID_ARGUMENT;
     k_sub_cg_matvec<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, s->part);
     MHD_TRY(cudaGetLastError());
     k_sub_final<1><<<1, 32, 0, s->stream>>>(s->part, s->blocks, s->dev_out);
     MHD_TRY(cudaGetLastError());
-    return read_small(s, 1, pq);
+    return sums_out(s, 1, pq);
 }
 
 mhd_status mhd_sub_cg_update(mhd_subdomain* s, double alpha, double out[2]) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    if (!out) return MHD_ERR_INVALID_ARGUMENT;
     k_sub_cg_update<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, alpha, s->part);
     MHD_TRY(cudaGetLastError());
     k_sub_final<2><<<1, 32, 0, s->stream>>>(s->part, s->blocks, s->dev_out);
     MHD_TRY(cudaGetLastError());
-    return read_small(s, 2, out);
+    return sums_out(s, 2, out);
+}
+
+mhd_status mhd_sub_sums(mhd_subdomain* s, double* out, int n) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!out || n < 1 || n != s->pending_sums) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < n; ++k) out[k] = s->host_out[k];
+    s->pending_sums = 0;
+    return MHD_OK;
 }
 
 mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta) {

@@ -23,8 +23,10 @@ kernels, and the global reductions of the implicit solve and the CFL step.
 
 A subdomain object needs: set_state, get_state, pack(set, side, width) -> buffer,
 unpack(set, side, width, buffer), synchronize, cfl_speed, set_step, stage(1|2), finalize,
-cg_rhs, cg_matvec, cg_update, cg_direction, cg_zero_solution, divb_sums. ``GpuSubdomain`` is the
-one over the C ABI.
+cg_rhs, cg_matvec, cg_update (each with wait=False: enqueue only, sums(n) returns the sums),
+cg_direction, cg_zero_solution, divb_sums; and, where its work runs on a stream, record_event /
+wait_event, with which LocalTransport orders the subdomains' streams without host waits.
+``GpuSubdomain`` is the one over the C ABI.
 """
 from __future__ import annotations
 
@@ -159,6 +161,16 @@ class GpuSubdomain:
     def synchronize(self):
         _check(self.lib.mhd_sub_synchronize(self.h), "mhd_sub_synchronize")
 
+    # stream ordering between subdomains (rings move without host waits)
+    def record_event(self):
+        ev = self.torch.cuda.Event()
+        ev.record(self.torch.cuda.ExternalStream(self.stream))
+        return ev
+
+    def wait_event(self, ev):
+        if ev is not None:
+            self.torch.cuda.ExternalStream(self.stream).wait_event(ev)
+
     def cfl_speed(self):
         v, bad = ctypes.c_double(), ctypes.c_int()
         _check(self.lib.mhd_sub_cfl_speed(self.h, ctypes.byref(v), ctypes.byref(bad)), "mhd_sub_cfl_speed")
@@ -173,20 +185,26 @@ class GpuSubdomain:
     def finalize(self):
         _check(self.lib.mhd_sub_finalize(self.h), "mhd_sub_finalize")
 
-    def cg_rhs(self, solve_index: int):
-        out = (ctypes.c_double * 2)()
+    # CG phases: wait=True returns the phase's sums; wait=False only enqueues (sums() reads them)
+    def cg_rhs(self, solve_index: int, wait: bool = True):
+        out = (ctypes.c_double * 2)() if wait else None
         _check(self.lib.mhd_sub_cg_rhs(self.h, solve_index, out), "mhd_sub_cg_rhs")
-        return [out[0], out[1]]
+        return [out[0], out[1]] if wait else None
 
-    def cg_matvec(self):
-        v = ctypes.c_double()
-        _check(self.lib.mhd_sub_cg_matvec(self.h, ctypes.byref(v)), "mhd_sub_cg_matvec")
-        return [v.value]
+    def cg_matvec(self, wait: bool = True):
+        v = ctypes.c_double() if wait else None
+        _check(self.lib.mhd_sub_cg_matvec(self.h, ctypes.byref(v) if wait else None), "mhd_sub_cg_matvec")
+        return [v.value] if wait else None
 
-    def cg_update(self, alpha: float):
-        out = (ctypes.c_double * 2)()
+    def cg_update(self, alpha: float, wait: bool = True):
+        out = (ctypes.c_double * 2)() if wait else None
         _check(self.lib.mhd_sub_cg_update(self.h, alpha, out), "mhd_sub_cg_update")
-        return [out[0], out[1]]
+        return [out[0], out[1]] if wait else None
+
+    def sums(self, n: int):
+        out = (ctypes.c_double * n)()
+        _check(self.lib.mhd_sub_sums(self.h, out, n), "mhd_sub_sums")
+        return list(out)
 
     def cg_direction(self, beta: float):
         _check(self.lib.mhd_sub_cg_direction(self.h, beta), "mhd_sub_cg_direction")
@@ -230,6 +248,7 @@ def _bind(lib):
     lib.mhd_sub_cg_zero_solution.argtypes = [vp]
     lib.mhd_sub_divb_sums.argtypes = [vp, dp]
     lib.mhd_sub_synchronize.argtypes = [vp]
+    lib.mhd_sub_sums.argtypes = [vp, dp, ip]
     assert lib.mhd_sub_halo() == HALO
     _bound.add(id(lib))
     return lib
@@ -257,19 +276,29 @@ class LocalTransport:
         return self.subs
 
     def exchange(self, set_: int, width: int):
+        """Both axes, west/east then south/north. Subdomains with streams (record_event) are
+        ordered by events: an unpack waits for the neighbour's pack, and a pack into a buffer
+        waits until the last unpack from it is done; no host waits. Others run in call order."""
+        evented = hasattr(self.subs[0], "record_event")
+        if not hasattr(self, "_consumed"):
+            self._consumed = {}
         for axis in ((EAST, WEST), (NORTH, SOUTH)):
-            bufs = {}
+            bufs, packed = {}, {}
             for i, s in enumerate(self.subs):
                 for side in axis:
+                    if evented:
+                        s.wait_event(self._consumed.get((i, set_, side, width)))
                     bufs[(i, side)] = s.pack(set_, side, width)
-            for s in self.subs:
-                s.synchronize()
+                    if evented:
+                        packed[(i, side)] = s.record_event()
             for i, s in enumerate(self.subs):
                 for side in axis:
                     nb = self.part.neighbour(i, side)
+                    if evented:
+                        s.wait_event(packed[(nb, OPPOSITE[side])])
                     s.unpack(set_, side, width, bufs[(nb, OPPOSITE[side])])
-            for s in self.subs:
-                s.synchronize()
+                    if evented:
+                        self._consumed[(nb, set_, OPPOSITE[side], width)] = s.record_event()
 
     def sum(self, rows) -> List[float]:
         return _ordered_sum(rows)
@@ -402,9 +431,16 @@ class DecomposedRun:
         dt_hyp = self.courant * hmin / smaxv
         return (dt_res if dt_res < dt_hyp else dt_hyp) * self.safety
 
+    @staticmethod
+    def _phase(own, launch, n):
+        """Enqueue a CG phase on every subdomain first, then read their sums (in order)."""
+        for s in own:
+            launch(s)
+        return [s.sums(n) for s in own]
+
     def _solve(self, index: int) -> int:
         own = self.tr.own
-        bb, abs_new = self.tr.sum([s.cg_rhs(index) for s in own])
+        bb, abs_new = self.tr.sum(self._phase(own, lambda s: s.cg_rhs(index, wait=False), 2))
         threshold = max(self.tol * self.tol * bb, DBL_MIN)
         if not math.isfinite(bb):
             self.status = "nonfinite"
@@ -415,9 +451,9 @@ class DecomposedRun:
         converged = False
         for _ in range(self.max_iters):
             self.tr.exchange(SET_DIRECTION, 1)
-            (pq,) = self.tr.sum([s.cg_matvec() for s in own])
+            (pq,) = self.tr.sum(self._phase(own, lambda s: s.cg_matvec(wait=False), 1))
             alpha = abs_new / pq
-            rr, rz = self.tr.sum([s.cg_update(alpha) for s in own])
+            rr, rz = self.tr.sum(self._phase(own, lambda s: s.cg_update(alpha, wait=False), 2))
             products += 1
             if not (math.isfinite(rr) and math.isfinite(alpha)):
                 self.status = "nonfinite"

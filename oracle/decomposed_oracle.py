@@ -154,8 +154,19 @@ class OracleSubdomain:
         for q in (1, 2, 3):
             self.S[q] = self.A[q].copy()
 
-    # -- conjugate gradient on the interior corners
-    def cg_rhs(self, index):
+    # -- conjugate gradient on the interior corners (wait=False keeps the sums for sums())
+    def sums(self, n):
+        out, self._sums = self._sums, None
+        assert out is not None and len(out) == n
+        return out
+
+    def _ret(self, vals, wait):
+        if wait:
+            return vals
+        self._sums = vals
+        return None
+
+    def cg_rhs(self, index, wait=True):
         bx, by = (self.T[4], self.T[5]) if index == 0 else (self.A[4], self.A[5])
         I = self.I
         idx, idy = 1.0 / self.dx, 1.0 / self.dy
@@ -164,21 +175,21 @@ class OracleSubdomain:
         self.zv[I] = self.invdiag * b[I]
         self.p[I] = self.zv[I]
         self.x[I] = 0.0
-        return [float(np.sum(b[I] * b[I])), float(np.sum(b[I] * self.zv[I]))]
+        return self._ret([float(np.sum(b[I] * b[I])), float(np.sum(b[I] * self.zv[I]))], wait)
 
-    def cg_matvec(self):
+    def cg_matvec(self, wait=True):
         I, p = self.I, self.p
         q = (-self.cy) * np.roll(p, 1, axis=0) + (-self.cx) * np.roll(p, 1, axis=1) + self.diag * p + \
             (-self.cx) * np.roll(p, -1, axis=1) + (-self.cy) * np.roll(p, -1, axis=0)
         self.q[I] = q[I]
-        return [float(np.sum(p[I] * q[I]))]
+        return self._ret([float(np.sum(p[I] * q[I]))], wait)
 
-    def cg_update(self, alpha):
+    def cg_update(self, alpha, wait=True):
         I = self.I
         self.x[I] = self.x[I] + alpha * self.p[I]
         self.r[I] = self.r[I] - alpha * self.q[I]
         self.zv[I] = self.invdiag * self.r[I]
-        return [float(np.sum(self.r[I] * self.r[I])), float(np.sum(self.r[I] * self.zv[I]))]
+        return self._ret([float(np.sum(self.r[I] * self.r[I])), float(np.sum(self.r[I] * self.zv[I]))], wait)
 
     def cg_direction(self, beta):
         I = self.I
