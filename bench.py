@@ -403,32 +403,50 @@ def run_gpu_arm(args):
               "k_stage_sweep<2>": per_kernel["stage2"]["ms"] / step_kernels_ms,
               "k_finalize_sweep": per_kernel["finalize"]["ms"] / step_kernels_ms}
     longest = max(KERNELS, key=lambda k: per_kernel[k]["ms"])
-    dominant = longest
-    traffic = None
+    # per kernel function: (per-launch algorithmic bytes, mean launch ms, launches per step, key of
+    # its measured DRAM bytes per zone and per unit, units per launch)
+    funcs = {
+        "k_stage_sweep<1>": (ALG_BYTES["stage1"] * zones, per_kernel["stage1"]["ms"], 1, "stage1", 1),
+        "k_cg_sweep": (ALG_BYTES["cg_per_iter"] * (k1 + k2) / 2 * zones, solver_ms / 2, 2, "cg", (k1 + k2) / 2),
+        "k_stage_sweep<2>": (ALG_BYTES["stage2"] * zones, per_kernel["stage2"]["ms"], 1, "stage2", 1),
+        "k_finalize_sweep": (ALG_BYTES["finalize"] * zones, per_kernel["finalize"]["ms"], 1, "finalize", 1),
+    }
+    dominant = max(funcs, key=lambda f: shares[f])  # the largest share of the step's time
+    tr = {}
     tr_path = os.path.join(ROOT, "profiles", "dram_bytes_per_zone.json")
     if os.path.exists(tr_path):
         try:
             with open(tr_path) as f:
                 tr = json.load(f)
-            key = "cg" if dominant.startswith("cg") else dominant
-            if key in tr:
-                per_zone = tr[key]["bytes_per_zone_per_unit"]
-                units = (k1 if dominant == "cg1" else k2) if key == "cg" else 1
-                traffic = per_zone * units * zones
         except Exception:
-            traffic = None
+            tr = {}
+
+    def traffic_of(name):
+        _, _, _, key, units = funcs[name]
+        if key not in tr:
+            return None
+        return tr[key]["bytes_per_zone_per_unit"] * units * zones
+
+    def figures(name):
+        alg, ms, launches, _, _ = funcs[name]
+        gbs = alg / (ms * 1e-3) / 1e9
+        return {"kernel": name, "launches_per_step": launches, "share_of_step": shares[name],
+                "alg_bytes_per_launch": alg, "ms_per_launch": ms, "achieved": gbs, "frac": gbs / peak,
+                "traffic": traffic_of(name)}
+
+    dom = figures(dominant)
+    longest_name = {"stage1": "k_stage_sweep<1>", "cg1": "k_cg_sweep", "stage2": "k_stage_sweep<2>",
+                    "cg2": "k_cg_sweep", "finalize": "k_finalize_sweep"}[longest]
     step_alg = (384.0 + 48.0 * (k1 + k2)) * zones
     step_ms = ms_max / args.steps
     roofline = {
         "bound": "hbm", "kernel": dominant,
-        "achieved": per_kernel[dominant]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-        "frac": per_kernel[dominant]["achieved_gbs"] / peak,
-        "traffic": traffic, "peak_source": peak_kind,
-        "kernel_is": "the longest single launch of the step",
-        "largest_share": {"kernel": "k_cg_sweep", "launches_per_step": 2,
-                          "share_of_step": shares["k_cg_sweep"], "ms_per_step": solver_ms,
-                          "alg_bytes_per_zone": ALG_BYTES["cg_per_iter"] * (k1 + k2),
-                          "achieved": solver_gbs, "frac": solver_gbs / peak},
+        "achieved": dom["achieved"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
+        "traffic": dom["traffic"], "peak_source": peak_kind,
+        "kernel_is": "the kernel with the largest share of the step's time (per launch: its "
+                     "algorithmic bytes over its mean launch time)",
+        "longest_launch": figures(longest_name),
+        "per_function": {f: figures(f) for f in funcs},
         "shares": shares,
         "step": {"alg_bytes_per_zone": 384.0 + 48.0 * (k1 + k2),
                  "achieved": step_alg / (step_ms * 1e-3) / 1e9,
