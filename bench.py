@@ -596,9 +596,9 @@ def measure_snapshots(torch, m, ctx, steps=100, every=50):
     }
 
 
-def measure_decomposed(torch, m, n=2048, P=2, Q=2, steps=3):
+def measure_decomposed(torch, m, n=4096, P=2, Q=2, steps=3):
     """The domain decomposition on one GPU: Orszag-Tang n^2 split P x Q, subdomains exchanging
-    their rings through device buffers (the ranks of a multi-GPU run emulated in one process),
+    their rings by device copies (the ranks of a multi-GPU run emulated in one process),
     against a single context on the same steps; wall time per step (the decomposed solve waits on
     the host for every product's sums) and the largest per-field difference."""
     from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
@@ -633,7 +633,7 @@ def measure_decomposed(torch, m, n=2048, P=2, Q=2, steps=3):
     single = time.perf_counter() - t1
     errs = [float(np.max(np.abs(g - w)) / max(float(np.max(np.abs(w))), 1.0))
             for g, w in zip(run.get_state(), ctx.get_state())]
-    out = {"what": f"Orszag-Tang {n}x{n} split {P}x{Q} on one GPU (rings through device buffers), "
+    out = {"what": f"Orszag-Tang {n}x{n} split {P}x{Q} on one GPU (rings by device copies), "
                    f"{steps} CFL steps, against a single context stepped with the same dts",
            "ms_per_step_decomposed": 1e3 * dec / steps,
            "ms_per_step_single_context": 1e3 * single / steps,

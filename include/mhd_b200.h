@@ -362,6 +362,11 @@ size_t mhd_sub_strip_doubles(mhd_subdomain* s, int set, int side, int width);
  * Asynchronous on the subdomain's stream. */
 mhd_status mhd_sub_pack(mhd_subdomain* s, int set, int side, int width, double* buf);
 mhd_status mhd_sub_unpack(mhd_subdomain* s, int set, int side, int width, const double* buf);
+/* Every ring of `set` (width 1..MHD_SUB_HALO) refreshed for P x Q subdomains that live in this
+ * process on one device (subs[q * P + p]): device-to-device copies from each neighbour's interior
+ * strips, west/east then south/north, on the receiving subdomain's stream, ordered by events; no
+ * host wait. Neighbours along x must have equal rows, along y equal columns. */
+mhd_status mhd_sub_exchange_local(mhd_subdomain* const* subs, int P, int Q, int set, int width);
 /* Largest CFL signal speed over the interior of the state (diagnostics.hpp:60-78), and whether a
  * value is not finite. Synchronous. */
 mhd_status mhd_sub_cfl_speed(mhd_subdomain* s, double* smax, int* nonfinite);

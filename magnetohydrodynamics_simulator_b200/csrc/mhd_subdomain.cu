@@ -290,6 +290,8 @@ struct mhd_subdomain {
     int st_blocks[2]{}, fn_blocks = 0;
     int blocks = 0;     // grid of the per-cell interior kernels
     int pending_sums = 0;  // sums enqueued by a CG phase without an output pointer
+    cudaEvent_t ev_ready = nullptr;  // in-process exchange: this subdomain's strips may be read
+    cudaEvent_t ev_done = nullptr;   // in-process exchange: this subdomain's rings are filled
 };
 
 namespace {
@@ -472,6 +474,9 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
     s->V.p = q; q += s->ne;
     s->V.q = q; q += s->ne;
     s->V.z = q;
+    if (cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming) != cudaSuccess)
+        return fail(MHD_ERR_CUDA);
     if (cudaMemsetAsync(s->pool, 0, (size_t)kSubPlanes * s->ne * sizeof(double), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->coeffs, 0, sizeof(StepCoeffs), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->scratch_status, 0, sizeof(DeviceStatus), s->stream) != cudaSuccess ||
@@ -491,6 +496,8 @@ mhd_status mhd_sub_destroy(mhd_subdomain* s) {
     cudaFree(s->part);
     cudaFree(s->dev_out);
     if (s->host_out) cudaFreeHost(s->host_out);
+    if (s->ev_ready) cudaEventDestroy(s->ev_ready);
+    if (s->ev_done) cudaEventDestroy(s->ev_done);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     cudaGetLastError();
     delete s;
@@ -564,6 +571,65 @@ mhd_status mhd_sub_unpack(mhd_subdomain* s, int set, int side, int width, const 
     k_sub_strip<false><<<blocks, kSubNT, 0, s->stream>>>(pl, np, s->iv.nxe, x0, y0, w, h,
                                                          const_cast<double*>(buf));
     MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_exchange_local(mhd_subdomain* const* subs, int P, int Q, int set, int width) {
+    if (!subs || P < 1 || Q < 1) return MHD_ERR_INVALID_ARGUMENT;
+    const int count = P * Q;
+    for (int i = 0; i < count; ++i) {
+        if (!subs[i] || subs[i]->device != subs[0]->device) return MHD_ERR_INVALID_ARGUMENT;
+        Planes pl;
+        int x0, y0, w, h;
+        if (set_planes(subs[i], set, &pl) == 0 || !strip_rect(subs[i], MHD_SUB_WEST, width, true, &x0, &y0, &w, &h))
+            return MHD_ERR_INVALID_ARGUMENT;
+    }
+    // neighbours must agree on the strips they exchange: equal rows along x, equal widths along y
+    for (int i = 0; i < count; ++i) {
+        const int p = i % P, q = i / P;
+        const mhd_subdomain* e = subs[q * P + (p + 1) % P];
+        const mhd_subdomain* n = subs[((q + 1) % Q) * P + p];
+        if (e->iv.ny != subs[i]->iv.ny || n->iv.nx != subs[i]->iv.nx) return MHD_ERR_INVALID_ARGUMENT;
+    }
+    MHD_TRY(cudaSetDevice(subs[0]->device));
+    const int sides[2][2] = {{MHD_SUB_WEST, MHD_SUB_EAST}, {MHD_SUB_SOUTH, MHD_SUB_NORTH}};
+    for (int axis = 0; axis < 2; ++axis) {
+        // every subdomain's work so far is done before a neighbour reads its strips
+        for (int i = 0; i < count; ++i) MHD_TRY(cudaEventRecord(subs[i]->ev_ready, subs[i]->stream));
+        for (int i = 0; i < count; ++i) {
+            mhd_subdomain* me = subs[i];
+            const int p = i % P, q = i / P;
+            for (int k = 0; k < 2; ++k) {
+                const int side = sides[axis][k];
+                const int opposite = side ^ 1;  // WEST <-> EAST, SOUTH <-> NORTH
+                int nb;
+                if (side == MHD_SUB_WEST) nb = q * P + (p + P - 1) % P;
+                else if (side == MHD_SUB_EAST) nb = q * P + (p + 1) % P;
+                else if (side == MHD_SUB_SOUTH) nb = ((q + Q - 1) % Q) * P + p;
+                else nb = ((q + 1) % Q) * P + p;
+                mhd_subdomain* from = subs[nb];
+                if (from != me) MHD_TRY(cudaStreamWaitEvent(me->stream, from->ev_ready, 0));
+                // my ring beyond `side` <- the neighbour's strip next to its opposite side
+                int dx0, dy0, w, h, sx0, sy0, sw, sh;
+                strip_rect(me, side, width, false, &dx0, &dy0, &w, &h);
+                strip_rect(from, opposite, width, true, &sx0, &sy0, &sw, &sh);
+                Planes dst, src;
+                const int np = set_planes(me, set, &dst);
+                set_planes(from, set, &src);
+                for (int c = 0; c < np; ++c)
+                    MHD_TRY(cudaMemcpy2DAsync(dst.f[c] + (size_t)dy0 * me->iv.nxe + dx0,
+                                              (size_t)me->iv.nxe * sizeof(double),
+                                              src.f[c] + (size_t)sy0 * from->iv.nxe + sx0,
+                                              (size_t)from->iv.nxe * sizeof(double), (size_t)w * sizeof(double),
+                                              h, cudaMemcpyDeviceToDevice, me->stream));
+            }
+        }
+        // a subdomain changes its interior again only after its neighbours have copied from it
+        for (int i = 0; i < count; ++i) MHD_TRY(cudaEventRecord(subs[i]->ev_done, subs[i]->stream));
+        for (int i = 0; i < count; ++i)
+            for (int j = 0; j < count; ++j)
+                if (j != i) MHD_TRY(cudaStreamWaitEvent(subs[i]->stream, subs[j]->ev_done, 0));
+    }
     return MHD_OK;
 }
 

@@ -249,6 +249,7 @@ def _bind(lib):
     lib.mhd_sub_divb_sums.argtypes = [vp, dp]
     lib.mhd_sub_synchronize.argtypes = [vp]
     lib.mhd_sub_sums.argtypes = [vp, dp, ip]
+    lib.mhd_sub_exchange_local.argtypes = [ctypes.POINTER(vp), ip, ip, ip, ip]
     assert lib.mhd_sub_halo() == HALO
     _bound.add(id(lib))
     return lib
@@ -266,19 +267,28 @@ def _ordered_sum(rows) -> List[float]:
 class LocalTransport:
     """Every subdomain in this process; `subs[i]` is subdomain i of the partition."""
 
-    def __init__(self, part: Partition, subs: Sequence):
+    def __init__(self, part: Partition, subs: Sequence, native: bool = True):
         assert len(subs) == part.count
         self.part = part
         self.subs = list(subs)
+        # GPU subdomains of one process exchange natively (device copies ordered by events);
+        # native=False moves their strips through pack/unpack buffers, as across GPUs
+        self._native = None
+        if native and all(isinstance(s_, GpuSubdomain) for s_ in self.subs):
+            self._native = (ctypes.c_void_p * part.count)(*[s_.h for s_ in self.subs])
 
     @property
     def own(self):
         return self.subs
 
     def exchange(self, set_: int, width: int):
-        """Both axes, west/east then south/north. Subdomains with streams (record_event) are
-        ordered by events: an unpack waits for the neighbour's pack, and a pack into a buffer
-        waits until the last unpack from it is done; no host waits. Others run in call order."""
+        """Both axes, west/east then south/north. GPU subdomains use mhd_sub_exchange_local (direct
+        device copies, ordered by events). Other subdomains with streams (record_event) pack and
+        unpack through buffers ordered by events; the rest run in call order."""
+        if self._native is not None:
+            _check(self.subs[0].lib.mhd_sub_exchange_local(self._native, self.part.P, self.part.Q,
+                                                           set_, width), "mhd_sub_exchange_local")
+            return
         evented = hasattr(self.subs[0], "record_event")
         if not hasattr(self, "_consumed"):
             self._consumed = {}

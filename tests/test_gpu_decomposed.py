@@ -26,23 +26,26 @@ def m():
     return mod
 
 
-def _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic):
+def _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=True):
     from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
                                                                 LocalTransport, Partition)
 
     part = Partition(nx, ny, P, Q)
     subs = [GpuSubdomain(*part.shape(i), dx, dy, eta) for i in range(part.count)]
-    run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, eta)
+    run = DecomposedRun(part, LocalTransport(part, subs, native=native), dx, dy, eta)
     run.set_state(ic)
     return run, subs
 
 
-@pytest.mark.parametrize("nx,ny,P,Q,steps", [(96, 80, 2, 2, 3), (70, 45, 3, 2, 2), (128, 128, 2, 1, 3)])
-def test_decomposed_steps_match_single_context(m, nx, ny, P, Q, steps):
+@pytest.mark.parametrize("nx,ny,P,Q,steps,native", [(96, 80, 2, 2, 3, True), (70, 45, 3, 2, 2, True),
+                                                    (128, 128, 2, 1, 3, True), (96, 80, 2, 2, 3, False)])
+def test_decomposed_steps_match_single_context(m, nx, ny, P, Q, steps, native):
+    """native: rings by mhd_sub_exchange_local; otherwise through mhd_sub_pack / mhd_sub_unpack
+    buffers (the path strips take between GPUs)."""
     dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
     eta = 0.02
     ic = smooth_state(nx, ny, dx, dy, seed=nx + ny)
-    run, subs = _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic)
+    run, subs = _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=native)
     ctx = m.Context(nx, ny, dx, dy, eta)
     ctx.set_state(ic)
     orc = Oracle(nx, ny, dx, dy, eta)
