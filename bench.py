@@ -345,8 +345,8 @@ def run_gpu_arm(args):
 
     # ---- end to end through the C ABI with host buffers: every step uploads its input state from
     # pinned host memory and reads its result back. Pipelined form (mhd_set_state_async /
-    # mhd_get_state_async): plane by plane on two copy streams, so one step's read-back overlaps the
-    # next step's upload; the timed region ends when the last read-back is in host memory.
+    # mhd_get_state_async): in quarter planes on two copy streams, so one step's read-back overlaps
+    # the next step's upload; the timed region ends when the last read-back is in host memory.
     pinned = [torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy() for _ in range(6)]
     ctx.get_state_into(pinned)
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
@@ -485,7 +485,7 @@ def run_gpu_arm(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
                 "d2h_bytes_per_step": int(6 * zones * 8), "steps": e2e_steps,
                 "how": "mhd_set_state_async + mhd_step + mhd_get_state_async per step from pinned "
-                       "host planes (read-back and next upload overlap plane by plane)",
+                       "host planes (read-back and next upload overlap piece by piece)",
                 "synchronous": {"value": world * zones * e2e_steps / (e2e_sync_ms * 1e-3),
                                 "ms_per_step": e2e_sync_ms / e2e_steps,
                                 "how": "mhd_set_state + mhd_step + mhd_get_state per step"}},

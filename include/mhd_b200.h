@@ -78,10 +78,10 @@ mhd_status mhd_get_state(mhd_context* ctx, double* const fields[6], int layout, 
 /* Pipelined host transfers, for streaming states through host memory step after step (no
  * counterpart in the reference, whose state lives on the host). Dense nx*ny host planes, pinned for
  * the copies to overlap (pageable memory works but serialises). Both calls only enqueue: the copies
- * run on two copy streams of the context, plane by plane, so that a state's read-back and the next
- * state's upload overlap in the two directions of the host link. mhd_set_state_async: the next
- * step waits for the upload, and plane k's upload waits for the previous mhd_get_state_async's
- * copy of plane k (the same host buffer may be passed to both). mhd_get_state_async: copies the
+ * run on two copy streams of the context, in quarter planes, so that a state's read-back and the
+ * next state's upload overlap in the two directions of the host link. mhd_set_state_async: the next
+ * step waits for the upload, and each piece's upload waits for the previous mhd_get_state_async's
+ * copy of that piece (the same host buffer may be passed to both). mhd_get_state_async: copies the
  * current state once the work queued so far is done; later steps wait for these copies before
  * they overwrite the state. The host buffers are ready after mhd_transfers_wait (or
  * mhd_synchronize). */

@@ -83,8 +83,10 @@ struct mhd_context {
     // pipelined host transfers (mhd_set_state_async / mhd_get_state_async), created on first use
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t ev_ctx = nullptr, ev_h2d = nullptr, ev_join = nullptr;
-    cudaEvent_t ev_d2h[6]{};
-    bool d2h_pending[6]{};
+    // pipelined transfers move each plane in kXferChunks pieces, one event per piece
+    static constexpr int kXferChunks = 4;
+    cudaEvent_t ev_d2h[6 * kXferChunks]{};
+    bool d2h_pending[6 * kXferChunks]{};
     bool join_pending = false;  // state planes still read by mhd_get_state_async's copies
 };
 
@@ -546,11 +548,16 @@ mhd_status mhd_set_state_async(mhd_context* c, const double* const f[6]) {
     // the planes are overwritten only after the work queued on the context so far
     MHD_TRY(cudaEventRecord(c->ev_ctx, c->stream));
     MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_ctx, 0));
+    constexpr int KC = mhd_context::kXferChunks;
     for (int k = 0; k < 6; ++k) {
-        // plane k's host buffer (and device plane) may still be read by the previous
-        // mhd_get_state_async: its copy goes first, the other planes' copies overlap it
-        if (c->d2h_pending[k]) MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_d2h[k], 0));
-        MHD_TRY(cudaMemcpyAsync(c->S[k], f[k], c->n * sizeof(double), cudaMemcpyHostToDevice, c->h2d));
+        for (int q = 0; q < KC; ++q) {
+            // this piece's host buffer (and device plane) may still be read by the previous
+            // mhd_get_state_async: its copy goes first, the later pieces' copies overlap it
+            const size_t b = c->n * q / KC, e = c->n * (q + 1) / KC;
+            if (c->d2h_pending[k * KC + q]) MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_d2h[k * KC + q], 0));
+            MHD_TRY(cudaMemcpyAsync(c->S[k] + b, f[k] + b, (e - b) * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->h2d));
+        }
     }
     if (c->join_pending) {  // copies of planes the last mhd_get_state_async skipped
         MHD_TRY(cudaStreamWaitEvent(c->h2d, c->ev_join, 0));
@@ -570,11 +577,16 @@ mhd_status mhd_get_state_async(mhd_context* c, double* const f[6]) {
     if ((s = ensure_transfer_streams(c)) != MHD_OK) return s;
     MHD_TRY(cudaEventRecord(c->ev_ctx, c->stream));
     MHD_TRY(cudaStreamWaitEvent(c->d2h, c->ev_ctx, 0));
+    constexpr int KC = mhd_context::kXferChunks;
     for (int k = 0; k < 6; ++k) {
         if (!f[k]) continue;
-        MHD_TRY(cudaMemcpyAsync(f[k], c->S[k], c->n * sizeof(double), cudaMemcpyDeviceToHost, c->d2h));
-        MHD_TRY(cudaEventRecord(c->ev_d2h[k], c->d2h));
-        c->d2h_pending[k] = true;
+        for (int q = 0; q < KC; ++q) {
+            const size_t b = c->n * q / KC, e = c->n * (q + 1) / KC;
+            MHD_TRY(cudaMemcpyAsync(f[k] + b, c->S[k] + b, (e - b) * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->d2h));
+            MHD_TRY(cudaEventRecord(c->ev_d2h[k * KC + q], c->d2h));
+            c->d2h_pending[k * KC + q] = true;
+        }
     }
     // work that writes the state planes waits for these copies (join_transfers); a following
     // mhd_set_state_async orders its own copies plane by plane instead, so the copies of two
