@@ -610,9 +610,10 @@ mhd_status mhd_sub_exchange_local(mhd_subdomain* const* subs, int P, int Q, int 
                 mhd_subdomain* from = subs[nb];
                 if (from != me) MHD_TRY(cudaStreamWaitEvent(me->stream, from->ev_ready, 0));
                 // my ring beyond `side` <- the neighbour's strip next to its opposite side
-                int dx0, dy0, w, h, sx0, sy0, sw, sh;
-                strip_rect(me, side, width, false, &dx0, &dy0, &w, &h);
-                strip_rect(from, opposite, width, true, &sx0, &sy0, &sw, &sh);
+                int dx0 = 0, dy0 = 0, w = 0, h = 0, sx0 = 0, sy0 = 0, sw = 0, sh = 0;
+                if (!strip_rect(me, side, width, false, &dx0, &dy0, &w, &h) ||
+                    !strip_rect(from, opposite, width, true, &sx0, &sy0, &sw, &sh))
+                    return MHD_ERR_INVALID_ARGUMENT;
                 Planes dst, src;
                 const int np = set_planes(me, set, &dst);
                 set_planes(from, set, &src);
