@@ -598,29 +598,45 @@ def measure_snapshots(torch, m, ctx, steps=100, every=50):
 
 def measure_decomposed(torch, m, n=4096, P=2, Q=2, steps=3):
     """The domain decomposition on one GPU: Orszag-Tang n^2 split P x Q, subdomains exchanging
-    their rings by device copies (the ranks of a multi-GPU run emulated in one process),
-    against a single context on the same steps; wall time per step (the decomposed solve waits on
-    the host for every product's sums) and the largest per-field difference."""
+    their rings by device kernels (the ranks of a multi-GPU run emulated in one process),
+    against a single context on the same steps; wall time per step and the largest per-field
+    difference. Three forms of the solve: the single-sweep solver with its decisions on the device
+    (the default: each iteration one replayed CUDA graph, the host polling a control block one
+    iteration behind), the two-sweep solve with decisions on the device, and the same with every
+    product's sums read back by the host (these two must agree bit for bit)."""
     from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
                                                                 LocalTransport, Partition)
 
     dx = m.problems.grid_spacing(n)
     ic = m.problems.orszag_tang(n, n, dx, dx)
     part = Partition(n, n, P, Q)
-    subs = [GpuSubdomain(*part.shape(i), dx, dx, ETA) for i in range(part.count)]
-    run = DecomposedRun(part, LocalTransport(part, subs), dx, dx, ETA, courant=COURANT)
-    run.set_state(ic)
-    run.step()  # warm-up
-    start = run.get_state()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    dts, prods = [], []
-    for _ in range(steps):
-        dt, k = run.step()
-        dts.append(dt)
-        prods.append(k)
-    torch.cuda.synchronize()
-    dec = time.perf_counter() - t0
+    start, dts, runs = None, None, {}
+    forms = {"sweep_device": (True, "sweep"), "two_sweep_device": (True, "two_sweep"),
+             "two_sweep_host": (False, "two_sweep")}
+    for mode, (device, form) in forms.items():
+        subs = [GpuSubdomain(*part.shape(i), dx, dx, ETA) for i in range(part.count)]
+        run = DecomposedRun(part, LocalTransport(part, subs), dx, dx, ETA, courant=COURANT,
+                            device_decisions=device, cg_form=form)
+        run.set_state(ic)
+        run.step()  # warm-up
+        if start is None:
+            start = run.get_state()
+        else:
+            run.set_state(start)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        got_dts, prods = [], []
+        for k in range(steps):
+            dt, kk = run.step(0.0 if dts is None else dts[k])
+            got_dts.append(dt)
+            prods.append(kk)
+        torch.cuda.synchronize()
+        runs[mode] = dict(ms=1e3 * (time.perf_counter() - t0) / steps, prods=prods, state=run.get_state(),
+                          divb=run.divb()[1], status=run.status)
+        dts = dts or got_dts
+        run.close()
+        for sd in subs:
+            sd.close()
     ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
     ctx.set_state(start)
     ctx.step(dts[0])  # warm-up of the single context, then the same steps again from the start
@@ -631,18 +647,29 @@ def measure_decomposed(torch, m, n=4096, P=2, Q=2, steps=3):
         ctx.step(dt)
     ctx.synchronize()
     single = time.perf_counter() - t1
-    errs = [float(np.max(np.abs(g - w)) / max(float(np.max(np.abs(w))), 1.0))
-            for g, w in zip(run.get_state(), ctx.get_state())]
-    out = {"what": f"Orszag-Tang {n}x{n} split {P}x{Q} on one GPU (rings by device copies), "
+    want = ctx.get_state()
+
+    def err(mode):
+        return max(float(np.max(np.abs(g - w)) / max(float(np.max(np.abs(w))), 1.0))
+                   for g, w in zip(runs[mode]["state"], want))
+
+    a, b = runs["two_sweep_device"], runs["two_sweep_host"]
+    same = all(np.array_equal(x, y) for x, y in zip(a["state"], b["state"])) and a["prods"] == b["prods"]
+    out = {"what": f"Orszag-Tang {n}x{n} split {P}x{Q} on one GPU (rings by device kernels), "
                    f"{steps} CFL steps, against a single context stepped with the same dts",
-           "ms_per_step_decomposed": 1e3 * dec / steps,
+           "ms_per_step_decomposed": runs["sweep_device"]["ms"],
+           "ms_per_step_two_sweep_device_decisions": a["ms"],
+           "ms_per_step_two_sweep_host_decisions": b["ms"],
            "ms_per_step_single_context": 1e3 * single / steps,
-           "cg_products": prods, "max_rel_linf_vs_single": max(errs), "divb_max": run.divb()[1],
-           "status": run.status,
-           "note": "wall time; the decomposed solve reads each product's partial sums on the host"}
+           "cg_products": runs["sweep_device"]["prods"],
+           "max_rel_linf_vs_single": err("sweep_device"),
+           "max_rel_linf_vs_single_two_sweep": err("two_sweep_device"),
+           "two_sweep_device_and_host_decisions_bit_identical": bool(same),
+           "divb_max": runs["sweep_device"]["divb"], "status": runs["sweep_device"]["status"],
+           "note": "wall time; the default form: the single context's single-sweep solver on every "
+                   "subdomain, one CUDA graph per iteration, the host polling the solve's control "
+                   "block one iteration behind"}
     ctx.close()
-    for sd in subs:
-        sd.close()
     return out
 
 

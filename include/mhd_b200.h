@@ -343,7 +343,9 @@ enum {
     MHD_SUB_SET_PREDICTOR = 1,      /* U1* (6 planes) */
     MHD_SUB_SET_ACCUMULATOR_B = 2,  /* the face fields of U2* (2 planes) */
     MHD_SUB_SET_SOLUTION = 3,       /* the corner field of the last solve */
-    MHD_SUB_SET_DIRECTION = 4       /* the CG direction p */
+    MHD_SUB_SET_DIRECTION = 4,      /* the CG direction p */
+    MHD_SUB_SET_CG_EVEN = 5,        /* single-sweep solve: r_k and p_{k-1} before an even iteration */
+    MHD_SUB_SET_CG_ODD = 6          /* ... before an odd iteration */
 };
 typedef struct mhd_subdomain mhd_subdomain;
 int mhd_sub_halo(void);
@@ -388,6 +390,78 @@ mhd_status mhd_sub_cg_update(mhd_subdomain* s, double alpha, double out[2]);
 mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta);
 mhd_status mhd_sub_cg_zero_solution(mhd_subdomain* s);
 mhd_status mhd_sub_sums(mhd_subdomain* s, double* out, int n);
+/* Decisions of the decomposed solve on the device. A group (mhd_subcg) holds a control block of
+ * MHD_SUBCG_CTL doubles and count sum slots of 4 doubles, in device memory. The *_dev phases write
+ * their subdomain's sums into its slot (mhd_subcg_slots(g) + 4 index; across ranks the slots are
+ * all-gathered into the group's array) and read alpha, beta and "still iterating" from the control
+ * block, doing nothing once the solve has ended; mhd_subcg_decide (phase 0 after cg_rhs_dev, 1
+ * after cg_matvec_dev, 2 after cg_update_dev) adds the slots in subdomain order and takes the
+ * decisions of the host driver, with the same arithmetic: the results are bit-identical. The
+ * subdomains and the group's stream must be ordered by the caller (one shared stream in one
+ * process). mhd_subcg_post(g, tag) enqueues a copy of the control block to pinned memory and
+ * mhd_subcg_read(g, tag, out) waits for it (two copies in flight: tags of one parity share one).
+ * cg_finish_dev zeroes x after a solve that met a non-finite value (as cg_zero_solution).
+ * mhd_subcg_decide_host applies the same rules to host arrays (no device needed). Phases 3 and 4
+ * are those of the single-sweep form below. */
+#define MHD_SUBCG_CTL 16
+enum {
+    MHD_SUBCG_ACTIVE = 0,     /* 1.0 while the solve iterates */
+    MHD_SUBCG_STATUS = 1,     /* MHD_SUBCG_OK / _NOT_CONVERGED / _NONFINITE */
+    MHD_SUBCG_PRODUCTS = 2,   /* matrix products so far */
+    MHD_SUBCG_BB = 3,         /* |b|^2 */
+    MHD_SUBCG_THRESHOLD = 4,  /* max(tol^2 |b|^2, DBL_MIN) */
+    MHD_SUBCG_ABSNEW = 5,     /* r.z */
+    MHD_SUBCG_ALPHA = 6,
+    MHD_SUBCG_BETA = 7,
+    MHD_SUBCG_RR = 8,         /* |r|^2 after the last update */
+    MHD_SUBCG_PQ = 9,         /* p.q of the last product (single-sweep form: p.Ap of the next) */
+    MHD_SUBCG_ALPHA_PREV = 10, /* single-sweep form: alpha of the previous iteration */
+    MHD_SUBCG_K_LAST = 11,    /* single-sweep form: the last iteration swept (-1: none) */
+    MHD_SUBCG_ALPHA_LAST = 12, /* single-sweep form: its alpha */
+    MHD_SUBCG_ZERO = 13       /* single-sweep form: 1 when the solution is x = 0 */
+};
+enum { MHD_SUBCG_OK = 0, MHD_SUBCG_NOT_CONVERGED = 1, MHD_SUBCG_NONFINITE = 2 };
+typedef struct mhd_subcg mhd_subcg;
+mhd_status mhd_sub_cg_rhs_dev(mhd_subdomain* s, int solve_index, double* slot);
+mhd_status mhd_sub_cg_matvec_dev(mhd_subdomain* s, const double* ctl, double* slot);
+mhd_status mhd_sub_cg_update_dev(mhd_subdomain* s, const double* ctl, double* slot);
+mhd_status mhd_sub_cg_direction_dev(mhd_subdomain* s, const double* ctl);
+mhd_status mhd_sub_cg_finish_dev(mhd_subdomain* s, const double* ctl);
+/* count: subdomains of the solve; stream: a cudaStream_t, or NULL for a stream of the group's own;
+ * slots: count x 4 doubles of device memory that the caller owns, or NULL (the group allocates). */
+mhd_status mhd_subcg_create(int count, void* stream, double* slots, mhd_subcg** out);
+mhd_status mhd_subcg_destroy(mhd_subcg* g);
+double* mhd_subcg_slots(mhd_subcg* g);
+const double* mhd_subcg_control(mhd_subcg* g);
+mhd_status mhd_subcg_decide(mhd_subcg* g, int phase, double tol, long long max_products);
+mhd_status mhd_subcg_post(mhd_subcg* g, int tag);
+mhd_status mhd_subcg_read(mhd_subcg* g, int tag, double* out);
+mhd_status mhd_subcg_decide_host(double* ctl, const double* slots, int count, int phase, double tol,
+                                 long long max_products);
+/* For subdomains of this process on their own streams (subs[i] writes slot i): decide_on orders the
+ * decision after every subdomain's work so far and their later work after it (events);
+ * mhd_subcg_product enqueues one whole product of the solve -- the exchange of p's 1-cell ring
+ * (mhd_sub_exchange_local), cg_matvec_dev, decision 1, cg_update_dev, decision 2,
+ * cg_direction_dev on all P x Q subdomains -- as one CUDA graph on the group's stream, captured at
+ * the first call for these arguments and replayed after, then posts the control block under `tag`. */
+mhd_status mhd_subcg_decide_on(mhd_subcg* g, mhd_subdomain* const* subs, int phase, double tol,
+                               long long max_products);
+mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                             long long max_products, int tag);
+/* The single-sweep form of the decomposed solve: the single context's solver (one sweep per
+ * product forming q = A p, r, z and the sums r.r, r.z, z.Az, z.q, with p.Ap carried by a
+ * recurrence, and the solution moved every second iteration) on each subdomain's interior.
+ * cg_sweep_rhs_dev: b = eta J_z(B*), r0 = b, slot = |b|^2, b.z0, z0.A z0 (then decision phase 3;
+ * the predictor's or accumulator's rings must hold 2 cells). Iteration k: exchange
+ * MHD_SUB_SET_CG_EVEN / _ODD (k even / odd) with a ring of 2, cg_sweep_iter_dev, decision phase 4.
+ * mhd_subcg_sweep_product enqueues that iteration as a replayed graph (one per parity) and posts
+ * the control block under `tag`. cg_sweep_finish_dev ends the solve (x = 0 after a zero right-hand
+ * side or a breakdown, the last alpha_k p_k after an even last iteration). */
+mhd_status mhd_sub_cg_sweep_rhs_dev(mhd_subdomain* s, int solve_index, double* slot);
+mhd_status mhd_sub_cg_sweep_iter_dev(mhd_subdomain* s, const double* ctl, double* slot);
+mhd_status mhd_sub_cg_sweep_finish_dev(mhd_subdomain* s, const double* ctl);
+mhd_status mhd_subcg_sweep_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                                   long long max_products, int k, int tag);
 /* Interior div B partials (diagnostics.hpp:15-42): out[0] = sum of div^2, out[1] = max |div|. */
 mhd_status mhd_sub_divb_sums(mhd_subdomain* s, double out[2]);
 mhd_status mhd_sub_synchronize(mhd_subdomain* s);

@@ -195,10 +195,6 @@ k_finalize_batch(const BatchInst* __restrict__ insts, const SweepItem* __restric
 // is active.
 
 constexpr int CGB_MAX_INST = 64;
-// 1: in the tile order a warp prefetches its next tile's first rows while it ends the current one
-#ifndef MHD_CGB_CARRY
-#define MHD_CGB_CARRY 1
-#endif
 // Threads per block of the batched solver (its own size: the per-warp partial sums of 64 instances
 // live in dynamic shared memory beside the rows' rings).
 #ifndef MHD_CGB_NT
@@ -334,8 +330,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         for (int c = 0; c < NV; ++c) wsum[wid][li][c] = 0.0;
     __syncwarp();
     const bool odd = (k & 1) != 0;
-    // one segment; tb, pre, nxt: the ring carry of cg_iter_segment
-    auto run = [&](int li, int sx, int r0, int r1, int tb, bool pre, const CgNext* nxt) {
+    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const CgSweepArgs g = cgb_args(a, I);
         CgScal s;
@@ -354,8 +349,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
             double* rk1 = odd ? g.r[0] : g.r[1];
             const double* pkm1 = odd ? g.p[0] : g.p[1];
             double* pk = odd ? g.p[1] : g.p[0];
-            cg_iter_segment<PH == 1, XM>(g, s, sx, r0, r1, dir, rk, pkm1, rk1, pk, ring, acc, tb, pre,
-                                         nxt);
+            cg_iter_segment<PH == 1, XM>(g, s, sx, r0, r1, dir, rk, pkm1, rk1, pk, ring, acc);
         }
 #pragma unroll
         for (int c = 0; c < NV; ++c)
@@ -365,53 +359,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
             for (int c = 0; c < NV; ++c) wsum[wid][li][c] += acc[c];
         }
         __syncwarp();
-    };
-#if MHD_CGB_CARRY
-    if (PH != 0 && a.order != 0) {
-        // tiles g, g + W, ...: each tile prefetches the first rows of the next one while it ends,
-        // when the next is of the same instance and has at least CG_RING - 2 sweep rows (so that
-        // all its prefetched rows are its own and its prefetch of the one after starts where the
-        // ring expects it)
-        const long long nw = (long long)gridDim.x * NW;
-        const long long T = pref[a.ninst];
-        long long j = (long long)blockIdx.x * NW + wid;
-        int li = 0;
-        if (j < T) while (pref[li + 1] <= j) ++li;
-        int tb = 0;
-        bool pre = false;
-        while (j < T) {
-            const int w = (int)(j - pref[li]);
-            const int sx = w % sh[li].strips;
-            const int r0 = (w / sh[li].strips) * a.rows;
-            const int r1 = min(r0 + a.rows, sh[li].ny);
-            const long long j2 = j + nw;
-            int li2 = li;
-            CgNext nx;
-            bool carry = false;
-            if (j2 < T) {
-                while (pref[li2 + 1] <= j2) ++li2;
-                const int w2 = (int)(j2 - pref[li2]);
-                const int sx2 = w2 % sh[li2].strips;
-                const int r02 = (w2 / sh[li2].strips) * a.rows;
-                const int r12 = min(r02 + a.rows, sh[li2].ny);
-                nx.total = (r12 - r02) + 4;
-                carry = li2 == li && nx.total >= CG_RING - 2;
-                if (carry) {
-                    nx.iw = wrap(sx2 * CG_W - CG_HALO + lane, a.insts[a.inst0 + li].D.nx);
-                    nx.jfirst = (dir > 0) ? r02 : r12 - 1;
-                }
-            }
-            run(li, sx, r0, r1, tb, pre, carry ? &nx : nullptr);
-            tb += (r1 - r0) + 4;
-            pre = carry;
-            j = j2;
-            li = li2;
-        }
-    } else
-#endif
-    {
-        cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) { run(li, sx, r0, r1, 0, false, nullptr); });
-    }
+    });
     __syncthreads();
     for (int q = threadIdx.x; q < a.ninst * NV; q += CGB_NT) {
         const int li = q / NV, c = q - li * NV;

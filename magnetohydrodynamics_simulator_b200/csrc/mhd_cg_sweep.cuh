@@ -54,6 +54,9 @@ struct CgSweepArgs {
     long long max_iters;
     double tol;
     double timeout_s;
+    // a subdomain's interior inside extended planes (the kSub forms of the segment sweeps): strips
+    // start at column col0, and columns from col_end on are not owned
+    int col0, col_end;
 };
 
 struct CgScal {
@@ -111,15 +114,16 @@ constexpr size_t kCgRingBytes = (size_t)(CGS_NT / 32) * CG_RING * CG_SLOT * size
 // r0), p0 = z0 = b/d, partials |b|^2, b.z0, p0.A p0 (acc[0..2]). Lane l holds corner column
 // c0 - 2 + l; lanes 2..29 own the results. Sweep row k (k = 0 is the row behind the first one) sits
 // in slot k % CG_RING.
+template <bool kSub = false>
 __device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
                                                int r1w, int dir, double* r0, double* ring,
                                                double (&acc)[4]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
-    const int c0 = sx * CG_W;
+    const int c0 = (kSub ? a.col0 : 0) + sx * CG_W;
     if (r0w >= r1w) return;
     const int i = c0 - CG_HALO + lane;
-    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
+    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < (kSub ? a.col_end : nx);
     const int iw = wrap(i, nx);
     const double idx = 1.0 / a.D.dx, idy = 1.0 / a.D.dy;
     const int jfirst = (dir > 0) ? r0w : r1w - 1;
@@ -183,37 +187,26 @@ __device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgSca
     cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
-// The segment a warp sweeps after the current one, in the same vectors, whose first rows the
-// current one prefetches into its ring while it ends (a warp that sweeps several segments of a
-// phase keeps its ring busy across them): its column (this lane's), first row and sweep rows.
-struct CgNext {
-    int iw, jfirst, total;
-};
-
 // One CG iteration k over rows [r0w, r1w) of column strip sx (the sweep of the header comment).
 // FIRST: k = 0, p_0 = z_0 (p_{-1} is not read). XM: the iteration's CgXMode. acc[0..3] receive r.r, r.z, z.Az, z.q_k of
 // the owned cells. Sweep row t holds grid row jfirst + (t - 2) dir, t = 0 .. nrows + 3; at sweep
 // row t the warp forms p_k of row t, q_k, r_{k+1}, z_{k+1} of row t-1 and A z_{k+1} and the outputs
 // of row t-2. Row t is copied into slot t % CG_RING by the end of sweep row t - 6.
-// tb: ring index of the segment's sweep row 0 (the ring numbering runs on across a warp's
-// segments); pre: its first CG_RING - 2 rows were issued by the previous segment; nxt (may be
-// null): the segment to prefetch in place of the rows past this one's end.
-template <bool FIRST, int XM>
+template <bool FIRST, int XM, bool kSub = false>
 __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
                                                 int r1w, int dir, const double* rk, const double* pkm1,
                                                 double* rk1, double* pk, double* ring,
-                                                double (&acc)[4], int tb = 0, bool pre = false,
-                                                const CgNext* nxt = nullptr) {
+                                                double (&acc)[4]) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
-    const int c0 = sx * CG_W;
+    const int c0 = (kSub ? a.col0 : 0) + sx * CG_W;
     if (r0w >= r1w) return;
     const int i = c0 - CG_HALO + lane;
-    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < nx;
+    const bool owner = lane >= CG_HALO && lane < CG_HALO + CG_W && i < (kSub ? a.col_end : nx);
     const int iw = wrap(i, nx);
     const int jfirst = (dir > 0) ? r0w : r1w - 1;
     const int total = (r1w - r0w) + 4;
-    auto slot = [&](int t) { return ring + (unsigned)((tb + t) & (CG_RING - 1)) * CG_SLOT; };
+    auto slot = [&](int t) { return ring + (unsigned)(t & (CG_RING - 1)) * CG_SLOT; };
     auto issue = [&](int t) {
         if (t < total) {
             double* sl = slot(t);
@@ -221,20 +214,11 @@ __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgSc
             cp_async8(&sl[lane], &rk[rp]);
             if constexpr (!FIRST) cp_async8(&sl[32 + lane], &pkm1[rp]);
             if constexpr (XM == kXPair) cp_async8(&sl[64 + lane], &a.x[rp]);
-        } else if (nxt != nullptr && t - total < nxt->total) {
-            // the next segment's sweep row t - total, into the slot it will read it from
-            double* sl = slot(t);
-            const size_t rp = (size_t)wrap(nxt->jfirst + (t - total - 2) * dir, ny) * nx + nxt->iw;
-            cp_async8(&sl[lane], &rk[rp]);
-            if constexpr (!FIRST) cp_async8(&sl[32 + lane], &pkm1[rp]);
-            if constexpr (XM == kXPair) cp_async8(&sl[64 + lane], &a.x[rp]);
         }
         cp_async_commit();
     };
-    if (!pre) {
 #pragma unroll
-        for (int t = 0; t < CG_RING - 2; ++t) issue(t);
-    }
+    for (int t = 0; t < CG_RING - 2; ++t) issue(t);
     double p_a = 0.0, p_b = 0.0;       // p_k of rows t-2, t-1
     double q_o = 0.0;                  // q_k of row t-2
     double r_o = 0.0, z_o = 0.0;       // r_{k+1}, z_{k+1} of row t-2
@@ -288,7 +272,7 @@ __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgSc
         r_o = r_b; z_o = z_b;
         issue(t + CG_RING - 2);  // into the slot of row t-2, no longer read
     }
-    if (nxt == nullptr) cp_async_wait<0>();  // leave no copy in flight into the ring
+    cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
 // Block-reduce NV partial sums (fixed order) and publish them in this block's slot.

@@ -18,12 +18,20 @@
 // Jacobi scaling, stop at |r|^2 < max(tol^2 |b|^2, DBL_MIN)), exchanging p's 1-cell ring before
 // every product. The CFL speed and the div B sums are interior scans whose maxima and sums the
 // driver combines the same way.
+//
+// The decisions can also stay on the device (mhd_subcg_*): the phases write their subdomain's sums
+// into a slot of a group's array, a one-thread kernel adds the slots in subdomain order and takes
+// the same decisions into a control block, and the later phases read alpha, beta and "still
+// iterating" from it, doing nothing once the solve has ended. The host then only polls the control
+// block, a product behind, instead of waiting for the sums of every phase.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/mhd_b200.h"
 #include "mhd_cg_sweep.cuh"
@@ -40,6 +48,8 @@ constexpr int kH = MHD_SUB_HALO;
 constexpr int kSubNT = 256;
 constexpr int kSubPlanes = 6 + 6 + 6 + 5;  // S, T, A, x r p q z
 constexpr int kSubMaxBlocks = 1024;
+constexpr int kSubCgNT = 256;  // threads of the single-sweep solve's blocks (8 warps, one ring each)
+constexpr size_t kSubCgRingBytes = (size_t)(kSubCgNT / 32) * CG_RING * CG_SLOT * sizeof(double);
 
 // Interior view of an extended plane: element (i, j) of the interior at base[(j + H) * nxe + i + H].
 struct Interior {
@@ -62,22 +72,33 @@ struct SubScal {
     double cx, cy, diag, invdiag;
 };
 
-// Sum block partials (K per block) in block order into out[K] (one warp).
+// Sum block partials (K per block) into out[K] with one warp, in a fixed order: lane l adds blocks
+// l, l + 32, ... in turn, then the lanes' sums meet in a butterfly (the same order on every run; a
+// single thread walking the blocks in turn took 25-48 us at 592 blocks, bound by load latency).
 template <int K>
 __global__ void k_sub_final(const double* __restrict__ part, int nblocks, double* out) {
-    if (threadIdx.x != 0) return;
+    const int l = threadIdx.x;
     double s[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) s[k] = 0.0;
-    for (int b = 0; b < nblocks; ++b) {
+    for (int b = l; b < nblocks; b += 32) {
 #pragma unroll
         for (int k = 0; k < K; ++k) s[k] += part[(size_t)b * K + k];
     }
 #pragma unroll
-    for (int k = 0; k < K; ++k) out[k] = s[k];
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] = s[k];
+    }
 }
 
-__global__ void k_sub_set_coeffs(StepCoeffs* C, double dt, double alpha, double g, double d) {
+// The step's coefficients and the implicit matrix (I - alpha L) of the solves: off-diagonal
+// cx = alpha/dx^2, cy = alpha/dy^2, diagonal 1 + 2 (cx + cy) (solvers.hpp:404-443), on the device
+// so that a captured solve reads this step's matrix.
+__global__ void k_sub_set_coeffs(StepCoeffs* C, SubScal* sc, double dt, double alpha, double g, double d,
+                                 double dx, double dy) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     C->dt = dt;
     C->c_g = dt * g;
@@ -85,6 +106,12 @@ __global__ void k_sub_set_coeffs(StepCoeffs* C, double dt, double alpha, double 
     C->c_1md = dt * (1.0 - d);
     C->c_1mg = dt * (1.0 - g);
     C->alpha = alpha;
+    const double cx = alpha / (dx * dx), cy = alpha / (dy * dy);
+    const double diag = 1.0 + 2.0 * (cx + cy);
+    sc->cx = cx;
+    sc->cy = cy;
+    sc->diag = diag;
+    sc->invdiag = (diag == 0.0) ? 1.0 : 1.0 / diag;
 }
 
 // Copy the rectangle [x0, x0 + w) x [y0, y0 + h) of np extended planes (row pitch nxe) into buf
@@ -108,11 +135,49 @@ k_sub_strip(Planes set, int np, int nxe, int x0, int y0, int w, int h, double* b
     }
 }
 
+// The ring of one subdomain (cells within `width` of its interior), gathered from the interiors of
+// the 3 x 3 subdomains around it (src[a][b]: the one dy = a - 1, dx = b - 1 away, periodic; itself
+// at [1][1] when the partition has one subdomain along an axis). A ring cell west of the interior
+// lies in the west neighbour's last columns, a corner cell in the diagonal neighbour's corner.
+struct RingSources {
+    const double* f[3][3][6];
+    int nxe[3][3];
+    int nx_w, ny_s;  // interior columns of the west neighbours, rows of the south neighbours
+};
+
+__global__ void __launch_bounds__(kSubNT)
+k_sub_ring_gather(Planes dst, int np, Interior v, int width, RingSources src) {
+    const int w = width, rowlen = v.nx + 2 * w;
+    const size_t band = (size_t)w * rowlen;         // cells of the south (or north) band
+    const size_t total = 2 * band + (size_t)2 * w * v.ny;
+    for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < total; t += (size_t)gridDim.x * kSubNT) {
+        int ii, jj;  // interior coordinates of the ring cell, in [-w, n + w)
+        if (t < 2 * band) {
+            const int r = (int)(t / rowlen);
+            ii = (int)(t - (size_t)r * rowlen) - w;
+            jj = (r < w) ? r - w : v.ny + (r - w);
+        } else {
+            const size_t u = t - 2 * band;
+            const int r = (int)(u / (2 * w)), c = (int)(u - (size_t)r * 2 * w);
+            jj = r;
+            ii = (c < w) ? c - w : v.nx + (c - w);
+        }
+        const int b = (ii < 0) ? 0 : (ii >= v.nx ? 2 : 1);
+        const int a = (jj < 0) ? 0 : (jj >= v.ny ? 2 : 1);
+        const int si = (b == 0) ? src.nx_w + ii : (b == 2 ? ii - v.nx : ii);  // the source's interior column
+        const int sj = (a == 0) ? src.ny_s + jj : (a == 2 ? jj - v.ny : jj);
+        const size_t gs = (size_t)(sj + kH) * src.nxe[a][b] + (si + kH);
+        const size_t gd = at(v, ii, jj);
+        for (int k = 0; k < np; ++k) dst.f[k][gd] = src.f[a][b][k][gs];
+    }
+}
+
 // b = eta J_z(B*) on the interior corners (solvers.hpp:450-461), r = b, z = p = b/d, x = 0;
 // block partials |b|^2, r.z.
 __global__ void __launch_bounds__(kSubNT)
 k_sub_cg_rhs(Interior v, double eta, double idx, double idy, const double* __restrict__ bxf,
-             const double* __restrict__ byf, SubVecs V, SubScal s, double* part) {
+             const double* __restrict__ byf, SubVecs V, const SubScal* __restrict__ sp, double* part) {
+    const SubScal s = *sp;
     __shared__ double red[kSubNT / 32 * 2];
     double acc[2] = {0.0, 0.0};
     const size_t n = (size_t)v.nx * v.ny;
@@ -139,8 +204,10 @@ k_sub_cg_rhs(Interior v, double eta, double idx, double idy, const double* __res
 // q = A p = (I - alpha L) p on the interior corners (p's 1-cell ring must hold the neighbours'
 // values), in the single context's operand order; block partial p.q.
 __global__ void __launch_bounds__(kSubNT)
-k_sub_cg_matvec(Interior v, SubVecs V, SubScal s, double* part) {
+k_sub_cg_matvec(Interior v, SubVecs V, const SubScal* __restrict__ sp, const double* ctl, double* part) {
+    const SubScal s = *sp;
     __shared__ double red[kSubNT / 32];
+    if (ctl && ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
     double acc[1] = {0.0};
     const size_t n = (size_t)v.nx * v.ny;
     for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < n; t += (size_t)gridDim.x * kSubNT) {
@@ -161,8 +228,14 @@ k_sub_cg_matvec(Interior v, SubVecs V, SubScal s, double* part) {
 
 // x += alpha p, r -= alpha q, z = r/d on the interior; block partials |r|^2, r.z.
 __global__ void __launch_bounds__(kSubNT)
-k_sub_cg_update(Interior v, SubVecs V, SubScal s, double alpha, double* part) {
+k_sub_cg_update(Interior v, SubVecs V, const SubScal* __restrict__ sp, double alpha, const double* ctl,
+                double* part) {
+    const SubScal s = *sp;
     __shared__ double red[kSubNT / 32 * 2];
+    if (ctl) {
+        if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
+        alpha = ctl[MHD_SUBCG_ALPHA];
+    }
     double acc[2] = {0.0, 0.0};
     const size_t n = (size_t)v.nx * v.ny;
     for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < n; t += (size_t)gridDim.x * kSubNT) {
@@ -184,7 +257,11 @@ k_sub_cg_update(Interior v, SubVecs V, SubScal s, double alpha, double* part) {
 }
 
 // p = z + beta p on the interior.
-__global__ void __launch_bounds__(kSubNT) k_sub_cg_dir(Interior v, SubVecs V, double beta) {
+__global__ void __launch_bounds__(kSubNT) k_sub_cg_dir(Interior v, SubVecs V, double beta, const double* ctl) {
+    if (ctl) {
+        if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
+        beta = ctl[MHD_SUBCG_BETA];
+    }
     const size_t n = (size_t)v.nx * v.ny;
     for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < n; t += (size_t)gridDim.x * kSubNT) {
         const int j = (int)(t / v.nx), i = (int)(t - (size_t)j * v.nx);
@@ -193,12 +270,232 @@ __global__ void __launch_bounds__(kSubNT) k_sub_cg_dir(Interior v, SubVecs V, do
     }
 }
 
-__global__ void __launch_bounds__(kSubNT) k_sub_zero_interior(Interior v, double* x) {
+// x = 0 on the interior (with a control block: only after a solve that met a non-finite value)
+__global__ void __launch_bounds__(kSubNT) k_sub_zero_interior(Interior v, double* x, const double* ctl) {
+    if (ctl && ctl[MHD_SUBCG_STATUS] != (double)MHD_SUBCG_NONFINITE) return;
     const size_t n = (size_t)v.nx * v.ny;
     for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < n; t += (size_t)gridDim.x * kSubNT) {
         const int j = (int)(t / v.nx), i = (int)(t - (size_t)j * v.nx);
         x[at(v, i, j)] = 0.0;
     }
+}
+
+// ---- the single-sweep form of the solve: the single context's sweeps (cg_rhs_segment,
+// cg_iter_segment) over the interior of the extended planes. An interior corner's results need the
+// rows and columns within 2 of it, so r_k and p_{k-1} are exchanged with a ring of 2 before each
+// iteration (the set MHD_SUB_SET_CG_EVEN / _ODD); their wrapped ring values are never used.
+// Vectors: r[0] = r, r[1] = z, p[0] = p, p[1] = q of the subdomain.
+
+__device__ __forceinline__ CgScal sub_cg_scal(const SubScal* sp) {
+    CgScal s;
+    s.cx = sp->cx;
+    s.cy = sp->cy;
+    s.diag = sp->diag;
+    s.invdiag = sp->invdiag;
+    s.beta = 0.0;
+    s.alpha = 0.0;
+    s.alpha_prev = 0.0;
+    return s;
+}
+
+// b = eta J_z(B*), r0 = b on the interior; block partials |b|^2, b.z0, z0.A z0.
+__global__ void __launch_bounds__(kSubCgNT, 2)
+k_sub_cg_sweep_rhs(CgSweepArgs a, const SubScal* __restrict__ sp, double* part) {
+    extern __shared__ __align__(16) double sub_ring_mem[];
+    __shared__ double red[kSubCgNT / 32 * 4];
+    double* const ring = sub_ring_mem + (size_t)(threadIdx.x >> 5) * CG_RING * CG_SLOT;
+    const CgScal s = sub_cg_scal(sp);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int rend = a.D.ny - kH;
+    for (int w = blockIdx.x * (kSubCgNT / 32) + (threadIdx.x >> 5); w < a.nwarps; w += gridDim.x * (kSubCgNT / 32)) {
+        const int sx = w % a.strips_x, r0w = kH + (w / a.strips_x) * a.seg_h;
+        cg_rhs_segment<true>(a, s, sx, r0w, min(r0w + a.seg_h, rend), 1, a.r[0], ring, acc);
+    }
+    block_sum<kSubCgNT, 4>(acc, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) part[(size_t)blockIdx.x * 4 + c] = acc[c];
+    }
+}
+
+// Iteration k = products so far (from the control block, which also gives alpha, beta and
+// alpha_{k-1}); nothing once the solve has ended. Block partials r.r, r.z, z.Az, z.q_k.
+__global__ void __launch_bounds__(kSubCgNT, 2)
+k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double* ctl, double* part) {
+    if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
+    extern __shared__ __align__(16) double sub_ring_mem[];
+    __shared__ double red[kSubCgNT / 32 * 4];
+    double* const ring = sub_ring_mem + (size_t)(threadIdx.x >> 5) * CG_RING * CG_SLOT;
+    CgScal s = sub_cg_scal(sp);
+    s.alpha = ctl[MHD_SUBCG_ALPHA];
+    s.beta = ctl[MHD_SUBCG_BETA];
+    s.alpha_prev = ctl[MHD_SUBCG_ALPHA_PREV];
+    const long long k = (long long)ctl[MHD_SUBCG_PRODUCTS];
+    const bool odd = (k & 1) != 0;
+    const double* rk = odd ? a.r[1] : a.r[0];
+    double* rk1 = odd ? a.r[0] : a.r[1];
+    const double* pkm1 = odd ? a.p[0] : a.p[1];
+    double* pk = odd ? a.p[1] : a.p[0];
+    const int dir = odd ? 1 : -1;  // alternate (the right-hand side runs upwards)
+    const int xm = cg_xmode(k);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int rend = a.D.ny - kH;
+    for (int w = blockIdx.x * (kSubCgNT / 32) + (threadIdx.x >> 5); w < a.nwarps; w += gridDim.x * (kSubCgNT / 32)) {
+        const int sx = w % a.strips_x, r0w = kH + (w / a.strips_x) * a.seg_h;
+        const int r1w = min(r0w + a.seg_h, rend);
+        if (k == 0)
+            cg_iter_segment<true, kXSkip, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+        else if (xm == kXSkip)
+            cg_iter_segment<false, kXSkip, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+        else if (xm == kXPairFirst)
+            cg_iter_segment<false, kXPairFirst, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+        else
+            cg_iter_segment<false, kXPair, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+    }
+    block_sum<kSubCgNT, 4>(acc, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) part[(size_t)blockIdx.x * 4 + c] = acc[c];
+    }
+}
+
+// The end of a single-sweep solve (as k_cg_sweep's): x = 0 after a zero right-hand side or a
+// breakdown; after an even last iteration k, its alpha_k p_k (x_0 = 0 when k = 0).
+__global__ void __launch_bounds__(kSubNT)
+k_sub_cg_sweep_finish(Interior v, double* x, const double* p0, const double* ctl) {
+    const bool zero = ctl[MHD_SUBCG_ZERO] != 0.0;
+    const long long kl = (long long)ctl[MHD_SUBCG_K_LAST];
+    const double al = ctl[MHD_SUBCG_ALPHA_LAST];
+    const bool fix = !zero && kl >= 0 && (kl & 1) == 0;  // the last iteration wrote p_k into p[0]
+    if (!zero && !fix) return;
+    const size_t n = (size_t)v.nx * v.ny;
+    for (size_t t = (size_t)blockIdx.x * kSubNT + threadIdx.x; t < n; t += (size_t)gridDim.x * kSubNT) {
+        const int j = (int)(t / v.nx), i = (int)(t - (size_t)j * v.nx);
+        const size_t g = at(v, i, j);
+        x[g] = zero ? 0.0 : (kl == 0 ? al * p0[g] : fma(al, p0[g], x[g]));
+    }
+}
+
+// The decisions of a decomposed solve after one of its phases (phase 0 right-hand side, 1 q = A p,
+// 2 the x/r/z update; the single-sweep form: 3 right-hand side, 4 an iteration), from the count
+// subdomains' sums (slots[4 i + k], added in subdomain order
+// from 0.0, as the host driver adds them) into the control block: Eigen's ConjugateGradient rules
+// (x0 = 0; stop when |r|^2 < max(tol^2 |b|^2, DBL_MIN); at most max_products products), the
+// single-context solver's (solvers.hpp:445-489).
+__host__ __device__ inline void subcg_decide(double* ctl, const double* slots, int count, int phase,
+                                             double tol, double max_products) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = 0; i < count; ++i) {
+        s0 += slots[4 * i];
+        s1 += slots[4 * i + 1];
+    }
+    if (phase == 0) {
+        ctl[MHD_SUBCG_PRODUCTS] = 0.0;
+        ctl[MHD_SUBCG_BB] = s0;
+        ctl[MHD_SUBCG_ABSNEW] = s1;
+        const double thr = tol * tol * s0;
+        ctl[MHD_SUBCG_THRESHOLD] = thr > DBL_MIN ? thr : DBL_MIN;
+        ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_OK;
+        if (!isfinite(s0)) {
+            ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NONFINITE;
+            ctl[MHD_SUBCG_ACTIVE] = 0.0;
+        } else {
+            // a zero (or negligible) right-hand side: x = 0, no product
+            ctl[MHD_SUBCG_ACTIVE] = (s0 == 0.0 || s0 < ctl[MHD_SUBCG_THRESHOLD]) ? 0.0 : 1.0;
+        }
+        return;
+    }
+    if (phase == 3) {
+        // the single-sweep form (the single context's k_cg_sweep): |b|^2, b.z0, z0.A z0
+        double s2 = 0.0;
+        for (int i = 0; i < count; ++i) s2 += slots[4 * i + 2];
+        ctl[MHD_SUBCG_PRODUCTS] = 0.0;
+        ctl[MHD_SUBCG_BB] = s0;
+        ctl[MHD_SUBCG_ABSNEW] = s1;
+        ctl[MHD_SUBCG_PQ] = s2;
+        const double thr = tol * tol * s0;
+        ctl[MHD_SUBCG_THRESHOLD] = thr > DBL_MIN ? thr : DBL_MIN;
+        ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_OK;
+        ctl[MHD_SUBCG_BETA] = 0.0;
+        ctl[MHD_SUBCG_ALPHA_PREV] = 0.0;
+        ctl[MHD_SUBCG_K_LAST] = -1.0;
+        ctl[MHD_SUBCG_ALPHA_LAST] = 0.0;
+        const bool zero = (s0 == 0.0) || (s0 < ctl[MHD_SUBCG_THRESHOLD]);
+        const bool breakdown = !isfinite(s0);
+        if (breakdown) ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NONFINITE;
+        ctl[MHD_SUBCG_ZERO] = (zero || breakdown) ? 1.0 : 0.0;
+        ctl[MHD_SUBCG_ACTIVE] = (zero || breakdown) ? 0.0 : 1.0;
+        if (!(zero || breakdown)) ctl[MHD_SUBCG_ALPHA] = s1 / s2;
+        return;
+    }
+    if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
+    if (phase == 4) {
+        // after iteration k of the single-sweep form: r.r, r.z, z.Az, z.q_k
+        double s2 = 0.0, s3 = 0.0;
+        for (int i = 0; i < count; ++i) {
+            s2 += slots[4 * i + 2];
+            s3 += slots[4 * i + 3];
+        }
+        const double k = ctl[MHD_SUBCG_PRODUCTS];
+        ctl[MHD_SUBCG_K_LAST] = k;
+        ctl[MHD_SUBCG_ALPHA_LAST] = ctl[MHD_SUBCG_ALPHA];
+        ctl[MHD_SUBCG_PRODUCTS] = k + 1.0;
+        ctl[MHD_SUBCG_RR] = s0;
+        if (!isfinite(s0) || !isfinite(ctl[MHD_SUBCG_ALPHA])) {
+            ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NONFINITE;
+            ctl[MHD_SUBCG_ZERO] = 1.0;
+            ctl[MHD_SUBCG_ACTIVE] = 0.0;
+            return;
+        }
+        if (s0 < ctl[MHD_SUBCG_THRESHOLD]) {
+            ctl[MHD_SUBCG_ACTIVE] = 0.0;
+            return;
+        }
+        // beta = r.z / r.z_old; p.Ap = z.Az + 2 beta z.q + beta^2 p.Ap (the previous p.Ap)
+        const double abs_old = ctl[MHD_SUBCG_ABSNEW];
+        ctl[MHD_SUBCG_ABSNEW] = s1;
+        const double beta = s1 / abs_old;
+        const double pap = s2 + 2.0 * beta * s3 + beta * beta * ctl[MHD_SUBCG_PQ];
+        ctl[MHD_SUBCG_BETA] = beta;
+        ctl[MHD_SUBCG_PQ] = pap;
+        if (!(pap > 0.0)) {
+            ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NONFINITE;
+            ctl[MHD_SUBCG_ZERO] = 1.0;
+            ctl[MHD_SUBCG_ACTIVE] = 0.0;
+            return;
+        }
+        ctl[MHD_SUBCG_ALPHA_PREV] = ctl[MHD_SUBCG_ALPHA];
+        ctl[MHD_SUBCG_ALPHA] = s1 / pap;
+        if (ctl[MHD_SUBCG_PRODUCTS] >= max_products) {
+            ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NOT_CONVERGED;
+            ctl[MHD_SUBCG_ACTIVE] = 0.0;
+        }
+        return;
+    }
+    if (phase == 1) {
+        ctl[MHD_SUBCG_PQ] = s0;
+        ctl[MHD_SUBCG_ALPHA] = ctl[MHD_SUBCG_ABSNEW] / s0;
+        return;
+    }
+    ctl[MHD_SUBCG_RR] = s0;
+    ctl[MHD_SUBCG_PRODUCTS] += 1.0;
+    if (!(isfinite(s0) && isfinite(ctl[MHD_SUBCG_ALPHA]))) {
+        ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NONFINITE;
+        ctl[MHD_SUBCG_ACTIVE] = 0.0;
+    } else if (s0 < ctl[MHD_SUBCG_THRESHOLD]) {
+        ctl[MHD_SUBCG_ACTIVE] = 0.0;
+    } else if (ctl[MHD_SUBCG_PRODUCTS] >= max_products) {
+        ctl[MHD_SUBCG_STATUS] = MHD_SUBCG_NOT_CONVERGED;
+        ctl[MHD_SUBCG_ACTIVE] = 0.0;
+    } else {
+        ctl[MHD_SUBCG_BETA] = s1 / ctl[MHD_SUBCG_ABSNEW];
+        ctl[MHD_SUBCG_ABSNEW] = s1;
+    }
+}
+
+__global__ void k_subcg_decide(double* ctl, const double* slots, int count, int phase, double tol,
+                               double max_products) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) subcg_decide(ctl, slots, count, phase, tol, max_products);
 }
 
 // Interior scan of the state: max CFL signal speed (diagnostics.hpp:60-78) and a non-finite flag;
@@ -278,7 +575,7 @@ struct mhd_subdomain {
     double* T[6]{};
     double* A[6]{};
     SubVecs V{};
-    SubScal sc{};
+    SubScal* sc = nullptr;  // device: the solves' matrix of this step
     double g = 0.0, d = 0.0;
     double dt = 0.0, alpha = 0.0;
     StepCoeffs* coeffs = nullptr;
@@ -289,9 +586,34 @@ struct mhd_subdomain {
     SweepGeom sg[2]{}, fg{};
     int st_blocks[2]{}, fn_blocks = 0;
     int blocks = 0;     // grid of the per-cell interior kernels
+    CgSweepArgs cga{};  // the single-sweep solve's sweep: the interior's strips and row segments
+    int cg_blocks = 0;
     int pending_sums = 0;  // sums enqueued by a CG phase without an output pointer
     cudaEvent_t ev_ready = nullptr;  // in-process exchange: this subdomain's strips may be read
     cudaEvent_t ev_done = nullptr;   // in-process exchange: this subdomain's rings are filled
+    cudaEvent_t ev_phase = nullptr;  // a decision group waits for this subdomain's work so far
+};
+
+// Device-resident decisions of one decomposed solve (mhd_subcg_*): the control block, the
+// subdomains' sum slots, and two pinned copies of the control block for the host to poll.
+struct mhd_subcg {
+    int count = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev_decided = nullptr;  // the subdomains' streams wait for the group's last decision
+    // one product of the solve captured as a CUDA graph (mhd_subcg_product), for these arguments
+    cudaGraphExec_t product = nullptr;
+    cudaGraphExec_t sweep[2]{};  // one iteration of the single-sweep form, even and odd k
+    std::vector<mhd_subdomain*> product_subs;
+    int product_P = 0, product_Q = 0;
+    double product_tol = 0.0;
+    long long product_max = 0;
+    double* ctl = nullptr;    // device, MHD_SUBCG_CTL doubles
+    double* slots = nullptr;  // device, count x 4
+    bool own_slots = false;
+    double* host = nullptr;   // pinned, 2 x MHD_SUBCG_CTL
+    cudaEvent_t ev[2]{};
 };
 
 namespace {
@@ -324,6 +646,14 @@ int set_planes(mhd_subdomain* s, int set, Planes* out) {
         case MHD_SUB_SET_DIRECTION:
             out->f[0] = s->V.p;
             return 1;
+        case MHD_SUB_SET_CG_EVEN:  // r_k = r[0], p_{k-1} = p[1] of the single-sweep form
+            out->f[0] = s->V.r;
+            out->f[1] = s->V.q;
+            return 2;
+        case MHD_SUB_SET_CG_ODD:  // r_k = r[1], p_{k-1} = p[0]
+            out->f[0] = s->V.z;
+            out->f[1] = s->V.p;
+            return 2;
         default:
             return 0;
     }
@@ -383,6 +713,77 @@ mhd_status sums_out(mhd_subdomain* s, int n, double* out) {
                             s->stream));
     s->pending_sums = n;
     return MHD_OK;
+}
+
+// The group's stream waits for every subdomain's work so far, and the subdomains' streams wait for
+// the group's (a subdomain on the group's own stream needs neither).
+mhd_status group_after_subs(mhd_subcg* g, mhd_subdomain* const* subs) {
+    for (int i = 0; i < g->count; ++i) {
+        if (subs[i]->stream == g->stream) continue;
+        MHD_TRY(cudaEventRecord(subs[i]->ev_phase, subs[i]->stream));
+        MHD_TRY(cudaStreamWaitEvent(g->stream, subs[i]->ev_phase, 0));
+    }
+    return MHD_OK;
+}
+
+mhd_status subs_after_group(mhd_subcg* g, mhd_subdomain* const* subs) {
+    MHD_TRY(cudaEventRecord(g->ev_decided, g->stream));
+    for (int i = 0; i < g->count; ++i)
+        if (subs[i]->stream != g->stream) MHD_TRY(cudaStreamWaitEvent(subs[i]->stream, g->ev_decided, 0));
+    return MHD_OK;
+}
+
+// Work on the subdomains' streams captured from the group's stream as a graph: the subdomains'
+// streams join the capture through the group's event, and rejoin it at the end.
+template <class Body>
+mhd_status capture_graph(mhd_subcg* g, mhd_subdomain* const* subs, Body body, cudaGraphExec_t* out) {
+    *out = nullptr;
+    MHD_TRY(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed));
+    mhd_status st = subs_after_group(g, subs);
+    if (st == MHD_OK) st = body();
+    if (st == MHD_OK) st = group_after_subs(g, subs);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+    if (st == MHD_OK && e != cudaSuccess) st = cuda_status(e);
+    if (st == MHD_OK) {
+        const cudaError_t ei = cudaGraphInstantiate(out, graph, 0);
+        if (ei != cudaSuccess) st = cuda_status(ei);
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (st != MHD_OK) {
+        *out = nullptr;
+        cudaGetLastError();
+    }
+    return st;
+}
+
+// One product of the two-sweep solve: p's ring, q = A p, decision, update, decision, direction.
+mhd_status capture_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                           long long max_products) {
+    return capture_graph(g, subs, [&]() -> mhd_status {
+        mhd_status st = mhd_sub_exchange_local(subs, P, Q, MHD_SUB_SET_DIRECTION, 1);
+        for (int i = 0; i < g->count && st == MHD_OK; ++i)
+            st = mhd_sub_cg_matvec_dev(subs[i], g->ctl, g->slots + 4 * i);
+        if (st == MHD_OK) st = mhd_subcg_decide_on(g, subs, 1, tol, max_products);
+        for (int i = 0; i < g->count && st == MHD_OK; ++i)
+            st = mhd_sub_cg_update_dev(subs[i], g->ctl, g->slots + 4 * i);
+        if (st == MHD_OK) st = mhd_subcg_decide_on(g, subs, 2, tol, max_products);
+        for (int i = 0; i < g->count && st == MHD_OK; ++i) st = mhd_sub_cg_direction_dev(subs[i], g->ctl);
+        return st;
+    }, &g->product);
+}
+
+// One iteration of the single-sweep solve of parity `odd`: the rings of r_k and p_{k-1}, the
+// sweep, the decision.
+mhd_status capture_sweep(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                         long long max_products, int odd) {
+    return capture_graph(g, subs, [&]() -> mhd_status {
+        mhd_status st = mhd_sub_exchange_local(subs, P, Q, odd ? MHD_SUB_SET_CG_ODD : MHD_SUB_SET_CG_EVEN, 2);
+        for (int i = 0; i < g->count && st == MHD_OK; ++i)
+            st = mhd_sub_cg_sweep_iter_dev(subs[i], g->ctl, g->slots + 4 * i);
+        if (st == MHD_OK) st = mhd_subcg_decide_on(g, subs, 4, tol, max_products);
+        return st;
+    }, &g->sweep[odd]);
 }
 
 }  // namespace
@@ -459,7 +860,8 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
     if (cudaMalloc(&s->pool, (size_t)kSubPlanes * s->ne * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&s->coeffs, sizeof(StepCoeffs)) != cudaSuccess ||
         cudaMalloc(&s->scratch_status, sizeof(DeviceStatus)) != cudaSuccess ||
-        cudaMalloc(&s->part, (size_t)2 * kSubMaxBlocks * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s->sc, sizeof(SubScal)) != cudaSuccess ||
+        cudaMalloc(&s->part, (size_t)4 * kSubMaxBlocks * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&s->dev_out, 8 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&s->host_out, 8 * sizeof(double)) != cudaSuccess) {
         cudaGetLastError();
@@ -474,12 +876,43 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
     s->V.p = q; q += s->ne;
     s->V.q = q; q += s->ne;
     s->V.z = q;
+    {
+        // the single-sweep solve: 28-column strips of the interior, row segments of seg_h rows,
+        // about half a device's resident warps (the subdomains of one device share it)
+        if (cudaFuncSetAttribute(k_sub_cg_sweep_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSubCgRingBytes) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sub_cg_sweep_iter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSubCgRingBytes) != cudaSuccess)
+            return fail(MHD_ERR_CUDA);
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sub_cg_sweep_iter, kSubCgNT, kSubCgRingBytes) !=
+                cudaSuccess || occ < 1)
+            return fail(MHD_ERR_CUDA);
+        CgSweepArgs& a = s->cga;
+        a.D = s->ext;
+        a.x = s->V.x;
+        a.r[0] = s->V.r;
+        a.r[1] = s->V.z;
+        a.p[0] = s->V.p;
+        a.p[1] = s->V.q;
+        a.col0 = kH;
+        a.col_end = kH + p->nx;
+        a.strips_x = (p->nx + CG_W - 1) / CG_W;
+        const int target = std::max(1, occ * s->num_sms * (kSubCgNT / 32) / 2);
+        const int segs = std::max(1, target / a.strips_x);
+        a.seg_h = std::max(32, (p->ny + segs - 1) / segs);
+        a.nwarps = a.strips_x * ((p->ny + a.seg_h - 1) / a.seg_h);
+        s->cg_blocks = std::min((a.nwarps + kSubCgNT / 32 - 1) / (kSubCgNT / 32),
+                                std::min(kSubMaxBlocks, occ * s->num_sms));
+    }
     if (cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_phase, cudaEventDisableTiming) != cudaSuccess)
         return fail(MHD_ERR_CUDA);
     if (cudaMemsetAsync(s->pool, 0, (size_t)kSubPlanes * s->ne * sizeof(double), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->coeffs, 0, sizeof(StepCoeffs), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->scratch_status, 0, sizeof(DeviceStatus), s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->sc, 0, sizeof(SubScal), s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess)
         return fail(MHD_ERR_CUDA);
     *out = s;
@@ -493,11 +926,13 @@ mhd_status mhd_sub_destroy(mhd_subdomain* s) {
     cudaFree(s->pool);
     cudaFree(s->coeffs);
     cudaFree(s->scratch_status);
+    cudaFree(s->sc);
     cudaFree(s->part);
     cudaFree(s->dev_out);
     if (s->host_out) cudaFreeHost(s->host_out);
     if (s->ev_ready) cudaEventDestroy(s->ev_ready);
     if (s->ev_done) cudaEventDestroy(s->ev_done);
+    if (s->ev_phase) cudaEventDestroy(s->ev_phase);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     cudaGetLastError();
     delete s;
@@ -592,44 +1027,52 @@ mhd_status mhd_sub_exchange_local(mhd_subdomain* const* subs, int P, int Q, int 
         if (e->iv.ny != subs[i]->iv.ny || n->iv.nx != subs[i]->iv.nx) return MHD_ERR_INVALID_ARGUMENT;
     }
     MHD_TRY(cudaSetDevice(subs[0]->device));
-    const int sides[2][2] = {{MHD_SUB_WEST, MHD_SUB_EAST}, {MHD_SUB_SOUTH, MHD_SUB_NORTH}};
-    for (int axis = 0; axis < 2; ++axis) {
-        // every subdomain's work so far is done before a neighbour reads its strips
+    // subdomains on one stream are ordered by it: no events
+    bool one_stream = true;
+    for (int i = 1; i < count; ++i) one_stream = one_stream && subs[i]->stream == subs[0]->stream;
+    // every subdomain's work so far is done before a neighbour reads its interior
+    if (!one_stream)
         for (int i = 0; i < count; ++i) MHD_TRY(cudaEventRecord(subs[i]->ev_ready, subs[i]->stream));
-        for (int i = 0; i < count; ++i) {
-            mhd_subdomain* me = subs[i];
-            const int p = i % P, q = i / P;
-            for (int k = 0; k < 2; ++k) {
-                const int side = sides[axis][k];
-                const int opposite = side ^ 1;  // WEST <-> EAST, SOUTH <-> NORTH
-                int nb;
-                if (side == MHD_SUB_WEST) nb = q * P + (p + P - 1) % P;
-                else if (side == MHD_SUB_EAST) nb = q * P + (p + 1) % P;
-                else if (side == MHD_SUB_SOUTH) nb = ((q + Q - 1) % Q) * P + p;
-                else nb = ((q + 1) % Q) * P + p;
-                mhd_subdomain* from = subs[nb];
-                if (from != me) MHD_TRY(cudaStreamWaitEvent(me->stream, from->ev_ready, 0));
-                // my ring beyond `side` <- the neighbour's strip next to its opposite side
-                int dx0 = 0, dy0 = 0, w = 0, h = 0, sx0 = 0, sy0 = 0, sw = 0, sh = 0;
-                if (!strip_rect(me, side, width, false, &dx0, &dy0, &w, &h) ||
-                    !strip_rect(from, opposite, width, true, &sx0, &sy0, &sw, &sh))
-                    return MHD_ERR_INVALID_ARGUMENT;
-                Planes dst, src;
-                const int np = set_planes(me, set, &dst);
-                set_planes(from, set, &src);
-                for (int c = 0; c < np; ++c)
-                    MHD_TRY(cudaMemcpy2DAsync(dst.f[c] + (size_t)dy0 * me->iv.nxe + dx0,
-                                              (size_t)me->iv.nxe * sizeof(double),
-                                              src.f[c] + (size_t)sy0 * from->iv.nxe + sx0,
-                                              (size_t)from->iv.nxe * sizeof(double), (size_t)w * sizeof(double),
-                                              h, cudaMemcpyDeviceToDevice, me->stream));
+    for (int i = 0; i < count; ++i) {
+        mhd_subdomain* me = subs[i];
+        const int p = i % P, q = i / P;
+        RingSources src{};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                mhd_subdomain* from = subs[((q + a - 1 + Q) % Q) * P + (p + b - 1 + P) % P];
+                if (!one_stream && from != me) {
+                    bool seen = false;  // wait once per distinct neighbour
+                    for (int a2 = 0; a2 <= a && !seen; ++a2)
+                        for (int b2 = 0; b2 < 3 && !seen; ++b2)
+                            if ((a2 < a || b2 < b) && subs[((q + a2 - 1 + Q) % Q) * P + (p + b2 - 1 + P) % P] == from)
+                                seen = true;
+                    if (!seen) MHD_TRY(cudaStreamWaitEvent(me->stream, from->ev_ready, 0));
+                }
+                Planes sp;
+                set_planes(from, set, &sp);
+                for (int k = 0; k < 6; ++k) src.f[a][b][k] = sp.f[k];
+                src.nxe[a][b] = from->iv.nxe;
             }
-        }
-        // a subdomain changes its interior again only after its neighbours have copied from it
+        src.nx_w = subs[q * P + (p + P - 1) % P]->iv.nx;
+        src.ny_s = subs[((q + Q - 1) % Q) * P + p]->iv.ny;
+        Planes dst;
+        const int np = set_planes(me, set, &dst);
+        const size_t cells = (size_t)2 * width * (me->iv.nx + 2 * width) + (size_t)2 * width * me->iv.ny;
+        const int blocks = (int)std::max<size_t>(1, std::min<size_t>((cells + kSubNT - 1) / kSubNT, 4 * me->num_sms));
+        k_sub_ring_gather<<<blocks, kSubNT, 0, me->stream>>>(dst, np, me->iv, width, src);
+        MHD_TRY(cudaGetLastError());
+    }
+    // a subdomain changes its interior again only after its neighbours have read from it
+    if (!one_stream) {
         for (int i = 0; i < count; ++i) MHD_TRY(cudaEventRecord(subs[i]->ev_done, subs[i]->stream));
-        for (int i = 0; i < count; ++i)
-            for (int j = 0; j < count; ++j)
-                if (j != i) MHD_TRY(cudaStreamWaitEvent(subs[i]->stream, subs[j]->ev_done, 0));
+        for (int i = 0; i < count; ++i) {
+            const int p = i % P, q = i / P;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    mhd_subdomain* nb = subs[((q + a - 1 + Q) % Q) * P + (p + b - 1 + P) % P];
+                    if (nb != subs[i]) MHD_TRY(cudaStreamWaitEvent(subs[i]->stream, nb->ev_done, 0));
+                }
+        }
     }
     return MHD_OK;
 }
@@ -660,12 +1103,8 @@ mhd_status mhd_sub_set_step(mhd_subdomain* s, double dt, double alpha) {
     if (!(dt > 0) || !std::isfinite(dt) || !(alpha >= 0) || !std::isfinite(alpha)) return MHD_ERR_INVALID_ARGUMENT;
     s->dt = dt;
     s->alpha = alpha;
-    k_sub_set_coeffs<<<1, 1, 0, s->stream>>>(s->coeffs, dt, alpha, s->g, s->d);
+    k_sub_set_coeffs<<<1, 1, 0, s->stream>>>(s->coeffs, s->sc, dt, alpha, s->g, s->d, s->prm.dx, s->prm.dy);
     MHD_TRY(cudaGetLastError());
-    s->sc.cx = alpha / (s->prm.dx * s->prm.dx);
-    s->sc.cy = alpha / (s->prm.dy * s->prm.dy);
-    s->sc.diag = 1 + 2 * (s->sc.cx + s->sc.cy);
-    s->sc.invdiag = (s->sc.diag == 0.0) ? 1.0 : 1.0 / s->sc.diag;
     return MHD_OK;
 }
 
@@ -723,7 +1162,7 @@ mhd_status mhd_sub_cg_rhs(mhd_subdomain* s, int solve_index, double out[2]) {
 mhd_status mhd_sub_cg_matvec(mhd_subdomain* s, double* pq) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    k_sub_cg_matvec<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, s->part);
+    k_sub_cg_matvec<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, nullptr, s->part);
     MHD_TRY(cudaGetLastError());
     k_sub_final<1><<<1, 32, 0, s->stream>>>(s->part, s->blocks, s->dev_out);
     MHD_TRY(cudaGetLastError());
@@ -733,7 +1172,7 @@ mhd_status mhd_sub_cg_matvec(mhd_subdomain* s, double* pq) {
 mhd_status mhd_sub_cg_update(mhd_subdomain* s, double alpha, double out[2]) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    k_sub_cg_update<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, alpha, s->part);
+    k_sub_cg_update<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, alpha, nullptr, s->part);
     MHD_TRY(cudaGetLastError());
     k_sub_final<2><<<1, 32, 0, s->stream>>>(s->part, s->blocks, s->dev_out);
     MHD_TRY(cudaGetLastError());
@@ -753,7 +1192,7 @@ mhd_status mhd_sub_sums(mhd_subdomain* s, double* out, int n) {
 mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    k_sub_cg_dir<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, beta);
+    k_sub_cg_dir<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, beta, nullptr);
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
 }
@@ -761,8 +1200,266 @@ mhd_status mhd_sub_cg_direction(mhd_subdomain* s, double beta) {
 mhd_status mhd_sub_cg_zero_solution(mhd_subdomain* s) {
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
-    k_sub_zero_interior<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V.x);
+    k_sub_zero_interior<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V.x, nullptr);
     MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_rhs_dev(mhd_subdomain* s, int solve_index, double* slot) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if ((solve_index != 0 && solve_index != 1) || !slot) return MHD_ERR_INVALID_ARGUMENT;
+    const double* bx = solve_index == 0 ? s->T[4] : s->A[4];
+    const double* by = solve_index == 0 ? s->T[5] : s->A[5];
+    k_sub_cg_rhs<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->prm.eta, 1.0 / s->prm.dx, 1.0 / s->prm.dy,
+                                                      bx, by, s->V, s->sc, s->part);
+    MHD_TRY(cudaGetLastError());
+    k_sub_final<2><<<1, 32, 0, s->stream>>>(s->part, s->blocks, slot);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_matvec_dev(mhd_subdomain* s, const double* ctl, double* slot) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl || !slot) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_cg_matvec<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, ctl, s->part);
+    MHD_TRY(cudaGetLastError());
+    k_sub_final<1><<<1, 32, 0, s->stream>>>(s->part, s->blocks, slot);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_update_dev(mhd_subdomain* s, const double* ctl, double* slot) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl || !slot) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_cg_update<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, s->sc, 0.0, ctl, s->part);
+    MHD_TRY(cudaGetLastError());
+    k_sub_final<2><<<1, 32, 0, s->stream>>>(s->part, s->blocks, slot);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_direction_dev(mhd_subdomain* s, const double* ctl) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_cg_dir<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V, 0.0, ctl);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_finish_dev(mhd_subdomain* s, const double* ctl) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_zero_interior<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V.x, ctl);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_sweep_rhs_dev(mhd_subdomain* s, int solve_index, double* slot) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if ((solve_index != 0 && solve_index != 1) || !slot) return MHD_ERR_INVALID_ARGUMENT;
+    CgSweepArgs a = s->cga;
+    a.bxf = solve_index == 0 ? s->T[4] : s->A[4];
+    a.byf = solve_index == 0 ? s->T[5] : s->A[5];
+    k_sub_cg_sweep_rhs<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(a, s->sc, s->part);
+    MHD_TRY(cudaGetLastError());
+    k_sub_final<4><<<1, 32, 0, s->stream>>>(s->part, s->cg_blocks, slot);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_sweep_iter_dev(mhd_subdomain* s, const double* ctl, double* slot) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl || !slot) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_cg_sweep_iter<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(s->cga, s->sc, ctl, s->part);
+    MHD_TRY(cudaGetLastError());
+    k_sub_final<4><<<1, 32, 0, s->stream>>>(s->part, s->cg_blocks, slot);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_sub_cg_sweep_finish_dev(mhd_subdomain* s, const double* ctl) {
+    mhd_status st = check_sub(s);
+    if (st != MHD_OK) return st;
+    if (!ctl) return MHD_ERR_INVALID_ARGUMENT;
+    k_sub_cg_sweep_finish<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, s->V.x, s->V.p, ctl);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_subcg_create(int count, void* stream, double* slots, mhd_subcg** out) {
+    if (!out || count < 1 || count > 1 << 20) return MHD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!mhd_device_available()) return MHD_ERR_NO_DEVICE;
+    mhd_subcg* g = new (std::nothrow) mhd_subcg();
+    if (!g) return MHD_ERR_OUT_OF_MEMORY;
+    g->count = count;
+    if (cudaGetDevice(&g->device) != cudaSuccess) {
+        delete g;
+        return MHD_ERR_NO_DEVICE;
+    }
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) == cudaSuccess) {
+        g->own_stream = true;
+    } else {
+        cudaGetLastError();
+        delete g;
+        return MHD_ERR_CUDA;
+    }
+    g->slots = slots;
+    g->own_slots = slots == nullptr;
+    if (cudaMalloc(&g->ctl, MHD_SUBCG_CTL * sizeof(double)) != cudaSuccess ||
+        (g->own_slots && cudaMalloc(&g->slots, (size_t)4 * count * sizeof(double)) != cudaSuccess) ||
+        cudaMallocHost(&g->host, 2 * MHD_SUBCG_CTL * sizeof(double)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->ev_decided, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        mhd_subcg_destroy(g);
+        return MHD_ERR_OUT_OF_MEMORY;
+    }
+    if (cudaMemsetAsync(g->ctl, 0, MHD_SUBCG_CTL * sizeof(double), g->stream) != cudaSuccess ||
+        cudaMemsetAsync(g->slots, 0, (size_t)4 * count * sizeof(double), g->stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->stream) != cudaSuccess) {
+        cudaGetLastError();
+        mhd_subcg_destroy(g);
+        return MHD_ERR_CUDA;
+    }
+    *out = g;
+    return MHD_OK;
+}
+
+mhd_status mhd_subcg_destroy(mhd_subcg* g) {
+    if (!g) return MHD_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->product) cudaGraphExecDestroy(g->product);
+    for (cudaGraphExec_t e : g->sweep)
+        if (e) cudaGraphExecDestroy(e);
+    for (cudaEvent_t e : g->ev)
+        if (e) cudaEventDestroy(e);
+    if (g->ev_decided) cudaEventDestroy(g->ev_decided);
+    if (g->host) cudaFreeHost(g->host);
+    if (g->own_slots) cudaFree(g->slots);
+    cudaFree(g->ctl);
+    if (g->own_stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return MHD_OK;
+}
+
+double* mhd_subcg_slots(mhd_subcg* g) { return g ? g->slots : nullptr; }
+const double* mhd_subcg_control(mhd_subcg* g) { return g ? g->ctl : nullptr; }
+
+mhd_status mhd_subcg_decide(mhd_subcg* g, int phase, double tol, long long max_products) {
+    if (!g || phase < 0 || phase > 4 || !(tol >= 0) || max_products < 1) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(g->device));
+    k_subcg_decide<<<1, 32, 0, g->stream>>>(g->ctl, g->slots, g->count, phase, tol, (double)max_products);
+    MHD_TRY(cudaGetLastError());
+    return MHD_OK;
+}
+
+mhd_status mhd_subcg_post(mhd_subcg* g, int tag) {
+    if (!g || tag < 0) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(g->device));
+    const int b = tag & 1;
+    MHD_TRY(cudaMemcpyAsync(g->host + b * MHD_SUBCG_CTL, g->ctl, MHD_SUBCG_CTL * sizeof(double),
+                            cudaMemcpyDeviceToHost, g->stream));
+    MHD_TRY(cudaEventRecord(g->ev[b], g->stream));
+    return MHD_OK;
+}
+
+mhd_status mhd_subcg_read(mhd_subcg* g, int tag, double* out) {
+    if (!g || tag < 0 || !out) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(g->device));
+    const int b = tag & 1;
+    MHD_TRY(cudaEventSynchronize(g->ev[b]));
+    memcpy(out, g->host + b * MHD_SUBCG_CTL, MHD_SUBCG_CTL * sizeof(double));
+    return MHD_OK;
+}
+
+mhd_status mhd_subcg_decide_on(mhd_subcg* g, mhd_subdomain* const* subs, int phase, double tol,
+                               long long max_products) {
+    if (!g || !subs || phase < 0 || phase > 4 || !(tol >= 0) || max_products < 1) return MHD_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < g->count; ++i)
+        if (!subs[i] || subs[i]->device != g->device) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(g->device));
+    mhd_status st = group_after_subs(g, subs);
+    if (st != MHD_OK) return st;
+    k_subcg_decide<<<1, 32, 0, g->stream>>>(g->ctl, g->slots, g->count, phase, tol, (double)max_products);
+    MHD_TRY(cudaGetLastError());
+    return subs_after_group(g, subs);
+}
+
+namespace {
+// Drop the captured graphs when the arguments they were captured for change.
+mhd_status check_graph_args(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                            long long max_products) {
+    if (!g || !subs || P < 1 || Q < 1 || P * Q != g->count || !(tol >= 0) || max_products < 1)
+        return MHD_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < g->count; ++i)
+        if (!subs[i] || subs[i]->device != g->device) return MHD_ERR_INVALID_ARGUMENT;
+    MHD_TRY(cudaSetDevice(g->device));
+    const bool same = !g->product_subs.empty() && g->product_P == P && g->product_Q == Q &&
+                      g->product_tol == tol && g->product_max == max_products &&
+                      std::equal(g->product_subs.begin(), g->product_subs.end(), subs);
+    if (!same) {
+        if (g->product) cudaGraphExecDestroy(g->product);
+        g->product = nullptr;
+        for (cudaGraphExec_t& e : g->sweep) {
+            if (e) cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+        g->product_subs.assign(subs, subs + g->count);
+        g->product_P = P;
+        g->product_Q = Q;
+        g->product_tol = tol;
+        g->product_max = max_products;
+    }
+    return MHD_OK;
+}
+
+// Replay a captured graph after the subdomains' work so far, post the control block under `tag`,
+// and order the subdomains' later work after both.
+mhd_status replay(mhd_subcg* g, mhd_subdomain* const* subs, cudaGraphExec_t exec, int tag) {
+    mhd_status st = group_after_subs(g, subs);
+    if (st != MHD_OK) return st;
+    MHD_TRY(cudaGraphLaunch(exec, g->stream));
+    if ((st = mhd_subcg_post(g, tag)) != MHD_OK) return st;
+    return subs_after_group(g, subs);
+}
+}  // namespace
+
+mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                             long long max_products, int tag) {
+    if (tag < 0) return MHD_ERR_INVALID_ARGUMENT;
+    mhd_status st = check_graph_args(g, subs, P, Q, tol, max_products);
+    if (st != MHD_OK) return st;
+    if (!g->product && (st = capture_product(g, subs, P, Q, tol, max_products)) != MHD_OK) return st;
+    return replay(g, subs, g->product, tag);
+}
+
+mhd_status mhd_subcg_sweep_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
+                                   long long max_products, int k, int tag) {
+    if (tag < 0 || k < 0) return MHD_ERR_INVALID_ARGUMENT;
+    mhd_status st = check_graph_args(g, subs, P, Q, tol, max_products);
+    if (st != MHD_OK) return st;
+    const int odd = k & 1;
+    if (!g->sweep[odd] && (st = capture_sweep(g, subs, P, Q, tol, max_products, odd)) != MHD_OK) return st;
+    return replay(g, subs, g->sweep[odd], tag);
+}
+
+mhd_status mhd_subcg_decide_host(double* ctl, const double* slots, int count, int phase, double tol,
+                                 long long max_products) {
+    if (!ctl || !slots || count < 1 || phase < 0 || phase > 4 || !(tol >= 0) || max_products < 1)
+        return MHD_ERR_INVALID_ARGUMENT;
+    subcg_decide(ctl, slots, count, phase, tol, (double)max_products);
     return MHD_OK;
 }
 

@@ -27,6 +27,13 @@ cg_rhs, cg_matvec, cg_update (each with wait=False: enqueue only, sums(n) return
 cg_direction, cg_zero_solution, divb_sums; and, where its work runs on a stream, record_event /
 wait_event, with which LocalTransport orders the subdomains' streams without host waits.
 ``GpuSubdomain`` is the one over the C ABI.
+
+The solve's decisions can stay on the device (``device_decisions``): the subdomains' phases
+(cg_rhs_dev, cg_matvec_dev, cg_update_dev, cg_direction_dev, cg_finish_dev) write their sums into
+a group's slots and read alpha and beta from its control block (``DeviceCgGroup``, mhd_subcg_* of
+the C ABI; ``HostCgGroup`` applies the same rules to host arrays for CPU stand-ins), and the host
+polls the control block one product behind instead of waiting for every phase's sums. The results
+are bit-identical to the host decisions.
 """
 from __future__ import annotations
 
@@ -42,9 +49,14 @@ HALO = 4
 WEST, EAST, SOUTH, NORTH = 0, 1, 2, 3
 OPPOSITE = {WEST: EAST, EAST: WEST, SOUTH: NORTH, NORTH: SOUTH}
 SET_STATE, SET_PREDICTOR, SET_ACCUMULATOR_B, SET_SOLUTION, SET_DIRECTION = 0, 1, 2, 3, 4
+SET_CG_EVEN, SET_CG_ODD = 5, 6  # the single-sweep solve's r_k and p_{k-1}
 DBL_MIN = 2.2250738585072014e-308
 EPS = 2.220446049250313e-16
 ARS_G = (2.0 - math.sqrt(2.0)) / 2.0  # solvers.hpp:41
+# control block of the device-resident decisions (MHD_SUBCG_* of include/mhd_b200.h)
+SUBCG_CTL = 16
+CG_ACTIVE, CG_STATUS, CG_PRODUCTS, CG_ALPHA, CG_BETA = 0, 1, 2, 6, 7
+CG_OK, CG_NOT_CONVERGED, CG_NONFINITE = 0, 1, 2
 
 
 class Partition:
@@ -217,6 +229,118 @@ class GpuSubdomain:
         _check(self.lib.mhd_sub_divb_sums(self.h, out), "mhd_sub_divb_sums")
         return [out[0], out[1]]
 
+    # CG phases with the decisions on the device: slot and ctl are device addresses (ints)
+    def cg_rhs_dev(self, solve_index: int, slot: int):
+        _check(self.lib.mhd_sub_cg_rhs_dev(self.h, solve_index, slot), "mhd_sub_cg_rhs_dev")
+
+    def cg_matvec_dev(self, ctl: int, slot: int):
+        _check(self.lib.mhd_sub_cg_matvec_dev(self.h, ctl, slot), "mhd_sub_cg_matvec_dev")
+
+    def cg_update_dev(self, ctl: int, slot: int):
+        _check(self.lib.mhd_sub_cg_update_dev(self.h, ctl, slot), "mhd_sub_cg_update_dev")
+
+    def cg_direction_dev(self, ctl: int):
+        _check(self.lib.mhd_sub_cg_direction_dev(self.h, ctl), "mhd_sub_cg_direction_dev")
+
+    def cg_finish_dev(self, ctl: int):
+        _check(self.lib.mhd_sub_cg_finish_dev(self.h, ctl), "mhd_sub_cg_finish_dev")
+
+    # the single-sweep form of the solve (the single context's sweeps on the interior)
+    def cg_sweep_rhs_dev(self, solve_index: int, slot: int):
+        _check(self.lib.mhd_sub_cg_sweep_rhs_dev(self.h, solve_index, slot), "mhd_sub_cg_sweep_rhs_dev")
+
+    def cg_sweep_iter_dev(self, ctl: int, slot: int):
+        _check(self.lib.mhd_sub_cg_sweep_iter_dev(self.h, ctl, slot), "mhd_sub_cg_sweep_iter_dev")
+
+    def cg_sweep_finish_dev(self, ctl: int):
+        _check(self.lib.mhd_sub_cg_sweep_finish_dev(self.h, ctl), "mhd_sub_cg_sweep_finish_dev")
+
+
+class DeviceCgGroup:
+    """The decisions of one decomposed solve on the device (mhd_subcg of the C ABI): a control
+    block and `count` sum slots. `slots`: a CUDA tensor of count * 4 doubles to use as the slots
+    (across ranks, where they are all-gathered), else the group allocates them."""
+
+    def __init__(self, lib, count: int, stream: int, slots=None):
+        self.lib = lib
+        self.count = count
+        self._slots_tensor = slots
+        h = ctypes.c_void_p()
+        _check(lib.mhd_subcg_create(count, ctypes.c_void_p(stream) if stream else None,
+                                    ctypes.c_void_p(slots.data_ptr()) if slots is not None else None,
+                                    ctypes.byref(h)), "mhd_subcg_create")
+        self.h = h
+        self.slots = lib.mhd_subcg_slots(h)
+        self.ctl = lib.mhd_subcg_control(h)
+
+    def slot(self, i: int) -> int:
+        return self.slots + 32 * i
+
+    def decide(self, phase: int, tol: float, max_products: int):
+        """On the group's stream (the subdomain shares it, or the caller orders them)."""
+        _check(self.lib.mhd_subcg_decide(self.h, phase, tol, max_products), "mhd_subcg_decide")
+
+    def decide_on(self, handles, phase: int, tol: float, max_products: int):
+        """Ordered by events after the subdomains' work so far, and their later work after it."""
+        _check(self.lib.mhd_subcg_decide_on(self.h, handles, phase, tol, max_products), "mhd_subcg_decide_on")
+
+    def product(self, handles, P: int, Q: int, tol: float, max_products: int, tag: int):
+        """One product of the solve on the P x Q subdomains as a replayed CUDA graph; posts `tag`."""
+        _check(self.lib.mhd_subcg_product(self.h, handles, P, Q, tol, max_products, tag), "mhd_subcg_product")
+
+    def sweep_product(self, handles, P: int, Q: int, tol: float, max_products: int, k: int, tag: int):
+        """Iteration k of the single-sweep solve as a replayed CUDA graph; posts `tag`."""
+        _check(self.lib.mhd_subcg_sweep_product(self.h, handles, P, Q, tol, max_products, k, tag),
+               "mhd_subcg_sweep_product")
+
+    def post(self, tag: int):
+        _check(self.lib.mhd_subcg_post(self.h, tag), "mhd_subcg_post")
+
+    def read(self, tag: int):
+        out = (ctypes.c_double * SUBCG_CTL)()
+        _check(self.lib.mhd_subcg_read(self.h, tag, out), "mhd_subcg_read")
+        return list(out)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_subcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostCgGroup:
+    """The same control block and slots in host memory, for CPU stand-in subdomains; the rules are
+    the library's (mhd_subcg_decide_host)."""
+
+    def __init__(self, lib, count: int):
+        self.lib = lib
+        self.count = count
+        self.ctl = np.zeros(SUBCG_CTL)
+        self.slots = np.zeros(4 * count)
+        self._posted = [None, None]
+
+    def slot(self, i: int):
+        return self.slots[4 * i:4 * i + 4]
+
+    def decide(self, phase: int, tol: float, max_products: int):
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self.lib.mhd_subcg_decide_host(self.ctl.ctypes.data_as(dp), self.slots.ctypes.data_as(dp),
+                                              self.count, phase, tol, max_products), "mhd_subcg_decide_host")
+
+    def post(self, tag: int):
+        self._posted[tag & 1] = self.ctl.copy()
+
+    def read(self, tag: int):
+        return [float(v) for v in self._posted[tag & 1]]
+
+    def close(self):
+        pass
+
 
 _bound = set()
 
@@ -250,6 +374,28 @@ def _bind(lib):
     lib.mhd_sub_synchronize.argtypes = [vp]
     lib.mhd_sub_sums.argtypes = [vp, dp, ip]
     lib.mhd_sub_exchange_local.argtypes = [ctypes.POINTER(vp), ip, ip, ip, ip]
+    lib.mhd_sub_cg_rhs_dev.argtypes = [vp, ip, vp]
+    lib.mhd_sub_cg_matvec_dev.argtypes = [vp, vp, vp]
+    lib.mhd_sub_cg_update_dev.argtypes = [vp, vp, vp]
+    lib.mhd_sub_cg_direction_dev.argtypes = [vp, vp]
+    lib.mhd_sub_cg_finish_dev.argtypes = [vp, vp]
+    lib.mhd_subcg_create.argtypes = [ip, vp, vp, ctypes.POINTER(vp)]
+    lib.mhd_subcg_destroy.argtypes = [vp]
+    lib.mhd_subcg_slots.argtypes = [vp]
+    lib.mhd_subcg_slots.restype = ctypes.c_size_t
+    lib.mhd_subcg_control.argtypes = [vp]
+    lib.mhd_subcg_control.restype = ctypes.c_size_t
+    lib.mhd_subcg_decide.argtypes = [vp, ip, ctypes.c_double, ctypes.c_longlong]
+    lib.mhd_subcg_post.argtypes = [vp, ip]
+    lib.mhd_subcg_read.argtypes = [vp, ip, dp]
+    lib.mhd_subcg_decide_host.argtypes = [dp, dp, ip, ip, ctypes.c_double, ctypes.c_longlong]
+    lib.mhd_subcg_decide_on.argtypes = [vp, ctypes.POINTER(vp), ip, ctypes.c_double, ctypes.c_longlong]
+    lib.mhd_subcg_product.argtypes = [vp, ctypes.POINTER(vp), ip, ip, ctypes.c_double, ctypes.c_longlong, ip]
+    lib.mhd_subcg_sweep_product.argtypes = [vp, ctypes.POINTER(vp), ip, ip, ctypes.c_double, ctypes.c_longlong,
+                                            ip, ip]
+    lib.mhd_sub_cg_sweep_rhs_dev.argtypes = [vp, ip, vp]
+    lib.mhd_sub_cg_sweep_iter_dev.argtypes = [vp, vp, vp]
+    lib.mhd_sub_cg_sweep_finish_dev.argtypes = [vp, vp]
     assert lib.mhd_sub_halo() == HALO
     _bound.add(id(lib))
     return lib
@@ -274,8 +420,11 @@ class LocalTransport:
         # GPU subdomains of one process exchange natively (device copies ordered by events);
         # native=False moves their strips through pack/unpack buffers, as across GPUs
         self._native = None
-        if native and all(isinstance(s_, GpuSubdomain) for s_ in self.subs):
-            self._native = (ctypes.c_void_p * part.count)(*[s_.h for s_ in self.subs])
+        self._handles = None
+        if all(isinstance(s_, GpuSubdomain) for s_ in self.subs):
+            self._handles = (ctypes.c_void_p * part.count)(*[s_.h for s_ in self.subs])
+            if native:
+                self._native = self._handles
 
     @property
     def own(self):
@@ -318,6 +467,24 @@ class LocalTransport:
 
     def any(self, flags) -> bool:
         return any(flags)
+
+    # device-resident decisions: every subdomain writes its own slot of one group
+    def cg_group(self):
+        """A decision group for the subdomains, or None where the host must decide: GPU
+        subdomains get a DeviceCgGroup on a stream of its own (ordered against theirs by events),
+        CPU stand-ins a HostCgGroup."""
+        gpu = [isinstance(s_, GpuSubdomain) for s_ in self.subs]
+        if all(gpu):
+            return DeviceCgGroup(self.subs[0].lib, self.part.count, 0)
+        if not any(gpu):
+            return HostCgGroup(_bind(load_library()), self.part.count)
+        return None
+
+    def own_slots(self, group):
+        return [group.slot(i) for i in range(self.part.count)]
+
+    def gather_slots(self, group):
+        pass
 
 
 class DistTransport:
@@ -386,13 +553,52 @@ class DistTransport:
         (mine,) = flags
         return bool(np.any(self._gather([1.0 if mine else 0.0])))
 
+    # device-resident decisions: this rank's sums go into a local slot, all-gathered into the
+    # group's slots in rank order before every decision
+    def cg_group(self):
+        torch = self.torch
+        if isinstance(self.sub, GpuSubdomain):
+            self._slots = torch.zeros(4 * self.part.count, dtype=torch.float64, device="cuda")
+            self._local = torch.zeros(4, dtype=torch.float64, device="cuda")
+            return DeviceCgGroup(self.sub.lib, self.part.count, self.sub.stream, slots=self._slots)
+        self._local = np.zeros(4)
+        return HostCgGroup(_bind(load_library()), self.part.count)
+
+    def own_slots(self, group):
+        return [self._local.data_ptr() if isinstance(group, DeviceCgGroup) else self._local]
+
+    def gather_slots(self, group):
+        torch = self.torch
+        if isinstance(group, DeviceCgGroup):
+            # on the subdomain's stream: the collective follows its phase and precedes the decision
+            with torch.cuda.stream(torch.cuda.ExternalStream(self.sub.stream)):
+                self.dist.all_gather_into_tensor(self._slots, self._local)
+            return
+        out = torch.empty(4 * self.part.count, dtype=torch.float64)
+        self.dist.all_gather_into_tensor(out, torch.from_numpy(self._local))
+        group.slots[:] = out.numpy()
+
 
 class DecomposedRun:
     """ARS(2,2,2) steps of one nx x ny periodic grid split over the transport's subdomains."""
 
     def __init__(self, part: Partition, transport, dx: float, dy: float, eta: float, *,
-                 courant: float = 0.5, safety: float = 0.9, cg_tol: float = 0.0, cg_max_iters: int = 0):
+                 courant: float = 0.5, safety: float = 0.9, cg_tol: float = 0.0, cg_max_iters: int = 0,
+                 device_decisions: bool = True, cg_form: str | None = None):
+        """device_decisions: take the solve's decisions on the device (DeviceCgGroup) where the
+        transport allows it; False keeps them on the host (both give bit-identical results).
+        cg_form: "sweep", the single context's single-sweep solver on every subdomain (GPU
+        subdomains with device decisions; the default there), or "two_sweep" (a matrix product
+        and an update per product; every other case)."""
         self.part, self.tr = part, transport
+        self._group = transport.cg_group() if device_decisions else None
+        self._slots = transport.own_slots(self._group) if self._group is not None else None
+        sweep_ok = isinstance(self._group, DeviceCgGroup)
+        if cg_form is None:
+            cg_form = "sweep" if sweep_ok else "two_sweep"
+        if cg_form not in ("sweep", "two_sweep") or (cg_form == "sweep" and not sweep_ok):
+            raise ValueError(f"cg_form {cg_form!r} needs GPU subdomains with device decisions")
+        self.cg_form = cg_form
         self.dx, self.dy, self.eta = dx, dy, eta
         self.courant, self.safety = courant, safety
         self.tol = cg_tol if cg_tol > 0 else EPS
@@ -449,6 +655,8 @@ class DecomposedRun:
         return [s.sums(n) for s in own]
 
     def _solve(self, index: int) -> int:
+        if self._group is not None:
+            return self._solve_device(index, self.cg_form == "sweep")
         own = self.tr.own
         bb, abs_new = self.tr.sum(self._phase(own, lambda s: s.cg_rhs(index, wait=False), 2))
         threshold = max(self.tol * self.tol * bb, DBL_MIN)
@@ -480,6 +688,93 @@ class DecomposedRun:
         if not converged:
             self.status = "cg_not_converged"
         return products
+
+    def _solve_device(self, index: int, sweep: bool = False) -> int:
+        """The solve with the decisions in the group's control block: each product is enqueued
+        before the previous one's state is read back, so the host waits only for work that is
+        already behind the device's queue; a product enqueued after the solve ended does nothing
+        but its ring exchange. GPU subdomains of one process run each product as one replayed
+        CUDA graph (mhd_subcg_product, mhd_subcg_sweep_product). sweep: the single-sweep form."""
+        g, own, slots, tr = self._group, self.tr.own, self._slots, self.tr
+        ctl = g.ctl
+        maxp, tol = self.max_iters, self.tol
+        handles = getattr(tr, "_handles", None) if isinstance(g, DeviceCgGroup) else None
+        if handles is not None:
+            def decide(phase):
+                g.decide_on(handles, phase, tol, maxp)
+        else:
+            def decide(phase):
+                tr.gather_slots(g)
+                g.decide(phase, tol, maxp)
+        graph = handles is not None and getattr(tr, "_native", None) is not None
+        if sweep:
+            return self._sweep_solve(index, g, own, slots, decide, graph, handles)
+        for s, sl in zip(own, slots):
+            s.cg_rhs_dev(index, sl)
+        decide(0)
+        tag = 0
+        g.post(tag)
+        for _ in range(maxp):
+            tag += 1
+            if graph:
+                g.product(handles, self.part.P, self.part.Q, tol, maxp, tag)
+            else:
+                tr.exchange(SET_DIRECTION, 1)
+                for s, sl in zip(own, slots):
+                    s.cg_matvec_dev(ctl, sl)
+                decide(1)
+                for s, sl in zip(own, slots):
+                    s.cg_update_dev(ctl, sl)
+                decide(2)
+                for s in own:
+                    s.cg_direction_dev(ctl)
+                g.post(tag)
+            if g.read(tag - 1)[CG_ACTIVE] == 0.0:
+                break
+        for s in own:
+            s.cg_finish_dev(ctl)
+        c = g.read(tag)
+        st = int(c[CG_STATUS])
+        if st == CG_NONFINITE:
+            self.status = "nonfinite"
+        elif st == CG_NOT_CONVERGED:
+            self.status = "cg_not_converged"
+        return int(c[CG_PRODUCTS])
+
+    def _sweep_solve(self, index, g, own, slots, decide, graph, handles) -> int:
+        ctl, maxp, tol = g.ctl, self.max_iters, self.tol
+        for s, sl in zip(own, slots):
+            s.cg_sweep_rhs_dev(index, sl)
+        decide(3)
+        tag = 0
+        g.post(tag)
+        for k in range(maxp):
+            tag += 1
+            if graph:
+                g.sweep_product(handles, self.part.P, self.part.Q, tol, maxp, k, tag)
+            else:
+                self.tr.exchange(SET_CG_ODD if k & 1 else SET_CG_EVEN, 2)
+                for s, sl in zip(own, slots):
+                    s.cg_sweep_iter_dev(ctl, sl)
+                decide(4)
+                g.post(tag)
+            if g.read(tag - 1)[CG_ACTIVE] == 0.0:
+                break
+        for s in own:
+            s.cg_sweep_finish_dev(ctl)
+        c = g.read(tag)
+        st = int(c[CG_STATUS])
+        if st == CG_NONFINITE:
+            self.status = "nonfinite"
+        elif st == CG_NOT_CONVERGED:
+            self.status = "cg_not_converged"
+        return int(c[CG_PRODUCTS])
+
+    def close(self):
+        """Release the decision group (the subdomains belong to the caller)."""
+        if self._group is not None:
+            self._group.close()
+            self._group = None
 
     def step(self, dt: float = 0.0, alpha: float | None = None):
         """One IMEX step; dt <= 0 takes the CFL step. alpha defaults to (dt * eta) * g (the matrix
@@ -516,4 +811,4 @@ class DecomposedRun:
 
 
 __all__ = ["Partition", "GpuSubdomain", "LocalTransport", "DistTransport", "DecomposedRun", "HALO",
-           "MHDError"]
+           "MHDError", "DeviceCgGroup", "HostCgGroup"]

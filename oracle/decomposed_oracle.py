@@ -197,3 +197,24 @@ class OracleSubdomain:
 
     def cg_zero_solution(self):
         self.x[self.I] = 0.0
+
+    # -- the same phases with the decisions in a control block (slot: this subdomain's 4 sums,
+    # ctl: the control block; both numpy arrays of a host decision group)
+    def cg_rhs_dev(self, index, slot):
+        slot[:2] = self.cg_rhs(index)
+
+    def cg_matvec_dev(self, ctl, slot):
+        if ctl[0] != 0.0:
+            slot[0] = self.cg_matvec()[0]
+
+    def cg_update_dev(self, ctl, slot):
+        if ctl[0] != 0.0:
+            slot[:2] = self.cg_update(float(ctl[6]))
+
+    def cg_direction_dev(self, ctl):
+        if ctl[0] != 0.0:
+            self.cg_direction(float(ctl[7]))
+
+    def cg_finish_dev(self, ctl):
+        if ctl[1] == 2.0:  # non-finite
+            self.cg_zero_solution()

@@ -5,7 +5,9 @@ on the extended planes), against the single-domain C oracle step (oracle/mhd_ora
 
 * in one process, 2 x 2 and 3 x 1 subdomains (LocalTransport);
 * over two gloo ranks on 127.0.0.1, one subdomain per rank (DistTransport): a 2 x 1 and a 1 x 2
-  split, so both axes exchange across ranks and along the other axis with themselves.
+  split, so both axes exchange across ranks and along the other axis with themselves;
+* the solve's decisions in a control block (the library's rules, mhd_subcg_decide_host) against
+  the host's decisions: bit-identical states and products, and the rules' edge cases.
 
 Tolerances: dt to 1e-14 relative, fields to 1e-12 relative L-infinity (the stand-in sums the
 decomposed dot products in another order than the oracle's CG, and forms the stages in the GPU's
@@ -45,8 +47,8 @@ def _check(got, dts, prods, want, want_dts, want_prods):
     assert max(errs) <= 1e-12, errs
 
 
-@pytest.mark.parametrize("P,Q", [(2, 2), (3, 1)])
-def test_local_decomposition_matches_single_domain(P, Q):
+@pytest.mark.parametrize("P,Q,device_decisions", [(2, 2, True), (3, 1, True), (2, 2, False)])
+def test_local_decomposition_matches_single_domain(P, Q, device_decisions):
     from magnetohydrodynamics_simulator_b200.decomposed import DecomposedRun, LocalTransport, Partition
     from oracle.decomposed_oracle import OracleSubdomain
 
@@ -54,7 +56,8 @@ def test_local_decomposition_matches_single_domain(P, Q):
     ic = smooth_state(NX, NY, dx, dy, seed=21)
     part = Partition(NX, NY, P, Q)
     subs = [OracleSubdomain(*part.shape(i), dx, dy, ETA) for i in range(part.count)]
-    run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, ETA)
+    run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, ETA, device_decisions=device_decisions)
+    assert (run._group is not None) == device_decisions
     run.set_state(ic)
     dts, prods = [], []
     for _ in range(3):
@@ -66,6 +69,81 @@ def test_local_decomposition_matches_single_domain(P, Q):
     assert run.status == "ok"
     rms, mx = run.divb()
     assert abs(mx - want_divb[1]) <= 1e-12 and abs(rms - want_divb[0]) <= 1e-12
+
+
+def test_control_block_decisions_are_the_hosts():
+    """The same 3 CFL steps with the decisions in a control block and on the host: identical bits."""
+    from magnetohydrodynamics_simulator_b200.decomposed import DecomposedRun, LocalTransport, Partition
+    from oracle.decomposed_oracle import OracleSubdomain
+
+    dx, dy = 2 * np.pi / NX, 1.7 * np.pi / NY
+    ic = smooth_state(NX, NY, dx, dy, seed=5)
+    part = Partition(NX, NY, 2, 2)
+    res = []
+    for mode in (True, False):
+        subs = [OracleSubdomain(*part.shape(i), dx, dy, ETA) for i in range(part.count)]
+        run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, ETA, device_decisions=mode)
+        run.set_state(ic)
+        steps = [run.step() for _ in range(3)]
+        res.append((steps, run.get_state()))
+    assert res[0][0] == res[1][0]
+    for a, b in zip(res[0][1], res[1][1]):
+        assert np.array_equal(a, b)
+
+
+def test_control_block_rules():
+    """mhd_subcg_decide_host: Eigen's rules over the slots added in order (zero and non-finite
+    right-hand sides, the threshold, the product cap, alpha and beta)."""
+    import ctypes
+
+    from magnetohydrodynamics_simulator_b200.capi import load_library
+    from magnetohydrodynamics_simulator_b200.decomposed import HostCgGroup, _bind
+
+    lib = _bind(load_library())
+    g = HostCgGroup(lib, 3)
+
+    def run(phase, sums, tol=1e-3, maxp=3):
+        for i, v in enumerate(sums):
+            g.slot(i)[:len(v)] = v
+        g.decide(phase, tol, maxp)
+        return g.ctl.copy()
+
+    c = run(0, [[0.0, 0.0]] * 3)
+    assert c[0] == 0.0 and c[1] == 0 and c[2] == 0  # b = 0: no product
+    c = run(0, [[1.0, 0.5], [np.nan, 0.0], [1.0, 0.5]])
+    assert c[0] == 0.0 and c[1] == 2  # non-finite right-hand side
+    c = run(0, [[1.0, 0.5], [2.0, 0.25], [4.0, 1.0]])
+    assert c[0] == 1.0 and c[3] == 7.0 and c[5] == 1.75 and c[4] == 1e-3 * 1e-3 * 7.0
+    c = run(1, [[0.5], [0.25], [0.125]])
+    assert c[6] == 1.75 / 0.875  # alpha = r.z / p.q
+    c = run(2, [[1.0, 0.7], [1.0, 0.0], [1.0, 0.0]])
+    assert c[0] == 1.0 and c[2] == 1 and c[7] == 0.7 / 1.75 and c[5] == 0.7  # beta, new r.z
+    c = run(2, [[1e-7, 0.1], [0.0, 0.0], [0.0, 0.0]])
+    assert c[0] == 0.0 and c[1] == 0 and c[2] == 2  # converged: |r|^2 below tol^2 |b|^2
+    run(0, [[1.0, 1.0], [1.0, 1.0], [1.0, 1.0]])
+    for k in range(3):
+        run(1, [[1.0], [0.0], [0.0]])
+        c = run(2, [[1.0, 1.0], [0.0, 0.0], [0.0, 0.0]])
+    assert c[0] == 0.0 and c[1] == 1 and c[2] == 3  # the product cap: not converged
+    c = run(2, [[1.0, 1.0]] * 3)
+    assert c[2] == 3  # an ended solve takes no further decision
+    assert lib.mhd_subcg_decide_host(None, g.slots.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     3, 0, 1e-3, 3) != 0
+
+    # the single-sweep form: phase 3 after the right-hand side (|b|^2, b.z, z.Az), 4 after an
+    # iteration (r.r, r.z, z.Az, z.q) with p.Ap by its recurrence
+    c = run(3, [[1.0, 0.5, 0.25], [2.0, 0.25, 0.25], [4.0, 1.0, 0.5]])
+    assert c[0] == 1.0 and c[3] == 7.0 and c[5] == 1.75 and c[9] == 1.0 and c[6] == 1.75
+    assert c[11] == -1.0 and c[13] == 0.0
+    c = run(4, [[1.0, 0.7, 0.5, 0.25], [0.0, 0.0, 0.0, 0.0], [0.0, 0.0, 0.0, 0.0]])
+    beta = 0.7 / 1.75
+    pap = 0.5 + 2.0 * beta * 0.25 + beta * beta * 1.0
+    assert c[0] == 1.0 and c[2] == 1 and c[11] == 0 and c[12] == 1.75 and c[7] == beta
+    assert c[9] == pap and c[10] == 1.75 and c[6] == 0.7 / pap
+    c = run(4, [[1.0, 0.7, -10.0, 0.0], [0.0] * 4, [0.0] * 4])
+    assert c[0] == 0.0 and c[1] == 2 and c[13] == 1.0  # p.Ap <= 0: breakdown, x = 0
+    c = run(3, [[0.0, 0.0, 0.0]] * 3)
+    assert c[0] == 0.0 and c[13] == 1.0 and c[1] == 0  # zero right-hand side
 
 
 def test_partition_sizes_and_neighbours():
@@ -91,14 +169,14 @@ from magnetohydrodynamics_simulator_b200.decomposed import DecomposedRun, DistTr
 from oracle.decomposed_oracle import OracleSubdomain
 from tests_helpers import smooth_state
 NX, NY, ETA = {nx}, {ny}, {eta}
-P, Q = {P}, {Q}
+P, Q, DEV = {P}, {Q}, {dev}
 dist.init_process_group("gloo", timeout=timedelta(seconds=60))
 rank = dist.get_rank()
 dx, dy = 2 * np.pi / NX, 1.7 * np.pi / NY
 ic = smooth_state(NX, NY, dx, dy, seed=21)
 part = Partition(NX, NY, P, Q)
 sub = OracleSubdomain(*part.shape(rank), dx, dy, ETA)
-run = DecomposedRun(part, DistTransport(part, sub), dx, dy, ETA)
+run = DecomposedRun(part, DistTransport(part, sub), dx, dy, ETA, device_decisions=DEV)
 run.set_state(ic)
 dts, prods = [], []
 for _ in range(3):
@@ -121,11 +199,11 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("P,Q", [(2, 1), (1, 2)])
-def test_two_gloo_ranks_match_single_domain(tmp_path, P, Q):
+@pytest.mark.parametrize("P,Q,dev", [(2, 1, True), (1, 2, False)])
+def test_two_gloo_ranks_match_single_domain(tmp_path, P, Q, dev):
     out = str(tmp_path / "rank0.npz")
     script = tmp_path / "worker.py"
-    script.write_text(WORKER.format(root=ROOT, nx=NX, ny=NY, eta=ETA, P=P, Q=Q, out=out))
+    script.write_text(WORKER.format(root=ROOT, nx=NX, ny=NY, eta=ETA, P=P, Q=Q, dev=dev, out=out))
     port = _free_port()
     procs = []
     for rank in range(2):

@@ -3,6 +3,11 @@ magnetohydrodynamics_simulator_b200.decomposed): P x Q subdomains on one GPU exc
 through device buffers (LocalTransport) -- the ranks of a multi-GPU run emulated in one process --
 against the single-domain context (mhd_step) and the C oracle on the same state.
 
+The solve's decisions are taken on the device (mhd_subcg_*: each product one replayed CUDA graph
+over the subdomains' streams) or on the host; in the same two-sweep form both must give the same
+bits. With device decisions the default form is the single context's single-sweep solver on every
+subdomain's interior.
+
 Tolerances: dt to 1e-14 relative, fields to 1e-12 relative L-infinity (the decomposed solve adds
 its dot products in another order), CG products within 1, |div B|_inf <= 1e-12.
 """
@@ -26,26 +31,45 @@ def m():
     return mod
 
 
-def _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=True):
+_streams = []
+
+
+def _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=True, shared=False, device=True, form=None):
+    """shared: every subdomain on one stream; device: the solve's decisions on the device; form:
+    the solve's form (None: the default)."""
+    import torch
     from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
                                                                 LocalTransport, Partition)
 
     part = Partition(nx, ny, P, Q)
-    subs = [GpuSubdomain(*part.shape(i), dx, dy, eta) for i in range(part.count)]
-    run = DecomposedRun(part, LocalTransport(part, subs, native=native), dx, dy, eta)
+    stream = None
+    if shared:
+        _streams.append(torch.cuda.Stream())
+        stream = _streams[-1].cuda_stream
+    subs = [GpuSubdomain(*part.shape(i), dx, dy, eta, stream=stream) for i in range(part.count)]
+    run = DecomposedRun(part, LocalTransport(part, subs, native=native), dx, dy, eta,
+                        device_decisions=device, cg_form=form)
+    assert (run._group is not None) == device
+    assert run.cg_form == (form or ("sweep" if device else "two_sweep"))
     run.set_state(ic)
     return run, subs
 
 
-@pytest.mark.parametrize("nx,ny,P,Q,steps,native", [(96, 80, 2, 2, 3, True), (70, 45, 3, 2, 2, True),
-                                                    (128, 128, 2, 1, 3, True), (96, 80, 2, 2, 3, False)])
-def test_decomposed_steps_match_single_context(m, nx, ny, P, Q, steps, native):
+@pytest.mark.parametrize("nx,ny,P,Q,steps,native,shared,device,form", [
+    (96, 80, 2, 2, 3, True, False, True, None), (70, 45, 3, 2, 2, True, False, True, None),
+    (128, 128, 2, 1, 3, True, False, True, None), (96, 80, 2, 2, 3, False, False, True, None),
+    (96, 80, 2, 2, 3, True, True, True, None), (96, 80, 1, 2, 3, True, False, True, None),
+    (96, 80, 2, 2, 3, True, False, True, "two_sweep"), (70, 45, 3, 2, 2, True, False, False, None),
+    (96, 80, 2, 2, 3, False, False, False, None)])
+def test_decomposed_steps_match_single_context(m, nx, ny, P, Q, steps, native, shared, device, form):
     """native: rings by mhd_sub_exchange_local; otherwise through mhd_sub_pack / mhd_sub_unpack
-    buffers (the path strips take between GPUs)."""
+    buffers (the path strips take between GPUs). shared: the subdomains on one stream. device:
+    decisions on the device (with native rings: one graph per product). form: the solve's form."""
     dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
     eta = 0.02
     ic = smooth_state(nx, ny, dx, dy, seed=nx + ny)
-    run, subs = _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=native)
+    run, subs = _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=native, shared=shared, device=device,
+                            form=form)
     ctx = m.Context(nx, ny, dx, dy, eta)
     ctx.set_state(ic)
     orc = Oracle(nx, ny, dx, dy, eta)
@@ -68,8 +92,31 @@ def test_decomposed_steps_match_single_context(m, nx, ny, P, Q, steps, native):
     assert mx <= 1e-12
     assert abs(mx - ctx.divb()[1]) <= 1e-13
     ctx.close()
+    run.close()
     for s in subs:
         s.close()
+
+
+def test_device_decisions_are_the_hosts(m):
+    """Decisions on the device and on the host: the same dts, products and bits, over steps whose
+    solves take several products."""
+    nx, ny = 96, 80
+    dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
+    eta = 0.05
+    ic = smooth_state(nx, ny, dx, dy, seed=3)
+    res = []
+    for device in (True, False):
+        run, subs = _decomposed(m, nx, ny, dx, dy, eta, 2, 2, ic, device=device, form="two_sweep")
+        steps = [run.step() for _ in range(3)]
+        res.append((steps, run.get_state(), run.status))
+        run.close()
+        for s in subs:
+            s.close()
+    assert res[0][0] == res[1][0]
+    assert all(k > 1 for _, ks in res[0][0] for k in ks)
+    assert res[0][2] == res[1][2] == "ok"
+    for a, b in zip(res[0][1], res[1][1]):
+        assert np.array_equal(a, b)
 
 
 def test_decomposed_orszag_tang_matches_reference_goldens(m):
@@ -93,3 +140,42 @@ def test_decomposed_orszag_tang_matches_reference_goldens(m):
     ctx.close()
     for s in subs:
         s.close()
+
+
+@pytest.mark.parametrize("form", ["sweep", "two_sweep"])
+def test_decomposed_solve_edges_match_single_context(m, form):
+    """A capped solve (2 products, not converged: the single-sweep form ends on an even iteration
+    after k = 1 and on an odd one for the cap 3) and a zero right-hand side (eta = 0: x = 0, no
+    product), against the single context with the same rules."""
+    import torch
+    from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
+                                                                LocalTransport, Partition)
+
+    nx, ny = 96, 80
+    dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
+    ic = smooth_state(nx, ny, dx, dy, seed=9)
+    for eta, cap in ((0.05, 2), (0.05, 3), (0.0, 0)):
+        part = Partition(nx, ny, 2, 2)
+        subs = [GpuSubdomain(*part.shape(i), dx, dy, eta) for i in range(part.count)]
+        run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, eta, cg_max_iters=cap, cg_form=form)
+        run.set_state(ic)
+        ctx = m.Context(nx, ny, dx, dy, eta, cg_max_iters=cap)
+        ctx.set_state(ic)
+        dt = ctx.cfl_dt()
+        _, prods = run.step(dt)
+        ctx.step(dt)
+        assert ctx.synchronize_status() == (4 if cap else 0)  # MHD_ERR_CG_NOT_CONVERGED when capped
+        want = ctx.last_cg_products()
+        if cap:
+            assert tuple(prods) == (cap, cap) == tuple(want), (prods, want)
+            assert run.status == "cg_not_converged"
+        else:
+            assert tuple(prods) == (0, 0) == tuple(want)
+            assert run.status == "ok"
+        errs = [rel_linf(g, w, 1.0) for g, w in zip(run.get_state(), ctx.get_state())]
+        assert max(errs) <= 1e-12, (eta, cap, errs)
+        torch.cuda.synchronize()
+        run.close()
+        ctx.close()
+        for s in subs:
+            s.close()
