@@ -899,12 +899,32 @@ def run_profile_case(args):
     adjoint  the 1024^2 state of the "adjoint" section, one 10-step trajectory (one checkpoint
              segment): forward, then backward;
     snapshot the Orszag-Tang state at 2048^2 (201 MB, above the L2), one step, then one snapshot
-             packed on the device and copied to the host (mhd_snapshot_pack, 235 MB)."""
+             packed on the device and copied to the host (mhd_snapshot_pack, 235 MB);
+    decomposed  Orszag-Tang 2048^2 split 2 x 2 on one GPU (the default single-sweep solve with
+             device decisions), one warm-up step and two CFL steps."""
     import torch
 
     import magnetohydrodynamics_simulator_b200 as m
 
     torch.cuda.set_device(0)
+    if args.profile_case == "decomposed":
+        from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
+                                                                    LocalTransport, Partition)
+
+        n = 2048
+        state, dx = make_state(n)
+        part = Partition(n, n, 2, 2)
+        subs = [GpuSubdomain(*part.shape(i), dx, dx, ETA) for i in range(part.count)]
+        run = DecomposedRun(part, LocalTransport(part, subs), dx, dx, ETA, courant=COURANT)
+        run.set_state(state)
+        for _ in range(3):
+            run.step()
+        torch.cuda.synchronize()
+        ok = run.status == "ok"
+        run.close()
+        for sd in subs:
+            sd.close()
+        return 0 if ok else 1
     if args.profile_case == "snapshot":
         n = 2048
         state, dx = make_state(n)
@@ -972,7 +992,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
     ap.add_argument("--no-decomposed", action="store_true")
-    ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot"), default=None,
+    ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot", "decomposed"), default=None,
                     help="run a small fixed case for a profiler and exit (no measurement)")
     args = ap.parse_args()
     if args.profile_case:

@@ -286,6 +286,37 @@ __global__ void __launch_bounds__(kSubNT) k_sub_zero_interior(Interior v, double
 // iteration (the set MHD_SUB_SET_CG_EVEN / _ODD); their wrapped ring values are never used.
 // Vectors: r[0] = r, r[1] = z, p[0] = p, p[1] = q of the subdomain.
 
+// Publish this block's 4 partials; the last block to arrive adds every block's partials in the
+// fixed order of k_sub_final (lane-strided, then a butterfly) into slot[0..3] and resets the
+// arrival counter for the next launch.
+__device__ __forceinline__ void sub_sums_to_slot(const double (&acc)[4], double* part, unsigned* arrivals,
+                                                 double* slot) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) part[(size_t)blockIdx.x * 4 + c] = acc[c];
+        __threadfence();
+        last = atomicAdd(arrivals, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    const int l = threadIdx.x;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = l; b < (int)gridDim.x; b += 32) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) s[c] += __ldcg(&part[(size_t)b * 4 + c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(0xffffffffu, s[c], o);
+    if (l == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) slot[c] = s[c];
+        *arrivals = 0u;
+    }
+}
+
 __device__ __forceinline__ CgScal sub_cg_scal(const SubScal* sp) {
     CgScal s;
     s.cx = sp->cx;
@@ -300,7 +331,8 @@ __device__ __forceinline__ CgScal sub_cg_scal(const SubScal* sp) {
 
 // b = eta J_z(B*), r0 = b on the interior; block partials |b|^2, b.z0, z0.A z0.
 __global__ void __launch_bounds__(kSubCgNT, 2)
-k_sub_cg_sweep_rhs(CgSweepArgs a, const SubScal* __restrict__ sp, double* part) {
+k_sub_cg_sweep_rhs(CgSweepArgs a, const SubScal* __restrict__ sp, double* part, unsigned* arrivals,
+                   double* slot) {
     extern __shared__ __align__(16) double sub_ring_mem[];
     __shared__ double red[kSubCgNT / 32 * 4];
     double* const ring = sub_ring_mem + (size_t)(threadIdx.x >> 5) * CG_RING * CG_SLOT;
@@ -312,16 +344,14 @@ k_sub_cg_sweep_rhs(CgSweepArgs a, const SubScal* __restrict__ sp, double* part) 
         cg_rhs_segment<true>(a, s, sx, r0w, min(r0w + a.seg_h, rend), 1, a.r[0], ring, acc);
     }
     block_sum<kSubCgNT, 4>(acc, red);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) part[(size_t)blockIdx.x * 4 + c] = acc[c];
-    }
+    sub_sums_to_slot(acc, part, arrivals, slot);
 }
 
 // Iteration k = products so far (from the control block, which also gives alpha, beta and
 // alpha_{k-1}); nothing once the solve has ended. Block partials r.r, r.z, z.Az, z.q_k.
 __global__ void __launch_bounds__(kSubCgNT, 2)
-k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double* ctl, double* part) {
+k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double* ctl, double* part,
+                    unsigned* arrivals, double* slot) {
     if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
     extern __shared__ __align__(16) double sub_ring_mem[];
     __shared__ double red[kSubCgNT / 32 * 4];
@@ -353,10 +383,7 @@ k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double*
             cg_iter_segment<false, kXPair, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
     }
     block_sum<kSubCgNT, 4>(acc, red);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) part[(size_t)blockIdx.x * 4 + c] = acc[c];
-    }
+    sub_sums_to_slot(acc, part, arrivals, slot);
 }
 
 // The end of a single-sweep solve (as k_cg_sweep's): x = 0 after a zero right-hand side or a
@@ -588,6 +615,7 @@ struct mhd_subdomain {
     int blocks = 0;     // grid of the per-cell interior kernels
     CgSweepArgs cga{};  // the single-sweep solve's sweep: the interior's strips and row segments
     int cg_blocks = 0;
+    unsigned* arrivals = nullptr;  // blocks of the running sweep that have published their sums
     int pending_sums = 0;  // sums enqueued by a CG phase without an output pointer
     cudaEvent_t ev_ready = nullptr;  // in-process exchange: this subdomain's strips may be read
     cudaEvent_t ev_done = nullptr;   // in-process exchange: this subdomain's rings are filled
@@ -861,6 +889,7 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
         cudaMalloc(&s->coeffs, sizeof(StepCoeffs)) != cudaSuccess ||
         cudaMalloc(&s->scratch_status, sizeof(DeviceStatus)) != cudaSuccess ||
         cudaMalloc(&s->sc, sizeof(SubScal)) != cudaSuccess ||
+        cudaMalloc(&s->arrivals, sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&s->part, (size_t)4 * kSubMaxBlocks * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&s->dev_out, 8 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&s->host_out, 8 * sizeof(double)) != cudaSuccess) {
@@ -913,6 +942,7 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
         cudaMemsetAsync(s->coeffs, 0, sizeof(StepCoeffs), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->scratch_status, 0, sizeof(DeviceStatus), s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->sc, 0, sizeof(SubScal), s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->arrivals, 0, sizeof(unsigned), s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess)
         return fail(MHD_ERR_CUDA);
     *out = s;
@@ -927,6 +957,7 @@ mhd_status mhd_sub_destroy(mhd_subdomain* s) {
     cudaFree(s->coeffs);
     cudaFree(s->scratch_status);
     cudaFree(s->sc);
+    cudaFree(s->arrivals);
     cudaFree(s->part);
     cudaFree(s->dev_out);
     if (s->host_out) cudaFreeHost(s->host_out);
@@ -1266,9 +1297,8 @@ mhd_status mhd_sub_cg_sweep_rhs_dev(mhd_subdomain* s, int solve_index, double* s
     CgSweepArgs a = s->cga;
     a.bxf = solve_index == 0 ? s->T[4] : s->A[4];
     a.byf = solve_index == 0 ? s->T[5] : s->A[5];
-    k_sub_cg_sweep_rhs<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(a, s->sc, s->part);
-    MHD_TRY(cudaGetLastError());
-    k_sub_final<4><<<1, 32, 0, s->stream>>>(s->part, s->cg_blocks, slot);
+    k_sub_cg_sweep_rhs<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(a, s->sc, s->part, s->arrivals,
+                                                                                slot);
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
 }
@@ -1277,9 +1307,8 @@ mhd_status mhd_sub_cg_sweep_iter_dev(mhd_subdomain* s, const double* ctl, double
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
     if (!ctl || !slot) return MHD_ERR_INVALID_ARGUMENT;
-    k_sub_cg_sweep_iter<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(s->cga, s->sc, ctl, s->part);
-    MHD_TRY(cudaGetLastError());
-    k_sub_final<4><<<1, 32, 0, s->stream>>>(s->part, s->cg_blocks, slot);
+    k_sub_cg_sweep_iter<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(s->cga, s->sc, ctl, s->part,
+                                                                                 s->arrivals, slot);
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
 }
