@@ -233,3 +233,13 @@ def test_gpu_subdomain_refuses_without_device():
 
     with pytest.raises(MHDError):
         GpuSubdomain(16, 16, 0.1, 0.1, 0.01)
+    from magnetohydrodynamics_simulator_b200.capi import load_library
+    from magnetohydrodynamics_simulator_b200.decomposed import DeviceCgGroup, _bind
+
+    lib = _bind(load_library())
+    with pytest.raises(MHDError):
+        DeviceCgGroup(lib, 4, 0)  # the device decision group too
+    # argument checks of the device entry points come before any device call
+    assert lib.mhd_sub_cg_sweep_iter_dev(None, None, None) != 0
+    assert lib.mhd_subcg_sweep_product(None, None, 2, 2, 1e-3, 10, 0, 1) != 0
+    assert lib.mhd_subcg_decide_on(None, None, 0, 1e-3, 10) != 0
