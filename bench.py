@@ -427,12 +427,37 @@ def run_gpu_arm(args):
             return None
         return tr[key]["bytes_per_zone_per_unit"] * units * zones
 
+    # FP64-pipe bound of each kernel from its ncu-counted FP64 thread instructions per zone: B200
+    # issues 64 per SM and clock (148 SMs at the 1965 MHz maximum SM clock)
+    fi = {}
+    fi_path = os.path.join(ROOT, "profiles", "fp64_inst_per_zone.json")
+    if os.path.exists(fi_path):
+        try:
+            with open(fi_path) as f:
+                fi = json.load(f)
+        except Exception:
+            fi = {}
+
+    def fp64_of(name, ms, alg):
+        _, _, _, key, units = funcs[name]
+        if key not in fi:
+            return None
+        inst = fi[key]["fp64_thread_inst_per_zone_per_unit"] * units * zones
+        rate_peak = fi.get("fp64_thread_inst_per_sm_per_clock", 64) * 148 * 1965e6
+        t_fp64 = inst / rate_peak
+        t_hbm = alg / (peak * 1e9)
+        return {"thread_inst_per_launch": inst, "achieved_inst_per_s": inst / (ms * 1e-3),
+                "peak_inst_per_s": rate_peak, "frac": t_fp64 / (ms * 1e-3),
+                "flops_per_launch": fi[key]["flops_per_zone_per_unit"] * units * zones,
+                "binding_roofline": "fp64" if t_fp64 > t_hbm else "hbm",
+                "hbm_frac_at_fp64_peak": min(1.0, t_hbm / t_fp64)}
+
     def figures(name):
         alg, ms, launches, _, _ = funcs[name]
         gbs = alg / (ms * 1e-3) / 1e9
         return {"kernel": name, "launches_per_step": launches, "share_of_step": shares[name],
                 "alg_bytes_per_launch": alg, "ms_per_launch": ms, "achieved": gbs, "frac": gbs / peak,
-                "traffic": traffic_of(name)}
+                "traffic": traffic_of(name), "fp64_pipe": fp64_of(name, ms, alg)}
 
     dom = figures(dominant)
     longest_name = {"stage1": "k_stage_sweep<1>", "cg1": "k_cg_sweep", "stage2": "k_stage_sweep<2>",
@@ -901,12 +926,24 @@ def run_profile_case(args):
     snapshot the Orszag-Tang state at 2048^2 (201 MB, above the L2), one step, then one snapshot
              packed on the device and copied to the host (mhd_snapshot_pack, 235 MB);
     decomposed  Orszag-Tang 2048^2 split 2 x 2 on one GPU (the default single-sweep solve with
-             device decisions), one warm-up step and two CFL steps."""
+             device decisions), one warm-up step and two CFL steps;
+    step     the Orszag-Tang state at 2048^2 (201 MB, above the L2), two CFL steps of a single
+             context (the headline workload's kernels at a quarter of its zones)."""
     import torch
 
     import magnetohydrodynamics_simulator_b200 as m
 
     torch.cuda.set_device(0)
+    if args.profile_case == "step":
+        n = 2048
+        state, dx = make_state(n)
+        ctx = m.Context(n, n, dx, dx, ETA, courant=COURANT)
+        ctx.set_state(state)
+        for _ in range(2):
+            ctx.step(0.0)
+        st = ctx.synchronize_status()
+        ctx.close()
+        return 0 if st == 0 else 1
     if args.profile_case == "decomposed":
         from magnetohydrodynamics_simulator_b200.decomposed import (DecomposedRun, GpuSubdomain,
                                                                     LocalTransport, Partition)
@@ -992,7 +1029,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
     ap.add_argument("--no-decomposed", action="store_true")
-    ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot", "decomposed"), default=None,
+    ap.add_argument("--profile-case", choices=("batched", "adjoint", "snapshot", "decomposed", "step"), default=None,
                     help="run a small fixed case for a profiler and exit (no measurement)")
     args = ap.parse_args()
     if args.profile_case:
