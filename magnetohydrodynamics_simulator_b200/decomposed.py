@@ -512,6 +512,8 @@ class DistTransport:
         return buf
 
     def exchange(self, set_: int, width: int):
+        if isinstance(self.sub, GpuSubdomain):
+            return self._exchange_stream_ordered(set_, width)
         for axis in ((EAST, WEST), (NORTH, SOUTH)):
             for side in axis:
                 # shift toward `side`: send this side's strip to that neighbour, receive the strip
@@ -534,6 +536,27 @@ class DistTransport:
                     self.torch.cuda.current_stream().synchronize()
                 self.sub.unpack(set_, OPPOSITE[side], width, rt.numpy() if isinstance(send, np.ndarray) else rt)
             self.sub.synchronize()
+
+    def _exchange_stream_ordered(self, set_: int, width: int):
+        """The same shifts for a GPU subdomain with every step on its stream: pack, the NCCL
+        transfer (issued with the subdomain's stream as torch's current stream, which then waits
+        for it) and unpack follow one another on the device without a host wait. The strips travel
+        in the subdomain's persistent pack and receive buffers."""
+        torch = self.torch
+        with torch.cuda.stream(torch.cuda.ExternalStream(self.sub.stream)):
+            for axis in ((EAST, WEST), (NORTH, SOUTH)):
+                for side in axis:
+                    send = self.sub.pack(set_, side, width)
+                    dst = self.part.neighbour(self.rank, side)
+                    src = self.part.neighbour(self.rank, OPPOSITE[side])
+                    if dst == self.rank:
+                        self.sub.unpack(set_, OPPOSITE[side], width, send)
+                        continue
+                    recv = self.sub.recv_buffer(set_, OPPOSITE[side], width)
+                    ops = [self.dist.P2POp(self.dist.isend, send, dst), self.dist.P2POp(self.dist.irecv, recv, src)]
+                    for req in self.dist.batch_isend_irecv(ops):
+                        req.wait()
+                    self.sub.unpack(set_, OPPOSITE[side], width, recv)
 
     def _gather(self, values) -> np.ndarray:
         t = self.torch.tensor(values, dtype=self.torch.float64, device=self.device)

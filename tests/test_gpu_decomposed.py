@@ -179,3 +179,83 @@ def test_decomposed_solve_edges_match_single_context(m, form):
         ctx.close()
         for s in subs:
             s.close()
+
+
+NCCL_WORKER = r"""
+import os, sys
+sys.path.insert(0, {root!r})
+sys.path.insert(0, os.path.join({root!r}, "tests"))
+from datetime import timedelta
+import numpy as np
+import torch
+import torch.distributed as dist
+from magnetohydrodynamics_simulator_b200.decomposed import DecomposedRun, DistTransport, GpuSubdomain, Partition
+from tests_helpers import smooth_state
+torch.cuda.set_device(0)
+dist.init_process_group("nccl", timeout=timedelta(seconds=60))
+nx, ny, eta = {nx}, {ny}, {eta}
+dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
+part = Partition(nx, ny, 1, 1)
+out = {{}}
+for dev in (True, False):
+    sub = GpuSubdomain(nx, ny, dx, dy, eta)
+    run = DecomposedRun(part, DistTransport(part, sub, device=torch.device("cuda")), dx, dy, eta,
+                        device_decisions=dev)
+    run.set_state(smooth_state(nx, ny, dx, dy, seed=4))
+    steps = [run.step() for _ in range(3)]
+    st = run.get_state()
+    out[f"dts_{{dev}}"] = np.array([d for d, _ in steps])
+    out[f"prods_{{dev}}"] = np.array([k for _, k in steps])
+    out[f"form_{{dev}}"] = run.cg_form
+    out[f"status_{{dev}}"] = run.status
+    for k in range(6):
+        out[f"f{{k}}_{{dev}}"] = st[k]
+    run.close()
+    sub.close()
+torch.cuda.synchronize()
+dist.barrier()
+dist.destroy_process_group()
+np.savez({out!r}, **out)
+print("ok")
+"""
+
+
+def test_distributed_transport_one_nccl_rank_matches_single_context(m, tmp_path):
+    """The DistTransport path on one GPU: one NCCL rank owning the whole grid (its rings come from
+    itself), with the solve's decisions on the device (the sum slots all-gathered over NCCL on the
+    subdomain's stream, the single-sweep form) and on the host (the two-sweep form), against the
+    single context stepped with the same dts."""
+    import os
+    import socket
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    nx, ny, eta = 96, 80, 0.03
+    out = str(tmp_path / "nccl1.npz")
+    script = tmp_path / "worker.py"
+    script.write_text(NCCL_WORKER.format(root=ROOT, nx=nx, ny=ny, eta=eta, out=out))
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0", MASTER_ADDR="127.0.0.1",
+               MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0")
+    p = subprocess.run([sys.executable, str(script)], env=env, stdout=subprocess.PIPE,
+                       stderr=subprocess.STDOUT, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout[-3000:]
+    d = np.load(out)
+    dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
+    for dev in (True, False):
+        assert str(d[f"form_{dev}"]) == ("sweep" if dev else "two_sweep")
+        assert str(d[f"status_{dev}"]) == "ok"
+        ctx = m.Context(nx, ny, dx, dy, eta)
+        ctx.set_state(smooth_state(nx, ny, dx, dy, seed=4))
+        for dt, k in zip(d[f"dts_{dev}"], d[f"prods_{dev}"]):
+            assert abs(ctx.cfl_dt() - dt) <= 1e-14 * dt
+            ctx.step(float(dt))
+            ctx.synchronize()
+            assert all(abs(a - b) <= 1 for a, b in zip(k, ctx.last_cg_products()))
+        errs = [rel_linf(d[f"f{k}_{dev}"], w, 1.0) for k, w in enumerate(ctx.get_state())]
+        assert max(errs) <= 1e-12, (dev, errs)
+        ctx.close()
