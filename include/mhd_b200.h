@@ -443,7 +443,8 @@ mhd_status mhd_subcg_decide_host(double* ctl, const double* slots, int count, in
  * mhd_subcg_product enqueues one whole product of the solve -- the exchange of p's 1-cell ring
  * (mhd_sub_exchange_local), cg_matvec_dev, decision 1, cg_update_dev, decision 2,
  * cg_direction_dev on all P x Q subdomains -- as one CUDA graph on the group's stream, captured at
- * the first call for these arguments and replayed after, then posts the control block under `tag`. */
+ * the first call for these arguments and replayed after, then posts the control block under `tag`.
+ * The subdomains' streams must not be the legacy default stream (MHD_ERR_INVALID_ARGUMENT). */
 mhd_status mhd_subcg_decide_on(mhd_subcg* g, mhd_subdomain* const* subs, int phase, double tol,
                                long long max_products);
 mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,

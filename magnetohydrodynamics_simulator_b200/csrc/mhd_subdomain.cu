@@ -30,6 +30,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <new>
 #include <vector>
 
@@ -620,6 +621,7 @@ struct mhd_subdomain {
     cudaEvent_t ev_ready = nullptr;  // in-process exchange: this subdomain's strips may be read
     cudaEvent_t ev_done = nullptr;   // in-process exchange: this subdomain's rings are filled
     cudaEvent_t ev_phase = nullptr;  // a decision group waits for this subdomain's work so far
+    unsigned long long uid = 0;      // unique per creation (a freed subdomain's address may recur)
 };
 
 // Device-resident decisions of one decomposed solve (mhd_subcg_*): the control block, the
@@ -633,7 +635,7 @@ struct mhd_subcg {
     // one product of the solve captured as a CUDA graph (mhd_subcg_product), for these arguments
     cudaGraphExec_t product = nullptr;
     cudaGraphExec_t sweep[2]{};  // one iteration of the single-sweep form, even and odd k
-    std::vector<mhd_subdomain*> product_subs;
+    std::vector<unsigned long long> product_subs;  // uids of the subdomains the graphs were captured for
     int product_P = 0, product_Q = 0;
     double product_tol = 0.0;
     long long product_max = 0;
@@ -834,6 +836,8 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
         mhd_sub_destroy(s);
         return st;
     };
+    static std::atomic<unsigned long long> next_uid{1};
+    s->uid = next_uid.fetch_add(1);
     s->prm = *p;
     s->iv.nx = p->nx;
     s->iv.ny = p->ny;
@@ -1432,12 +1436,13 @@ mhd_status check_graph_args(mhd_subcg* g, mhd_subdomain* const* subs, int P, int
                             long long max_products) {
     if (!g || !subs || P < 1 || Q < 1 || P * Q != g->count || !(tol >= 0) || max_products < 1)
         return MHD_ERR_INVALID_ARGUMENT;
+    // a captured graph joins the subdomains' streams, which the legacy default stream cannot
     for (int i = 0; i < g->count; ++i)
-        if (!subs[i] || subs[i]->device != g->device) return MHD_ERR_INVALID_ARGUMENT;
+        if (!subs[i] || subs[i]->device != g->device || !subs[i]->stream) return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaSetDevice(g->device));
-    const bool same = !g->product_subs.empty() && g->product_P == P && g->product_Q == Q &&
-                      g->product_tol == tol && g->product_max == max_products &&
-                      std::equal(g->product_subs.begin(), g->product_subs.end(), subs);
+    bool same = !g->product_subs.empty() && g->product_P == P && g->product_Q == Q &&
+                g->product_tol == tol && g->product_max == max_products;
+    for (int i = 0; i < g->count && same; ++i) same = g->product_subs[i] == subs[i]->uid;
     if (!same) {
         if (g->product) cudaGraphExecDestroy(g->product);
         g->product = nullptr;
@@ -1445,7 +1450,8 @@ mhd_status check_graph_args(mhd_subcg* g, mhd_subdomain* const* subs, int P, int
             if (e) cudaGraphExecDestroy(e);
             e = nullptr;
         }
-        g->product_subs.assign(subs, subs + g->count);
+        g->product_subs.resize(g->count);
+        for (int i = 0; i < g->count; ++i) g->product_subs[i] = subs[i]->uid;
         g->product_P = P;
         g->product_Q = Q;
         g->product_tol = tol;
