@@ -536,6 +536,7 @@ mhd_status mhd_adj_set_eta(mhd_adjoint* a, double eta) {
 }
 
 mhd_status mhd_adj_forward(mhd_adjoint* a, const double* const u0[6], double* const uT[6]) {
+    MHD_NVTX_RANGE("mhd_adj_forward");
     mhd_status s = check_adj(a);
     if (s != MHD_OK) return s;
     if (!u0 || !uT) return MHD_ERR_INVALID_ARGUMENT;
@@ -559,6 +560,7 @@ mhd_status mhd_adj_forward(mhd_adjoint* a, const double* const u0[6], double* co
 
 mhd_status mhd_adj_backward(mhd_adjoint* a, const double* const grad_uT[6], double* const grad_u0[6],
                             double* grad_eta) {
+    MHD_NVTX_RANGE("mhd_adj_backward");
     mhd_status s = check_adj(a);
     if (s != MHD_OK) return s;
     if (!grad_uT || !grad_u0) return MHD_ERR_INVALID_ARGUMENT;

@@ -555,6 +555,7 @@ mhd_status mhd_batch_set_implicit_coefficient(mhd_batch* b, int index, double al
 }
 
 mhd_status mhd_batch_step(mhd_batch* b, const double* dts) {
+    MHD_NVTX_RANGE("mhd_batch_step");
     mhd_status s = check_batch(b);
     if (s != MHD_OK) return s;
     if (!all_states_set(b)) return MHD_ERR_NO_STATE;
@@ -570,6 +571,7 @@ mhd_status mhd_batch_step(mhd_batch* b, const double* dts) {
 
 mhd_status mhd_batch_run(mhd_batch* b, int nsteps, double dt_fixed, double t_end, double* dts_out,
                          long long* prods_out) {
+    MHD_NVTX_RANGE("mhd_batch_run");
     mhd_status s = check_batch(b);
     if (s != MHD_OK) return s;
     if (!all_states_set(b)) return MHD_ERR_NO_STATE;

@@ -513,6 +513,7 @@ static mhd_status ensure_transfer_streams(mhd_context* c) {
 }
 
 mhd_status mhd_set_state(mhd_context* c, const double* const f[6], int layout, int ng) {
+    MHD_NVTX_RANGE("mhd_set_state");
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
     if ((s = join_transfers(c)) != MHD_OK) return s;
@@ -620,6 +621,7 @@ mhd_status mhd_set_state_device(mhd_context* c, const double* const f[6]) {
 }
 
 mhd_status mhd_get_state(mhd_context* c, double* const f[6], int layout, int ng) {
+    MHD_NVTX_RANGE("mhd_get_state");
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
     if (!f || (layout != MHD_LAYOUT_DENSE && layout != MHD_LAYOUT_PADDED) ||
@@ -681,6 +683,7 @@ mhd_status mhd_set_implicit_coefficient(mhd_context* c, double alpha) {
 }
 
 mhd_status mhd_step(mhd_context* c, double dt) {
+    MHD_NVTX_RANGE("mhd_step");
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
     if ((s = join_transfers(c)) != MHD_OK) return s;
@@ -693,6 +696,7 @@ mhd_status mhd_step(mhd_context* c, double dt) {
 
 mhd_status mhd_run(mhd_context* c, int nsteps, double dt_fixed, double t_end, double* dts_out,
                    long long* prods_out) {
+    MHD_NVTX_RANGE("mhd_run");
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
     if ((s = join_transfers(c)) != MHD_OK) return s;
@@ -835,6 +839,7 @@ size_t mhd_snapshot_bytes(mhd_context* c, int ng) {
 
 mhd_status mhd_snapshot_write(mhd_context* c, const char* path, int ng, int snapshot_rate,
                               double dt) {
+    MHD_NVTX_RANGE("mhd_snapshot_write");
     mhd_status s = check_ctx(c);
     if (s != MHD_OK) return s;
     const size_t bytes = mhd_snapshot_bytes(c, ng);

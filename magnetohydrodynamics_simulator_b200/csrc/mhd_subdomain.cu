@@ -1045,6 +1045,7 @@ mhd_status mhd_sub_unpack(mhd_subdomain* s, int set, int side, int width, const 
 }
 
 mhd_status mhd_sub_exchange_local(mhd_subdomain* const* subs, int P, int Q, int set, int width) {
+    MHD_NVTX_RANGE("mhd_sub_exchange_local");
     if (!subs || P < 1 || Q < 1) return MHD_ERR_INVALID_ARGUMENT;
     const int count = P * Q;
     for (int i = 0; i < count; ++i) {
@@ -1144,6 +1145,7 @@ mhd_status mhd_sub_set_step(mhd_subdomain* s, double dt, double alpha) {
 }
 
 mhd_status mhd_sub_stage(mhd_subdomain* s, int stage) {
+    MHD_NVTX_RANGE("mhd_sub_stage");
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
     CPlanes in;
@@ -1473,6 +1475,7 @@ mhd_status replay(mhd_subcg* g, mhd_subdomain* const* subs, cudaGraphExec_t exec
 
 mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
                              long long max_products, int tag) {
+    MHD_NVTX_RANGE("mhd_subcg_product");
     if (tag < 0) return MHD_ERR_INVALID_ARGUMENT;
     mhd_status st = check_graph_args(g, subs, P, Q, tol, max_products);
     if (st != MHD_OK) return st;
@@ -1482,6 +1485,7 @@ mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, in
 
 mhd_status mhd_subcg_sweep_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
                                    long long max_products, int k, int tag) {
+    MHD_NVTX_RANGE("mhd_subcg_sweep_product");
     if (tag < 0 || k < 0) return MHD_ERR_INVALID_ARGUMENT;
     mhd_status st = check_graph_args(g, subs, P, Q, tol, max_products);
     if (st != MHD_OK) return st;
