@@ -489,6 +489,9 @@ def run_gpu_arm(args):
     batched = None
     if not args.no_batch:
         batched = measure_batched(torch, m, args.batch_steps)
+        # the single context's solver on the headline grid, per zone and matrix product
+        batched["solver_work"]["single_context_ps_per_zone_product"] = (
+            solver_ms * 1e9 / (zones * (k1 + k2)))
     adjoint = None
     if not args.no_adjoint:
         adjoint = measure_adjoint(torch, m)
@@ -713,6 +716,12 @@ def measure_batched(torch, m, steps):
     for i, f in enumerate(ics):
         b.set_state(i, f)
     tuning = b.autotune()
+    # the work of the solves in the tuning step: one step of the chosen decomposition from the same
+    # initial states gives every instance's products (the states are set again before timing)
+    b.step()
+    b.synchronize()
+    prods0 = b.last_cg_products()
+    zone_products = float(sum(s["nx"] * s["ny"] * int(p[0] + p[1]) for s, p in zip(insts, prods0)))
     bstream = torch.cuda.ExternalStream(b.stream)
     b.run(4, record=False)  # warm-up (graph capture path included)
     for i, f in enumerate(ics):
@@ -768,6 +777,11 @@ def measure_batched(torch, m, steps):
         "tuning": {k: tuning[k] for k in ("stage_rows", "cg_rows", "cg_order")},
         "tuning_step_ms": {"explicit_kernels": tuning["stage_ms"], "implicit_solves": tuning["cg_ms"],
                            "note": "device time of one autotuning step of the chosen decomposition"},
+        "solver_work": {"zone_products": zone_products,
+                        "mean_products_per_solve": zone_products / (2.0 * zones),
+                        "ps_per_zone_product": tuning["cg_ms"] * 1e9 / zone_products,
+                        "note": "the tuning step's solves: every instance's matrix products times "
+                                "its zones; converged instances drop out of the lockstep"},
         "plain_loop": {"value": zones * steps / (plain_ms * 1e-3), "unit": UNIT,
                        "ms_per_step": plain_ms / steps,
                        "how": "one context per instance on one stream, run(steps) in turn (CUDA graph, "
