@@ -187,16 +187,33 @@ __device__ __forceinline__ void cg_rhs_segment(const CgSweepArgs& a, const CgSca
     cp_async_wait<0>();  // leave no copy in flight into the ring
 }
 
+// A subdomain's 3 x 3 neighbourhood for sweeps that read the cells around its interior straight
+// from the neighbours' interiors instead of its own halo ring (subdomains of one process, on one
+// device): entry a * 3 + b is the subdomain dy = a - 1, dx = b - 1 away (periodic; 4 is itself).
+// A cell west of the interior lies in the west neighbour's last columns, a corner cell in the
+// diagonal neighbour's corner; cells more than `halo` away are clamped to the ring (never used).
+struct CgSubNeighbours {
+    const double* r[2][9];  // the neighbours' r[0], r[1] of the single-sweep solve
+    const double* p[2][9];  // ... and p[0], p[1]
+    int nxe[9];             // their extended row pitch
+    int nx, ny;             // this subdomain's interior
+    int nx_w, ny_s;         // interior columns of the west neighbours, rows of the south ones
+    int halo;               // ring width of the extended planes
+};
+
 // One CG iteration k over rows [r0w, r1w) of column strip sx (the sweep of the header comment).
 // FIRST: k = 0, p_0 = z_0 (p_{-1} is not read). XM: the iteration's CgXMode. acc[0..3] receive r.r, r.z, z.Az, z.q_k of
 // the owned cells. Sweep row t holds grid row jfirst + (t - 2) dir, t = 0 .. nrows + 3; at sweep
 // row t the warp forms p_k of row t, q_k, r_{k+1}, z_{k+1} of row t-1 and A z_{k+1} and the outputs
 // of row t-2. Row t is copied into slot t % CG_RING by the end of sweep row t - 6.
-template <bool FIRST, int XM, bool kSub = false>
+// kNb (with kSub): r_k and p_{k-1} are read from the neighbourhood nb (buffers rsel and psel of
+// each neighbour) rather than from this subdomain's rings; the results are the same.
+template <bool FIRST, int XM, bool kSub = false, bool kNb = false>
 __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgScal& s, int sx, int r0w,
                                                 int r1w, int dir, const double* rk, const double* pkm1,
                                                 double* rk1, double* pk, double* ring,
-                                                double (&acc)[4]) {
+                                                double (&acc)[4], const CgSubNeighbours* nb = nullptr,
+                                                int rsel = 0, int psel = 0) {
     const int lane = threadIdx.x & 31;
     const int nx = a.D.nx, ny = a.D.ny;
     const int c0 = (kSub ? a.col0 : 0) + sx * CG_W;
@@ -207,13 +224,31 @@ __device__ __forceinline__ void cg_iter_segment(const CgSweepArgs& a, const CgSc
     const int jfirst = (dir > 0) ? r0w : r1w - 1;
     const int total = (r1w - r0w) + 4;
     auto slot = [&](int t) { return ring + (unsigned)(t & (CG_RING - 1)) * CG_SLOT; };
+    // kNb: this lane's column in the neighbourhood (clamped to the ring), fixed for the strip
+    int nb_b = 1, nb_si = 0;
+    if constexpr (kNb) {
+        const int ii = min(max(i - nb->halo, -nb->halo), nb->nx + nb->halo - 1);
+        nb_b = (ii < 0) ? 0 : (ii >= nb->nx ? 2 : 1);
+        nb_si = (nb_b == 0) ? nb->nx_w + ii : (nb_b == 2 ? ii - nb->nx : ii);
+    }
     auto issue = [&](int t) {
         if (t < total) {
             double* sl = slot(t);
-            const size_t rp = (size_t)wrap(jfirst + (t - 2) * dir, ny) * nx + iw;
-            cp_async8(&sl[lane], &rk[rp]);
-            if constexpr (!FIRST) cp_async8(&sl[32 + lane], &pkm1[rp]);
-            if constexpr (XM == kXPair) cp_async8(&sl[64 + lane], &a.x[rp]);
+            const int j = jfirst + (t - 2) * dir;
+            const size_t rp = (size_t)wrap(j, ny) * nx + iw;
+            if constexpr (kNb) {
+                const int jj = min(max(j - nb->halo, -nb->halo), nb->ny + nb->halo - 1);
+                const int na = (jj < 0) ? 0 : (jj >= nb->ny ? 2 : 1);
+                const int sj = (na == 0) ? nb->ny_s + jj : (na == 2 ? jj - nb->ny : jj);
+                const int e = na * 3 + nb_b;
+                const size_t q = (size_t)(sj + nb->halo) * nb->nxe[e] + (nb_si + nb->halo);
+                cp_async8(&sl[lane], &nb->r[rsel][e][q]);
+                if constexpr (!FIRST) cp_async8(&sl[32 + lane], &nb->p[psel][e][q]);
+            } else {
+                cp_async8(&sl[lane], &rk[rp]);
+                if constexpr (!FIRST) cp_async8(&sl[32 + lane], &pkm1[rp]);
+            }
+            if constexpr (XM == kXPair) cp_async8(&sl[64 + lane], &a.x[rp]);  // read by owner lanes only
         }
         cp_async_commit();
     };

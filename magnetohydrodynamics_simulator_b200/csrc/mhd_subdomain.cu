@@ -349,10 +349,12 @@ k_sub_cg_sweep_rhs(CgSweepArgs a, const SubScal* __restrict__ sp, double* part, 
 }
 
 // Iteration k = products so far (from the control block, which also gives alpha, beta and
-// alpha_{k-1}); nothing once the solve has ended. Block partials r.r, r.z, z.Az, z.q_k.
+// alpha_{k-1}); nothing once the solve has ended. Block partials r.r, r.z, z.Az, z.q_k. kNb: the
+// cells around the interior are read from the neighbours' interiors (nb), not from the rings.
+template <bool kNb>
 __global__ void __launch_bounds__(kSubCgNT, 2)
 k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double* ctl, double* part,
-                    unsigned* arrivals, double* slot) {
+                    unsigned* arrivals, double* slot, CgSubNeighbours nb) {
     if (ctl[MHD_SUBCG_ACTIVE] == 0.0) return;
     extern __shared__ __align__(16) double sub_ring_mem[];
     __shared__ double red[kSubCgNT / 32 * 4];
@@ -369,19 +371,24 @@ k_sub_cg_sweep_iter(CgSweepArgs a, const SubScal* __restrict__ sp, const double*
     double* pk = odd ? a.p[1] : a.p[0];
     const int dir = odd ? 1 : -1;  // alternate (the right-hand side runs upwards)
     const int xm = cg_xmode(k);
+    const int rsel = odd ? 1 : 0, psel = odd ? 0 : 1;  // the neighbours' r_k and p_{k-1}
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int rend = a.D.ny - kH;
     for (int w = blockIdx.x * (kSubCgNT / 32) + (threadIdx.x >> 5); w < a.nwarps; w += gridDim.x * (kSubCgNT / 32)) {
         const int sx = w % a.strips_x, r0w = kH + (w / a.strips_x) * a.seg_h;
         const int r1w = min(r0w + a.seg_h, rend);
         if (k == 0)
-            cg_iter_segment<true, kXSkip, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<true, kXSkip, true, kNb>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc,
+                                                     &nb, rsel, psel);
         else if (xm == kXSkip)
-            cg_iter_segment<false, kXSkip, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<false, kXSkip, true, kNb>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc,
+                                                      &nb, rsel, psel);
         else if (xm == kXPairFirst)
-            cg_iter_segment<false, kXPairFirst, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<false, kXPairFirst, true, kNb>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring,
+                                                           acc, &nb, rsel, psel);
         else
-            cg_iter_segment<false, kXPair, true>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc);
+            cg_iter_segment<false, kXPair, true, kNb>(a, s, sx, r0w, r1w, dir, rk, pkm1, rk1, pk, ring, acc,
+                                                      &nb, rsel, psel);
     }
     block_sum<kSubCgNT, 4>(acc, red);
     sub_sums_to_slot(acc, part, arrivals, slot);
@@ -803,16 +810,43 @@ mhd_status capture_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int 
     }, &g->product);
 }
 
-// One iteration of the single-sweep solve of parity `odd`: the rings of r_k and p_{k-1}, the
-// sweep, the decision.
+// Subdomain i's 3 x 3 neighbourhood among the P x Q subdomains subs[q * P + p].
+CgSubNeighbours neighbourhood(mhd_subdomain* const* subs, int P, int Q, int i) {
+    CgSubNeighbours nb{};
+    const int p = i % P, q = i / P;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const mhd_subdomain* n = subs[((q + a - 1 + Q) % Q) * P + (p + b - 1 + P) % P];
+            const int e = a * 3 + b;
+            nb.r[0][e] = n->V.r;
+            nb.r[1][e] = n->V.z;
+            nb.p[0][e] = n->V.p;
+            nb.p[1][e] = n->V.q;
+            nb.nxe[e] = n->iv.nxe;
+        }
+    nb.nx = subs[i]->iv.nx;
+    nb.ny = subs[i]->iv.ny;
+    nb.nx_w = subs[q * P + (p + P - 1) % P]->iv.nx;
+    nb.ny_s = subs[((q + Q - 1) % Q) * P + p]->iv.ny;
+    nb.halo = kH;
+    return nb;
+}
+
+// One iteration of the single-sweep solve of parity `odd`: the sweeps, which read the cells around
+// each interior from the neighbours' interiors (the previous decision has ordered every
+// subdomain's last sweep before them, and r and p are double-buffered, so nothing they read is
+// being written), then the decision.
 mhd_status capture_sweep(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
                          long long max_products, int odd) {
+    (void)odd;  // the sweep takes k, and with it the buffers, from the control block
     return capture_graph(g, subs, [&]() -> mhd_status {
-        mhd_status st = mhd_sub_exchange_local(subs, P, Q, odd ? MHD_SUB_SET_CG_ODD : MHD_SUB_SET_CG_EVEN, 2);
-        for (int i = 0; i < g->count && st == MHD_OK; ++i)
-            st = mhd_sub_cg_sweep_iter_dev(subs[i], g->ctl, g->slots + 4 * i);
-        if (st == MHD_OK) st = mhd_subcg_decide_on(g, subs, 4, tol, max_products);
-        return st;
+        for (int i = 0; i < g->count; ++i) {
+            mhd_subdomain* s = subs[i];
+            k_sub_cg_sweep_iter<true><<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(
+                s->cga, s->sc, g->ctl, s->part, s->arrivals, g->slots + 4 * i, neighbourhood(subs, P, Q, i));
+            MHD_TRY(cudaGetLastError());
+        }
+        return mhd_subcg_decide_on(g, subs, 4, tol, max_products);
     }, &g->sweep[odd]);
 }
 
@@ -914,13 +948,19 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
         // about half a device's resident warps (the subdomains of one device share it)
         if (cudaFuncSetAttribute(k_sub_cg_sweep_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSubCgRingBytes) != cudaSuccess ||
-            cudaFuncSetAttribute(k_sub_cg_sweep_iter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_sub_cg_sweep_iter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSubCgRingBytes) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sub_cg_sweep_iter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSubCgRingBytes) != cudaSuccess)
             return fail(MHD_ERR_CUDA);
-        int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sub_cg_sweep_iter, kSubCgNT, kSubCgRingBytes) !=
-                cudaSuccess || occ < 1)
+        int occ = 0, occ_nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_nb, k_sub_cg_sweep_iter<true>, kSubCgNT,
+                                                          kSubCgRingBytes) != cudaSuccess)
             return fail(MHD_ERR_CUDA);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sub_cg_sweep_iter<false>, kSubCgNT, kSubCgRingBytes) !=
+                cudaSuccess || occ < 1 || occ_nb < 1)
+            return fail(MHD_ERR_CUDA);
+        occ = std::min(occ, occ_nb);
         CgSweepArgs& a = s->cga;
         a.D = s->ext;
         a.x = s->V.x;
@@ -1313,8 +1353,8 @@ mhd_status mhd_sub_cg_sweep_iter_dev(mhd_subdomain* s, const double* ctl, double
     mhd_status st = check_sub(s);
     if (st != MHD_OK) return st;
     if (!ctl || !slot) return MHD_ERR_INVALID_ARGUMENT;
-    k_sub_cg_sweep_iter<<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(s->cga, s->sc, ctl, s->part,
-                                                                                 s->arrivals, slot);
+    k_sub_cg_sweep_iter<false><<<s->cg_blocks, kSubCgNT, kSubCgRingBytes, s->stream>>>(
+        s->cga, s->sc, ctl, s->part, s->arrivals, slot, CgSubNeighbours{});
     MHD_TRY(cudaGetLastError());
     return MHD_OK;
 }

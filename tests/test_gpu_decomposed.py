@@ -119,6 +119,27 @@ def test_device_decisions_are_the_hosts(m):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("nx,ny,P,Q", [(96, 80, 2, 2), (70, 45, 3, 2), (96, 80, 1, 2)])
+def test_sweep_reading_neighbours_equals_sweep_reading_rings(m, nx, ny, P, Q):
+    """The single-sweep solve's graphs read the cells around each interior from the neighbours'
+    interiors; without graphs (rings through pack/unpack buffers) the same sweep reads its own
+    rings. Both must give the same bits."""
+    dx, dy = 2 * np.pi / nx, 1.6 * np.pi / ny
+    eta = 0.04
+    ic = smooth_state(nx, ny, dx, dy, seed=11)
+    res = []
+    for native in (True, False):
+        run, subs = _decomposed(m, nx, ny, dx, dy, eta, P, Q, ic, native=native)
+        steps = [run.step() for _ in range(3)]
+        res.append((steps, run.get_state()))
+        run.close()
+        for s in subs:
+            s.close()
+    assert res[0][0] == res[1][0]
+    for a, b in zip(res[0][1], res[1][1]):
+        assert np.array_equal(a, b)
+
+
 def test_decomposed_orszag_tang_matches_reference_goldens(m):
     """Orszag-Tang 128^2 split 2 x 2, the reference driver's dt sequence (first 20 steps of the
     golden run), against the single context stepped with the same dts."""
