@@ -455,8 +455,10 @@ mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, in
  * cg_sweep_rhs_dev: b = eta J_z(B*), r0 = b, slot = |b|^2, b.z0, z0.A z0 (then decision phase 3;
  * the predictor's or accumulator's rings must hold 2 cells). Iteration k: exchange
  * MHD_SUB_SET_CG_EVEN / _ODD (k even / odd) with a ring of 2, cg_sweep_iter_dev, decision phase 4.
- * mhd_subcg_sweep_product enqueues that iteration as a replayed graph (one per parity) and posts
- * the control block under `tag`. cg_sweep_finish_dev ends the solve (x = 0 after a zero right-hand
+ * mhd_subcg_sweep_product enqueues iteration k of subdomains that share a device as a replayed
+ * graph (one per parity), with no exchange: each sweep reads the cells around its interior from
+ * its neighbours' interiors (same results); it then posts the control block under `tag`.
+ * cg_sweep_finish_dev ends the solve (x = 0 after a zero right-hand
  * side or a breakdown, the last alpha_k p_k after an even last iteration). */
 mhd_status mhd_sub_cg_sweep_rhs_dev(mhd_subdomain* s, int solve_index, double* slot);
 mhd_status mhd_sub_cg_sweep_iter_dev(mhd_subdomain* s, const double* ctl, double* slot);
