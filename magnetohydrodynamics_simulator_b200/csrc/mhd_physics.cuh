@@ -120,7 +120,8 @@ __device__ __forceinline__ Flux conserved(const Prim& w) {
 // HLL average for every face and select the case afterwards instead of returning early (the same
 // values; straight-line code that schedules better where registers allow it, measured on B200:
 // stage 1 1.030 -> 1.010 ms at 4096^2; stage 2 uses it once its carried values live in shared
-// memory, the batch's stage 2 does not, as it spills there).
+// memory; in the batch's stage 2 it fits without spills too but gains nothing, 6.97-6.99 against
+// 6.98 ms per batched step, so the batch keeps the branches).
 template <int DIR, bool SELECT = false>
 __device__ __forceinline__ Flux hll(const Prim& L, const Prim& R) {
     const Flux FL = phys_flux<DIR>(L);
