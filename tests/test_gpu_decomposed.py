@@ -280,3 +280,27 @@ def test_distributed_transport_one_nccl_rank_matches_single_context(m, tmp_path)
         errs = [rel_linf(d[f"f{k}_{dev}"], w, 1.0) for k, w in enumerate(ctx.get_state())]
         assert max(errs) <= 1e-12, (dev, errs)
         ctx.close()
+
+
+@pytest.mark.parametrize("device", [True, False])
+def test_decomposed_solve_reports_nonfinite(m, device):
+    """A NaN in one face of the field reaches the solve's right-hand side: the decomposed solve
+    (decisions on the device or on the host) ends with status "nonfinite" after a fixed-dt step,
+    as the single context reports MHD_ERR_NONFINITE for the same state."""
+    nx, ny = 64, 48
+    dx, dy = 2 * np.pi / nx, 2 * np.pi / ny
+    eta = 0.05
+    ic = smooth_state(nx, ny, dx, dy, seed=2)
+    ic[4] = ic[4].copy()
+    ic[4][30, 40] = np.nan  # bxf of a cell inside subdomain (1, 1) of the 2 x 2 split
+    run, subs = _decomposed(m, nx, ny, dx, dy, eta, 2, 2, ic, device=device)
+    run.step(1e-3)
+    assert run.status == "nonfinite"
+    ctx = m.Context(nx, ny, dx, dy, eta)
+    ctx.set_state(ic)
+    ctx.step(1e-3)
+    assert ctx.synchronize_status() == 3  # MHD_ERR_NONFINITE
+    ctx.close()
+    run.close()
+    for s in subs:
+        s.close()
