@@ -221,7 +221,9 @@ typedef struct mhd_batch mhd_batch;
 typedef struct mhd_batch_tuning {
     int stage_rows;  /* rows per work item of the explicit stages and the finalize (>= 1; a strip
                       * is cut into equal items of at most this many rows) */
-    int cg_rows;     /* implicit solve: rows of a band (cg_order 0) or of a tile (1), >= 1 */
+    int cg_rows;     /* implicit solve: rows of a band (cg_order 0) or of a tile (1), >= 1; with
+                      * cg_order 1, 0 lets every phase choose its tile height (16-256 rows) for the
+                      * instances still iterating */
     int cg_order;    /* implicit solve: each phase deals the work of the instances still
                       * iterating evenly over the warps, 0: as equal row ranges (numbered in bands
                       * of cg_rows rows, strip by strip within a band), 1: as 28 x cg_rows tiles,

@@ -31,7 +31,9 @@ constexpr int kQueues = 3;  // work counters: stage 1, stage 2, finalize
 // item), solver rows (each with both decompositions).
 constexpr int kStageCand[][2] = {{64, 0},   {128, 0},  {256, 0},  {128, 32}, {256, 32},
                                  {256, 64}, {512, 32}, {384, 32}, {192, 32}, {512, 64}};
-constexpr int kCgRowsCand[] = {32, 64, 128, 256};
+// solver candidates (rows, order): even row ranges and fixed tiles of 32-256 rows, and tiles of a
+// height chosen phase by phase (rows 0)
+constexpr int kCgCand[][2] = {{32, 0}, {64, 0}, {128, 0}, {256, 0}, {32, 1}, {64, 1}, {128, 1}, {256, 1}, {0, 1}};
 
 }  // namespace
 
@@ -158,8 +160,9 @@ void strip_items(const mhd_batch* b, int rows, int tail_rows, std::vector<SweepI
 // them from a counter), so the small ones fill the end of the launch. Finalize: items that fill
 // one wave of its resident warps (at least 16 rows), as a single context's finalize.
 mhd_status apply_tuning(mhd_batch* b, const mhd_batch_tuning& t) {
-    if (t.stage_rows < 1 || t.cg_rows < 1 || (t.cg_order != 0 && t.cg_order != 1) ||
-        t.stage_tail_rows < 0)
+    // cg_rows = 0: tiles whose height the solver chooses phase by phase (order 1 only)
+    if (t.stage_rows < 1 || t.cg_rows < 0 || (t.cg_order != 0 && t.cg_order != 1) ||
+        (t.cg_rows == 0 && t.cg_order != 1) || t.stage_tail_rows < 0)
         return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaStreamSynchronize(b->stream));  // in-flight steps still read the old lists
     std::vector<SweepItem> st_items, fin_items;
@@ -706,20 +709,20 @@ mhd_status mhd_batch_autotune(mhd_batch* b, mhd_batch_tuning* out) {
     for (const auto& c : kStageCand) stage_cand.emplace_back(c[0], c[1]);
     for (int waves : {1, 2, 3, 4, 6}) stage_cand.emplace_back(balanced_stage_rows(b, waves), 0);
     const int nst = (int)stage_cand.size();
-    constexpr int ncg = sizeof(kCgRowsCand) / sizeof(int);
+    constexpr int ncg = sizeof(kCgCand) / sizeof(kCgCand[0]);
     double best_stage = 1e300, best_cg = 1e300;
     int best_stage_rows = before.stage_rows, best_tail = before.stage_tail_rows;
     int best_cg_rows = before.cg_rows, best_order = before.cg_order;
-    // trial -1 warms the kernels up; the others cover every solver candidate (both dealing orders)
-    // and every explicit-stage candidate
-    const int ntrials = std::max(nst, 2 * ncg);
+    // trial -1 warms the kernels up; the others cover every solver candidate and every
+    // explicit-stage candidate
+    const int ntrials = std::max(nst, ncg);
     for (int trial = -1; trial < ntrials; ++trial) {
         mhd_batch_tuning t{};
         const int tk = std::max(trial, 0);
         t.stage_rows = stage_cand[tk % nst].first;
         t.stage_tail_rows = stage_cand[tk % nst].second;
-        t.cg_rows = kCgRowsCand[tk % ncg];
-        t.cg_order = (tk / ncg) & 1;
+        t.cg_rows = kCgCand[tk % ncg][0];
+        t.cg_order = kCgCand[tk % ncg][1];
         if ((s = apply_tuning(b, t)) != MHD_OK) return s;
         if ((s = enqueue_step(b, nullptr, 0.0, 1, 0.0, false, ev)) != MHD_OK) return s;
         MHD_TRY(cudaStreamSynchronize(b->stream));

@@ -216,14 +216,13 @@ struct CgBInst {
     long long products;
     int status;
     int ny, strips;   // rows, 28-column strips
-    long long units;  // work units of the instance: strip rows (order 0) or tiles (order 1)
 };
 
 struct CgBatchArgs {
     const BatchInst* insts;  // descriptors of this step's parity
     int inst0, ninst;        // instances [inst0, inst0 + ninst) of this launch
     int order;               // 0: even row ranges in bands of `rows` rows; 1: tiles of `rows` rows
-    int rows;
+    int rows;                // order 1 with rows = 0: the tile height is chosen phase by phase
     double* partials;        // [2][CGB_MAX_INST][gridDim.x][4]
     CgSync* sync;
     int solve_index;         // 0: B* = U1*_B (T planes), 1: B* = U2*_B (A planes)
@@ -247,16 +246,48 @@ __device__ __forceinline__ CgSweepArgs cgb_args(const CgBatchArgs& a, const Batc
     return g;
 }
 
-// Prefix sum over the chunk's instances (at most 64) of the work units of those with
-// pick(instance), by a scan in the first warp (lane l: instances l and l + 32), then a block
-// barrier. Every block computes the same prefix from the same statuses.
+// Tile heights the phase-by-phase choice picks from (order 1 with rows = 0).
+constexpr int kCgbNHeights = 16;
+__device__ __constant__ const int kCgbHeights[kCgbNHeights] = {16,  20,  24,  28,  32,  40,  48,  56,
+                                                               64,  80,  96,  112, 128, 160, 192, 256};
+
+// The phase's decomposition of the instances with pick(instance): the tile height h (order 1) and
+// the prefix sum over the chunk's instances (at most 64) of their work units, strip rows (order 0)
+// or tiles of h rows (order 1), by the first warp (lane l: instances l and l + 32), then a block
+// barrier. With rows = 0 the height is the one among kCgbHeights that minimises the sweep rows of
+// the busiest warp, ceil(tiles / warps) x (h + 4): few tall tiles while many instances iterate,
+// short ones for the last few. Every block computes the same plan from the same statuses.
 template <class Pick>
-__device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long long* pref, Pick pick) {
+__device__ __forceinline__ int cgb_prefix(const CgBatchArgs& a, const CgBInst* sh, long long* pref,
+                                          int* h_out, Pick pick) {
     static_assert(CGB_MAX_INST <= 64, "two instances per lane");
+    const int ninst = a.ninst;
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
-        const long long u0 = (l < ninst && pick(sh[l])) ? sh[l].units : 0;
-        const long long u1 = (l + 32 < ninst && pick(sh[l + 32])) ? sh[l + 32].units : 0;
+        int h = a.rows;
+        if (a.order != 0 && a.rows == 0) {
+            const long long W = (long long)gridDim.x * CGB_NW;
+            int hl = kCgbHeights[l % kCgbNHeights];
+            long long tiles = 0;
+            for (int li = 0; li < ninst; ++li)
+                if (pick(sh[li])) tiles += (long long)sh[li].strips * ((sh[li].ny + hl - 1) / hl);
+            long long cost = ((tiles + W - 1) / W) * (hl + 4);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {  // lowest cost, then the taller tile: one answer in all lanes
+                const long long oc = __shfl_xor_sync(0xffffffffu, cost, o);
+                const int oh = __shfl_xor_sync(0xffffffffu, hl, o);
+                if (oc < cost || (oc == cost && oh > hl)) {
+                    cost = oc;
+                    hl = oh;
+                }
+            }
+            h = hl;
+        }
+        auto units = [&](const CgBInst& S) -> long long {
+            return (a.order == 0) ? (long long)S.strips * S.ny : (long long)S.strips * ((S.ny + h - 1) / h);
+        };
+        const long long u0 = (l < ninst && pick(sh[l])) ? units(sh[l]) : 0;
+        const long long u1 = (l + 32 < ninst && pick(sh[l + 32])) ? units(sh[l + 32]) : 0;
         long long s0 = u0, s1 = u1;  // inclusive scans over the lanes
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -271,14 +302,17 @@ __device__ __forceinline__ void cgb_prefix(const CgBInst* sh, int ninst, long lo
         if (l < ninst) pref[l] = s0 - u0;
         if (l + 32 < ninst) pref[l + 32] = first + s1 - u1;
         if (l == 31) pref[ninst] = first + s1;
+        if (l == 0) *h_out = h;
     }
     __syncthreads();
+    return *h_out;
 }
 
-// This warp's share of the phase as segments f(li, sx, r0, r1), in increasing unit number.
+// This warp's share of the phase as segments f(li, sx, r0, r1), in increasing unit number; h: the
+// phase's tile height (order 1).
 template <class F>
 __device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst* sh,
-                                             const long long* pref, F&& f) {
+                                             const long long* pref, int h, F&& f) {
     constexpr int NW = CGB_NW;
     const long long nw = (long long)gridDim.x * NW;
     const long long g = (long long)blockIdx.x * NW + (threadIdx.x >> 5);
@@ -289,8 +323,8 @@ __device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst
             while (pref[li + 1] <= j) ++li;
             const int w = (int)(j - pref[li]);
             const int sx = w % sh[li].strips;
-            const int r0 = (w / sh[li].strips) * a.rows;
-            f(li, sx, r0, min(r0 + a.rows, sh[li].ny));
+            const int r0 = (w / sh[li].strips) * h;
+            f(li, sx, r0, min(r0 + h, sh[li].ny));
         }
         return;
     }
@@ -321,7 +355,7 @@ __device__ __forceinline__ void cgb_segments(const CgBatchArgs& a, const CgBInst
 // of every instance published in part_out.
 template <int PH, int NV, int XM = kXSkip>
 __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* sh, const long long* pref,
-                                          double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
+                                          int h, double (*wsum)[CGB_MAX_INST][4], double* ring, int k,
                                           int dir, double* part_out) {
     constexpr int NW = CGB_NW;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -330,7 +364,7 @@ __device__ __forceinline__ void cgb_phase(const CgBatchArgs& a, const CgBInst* s
         for (int c = 0; c < NV; ++c) wsum[wid][li][c] = 0.0;
     __syncwarp();
     const bool odd = (k & 1) != 0;
-    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+    cgb_segments(a, sh, pref, h, [&](int li, int sx, int r0, int r1) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const CgSweepArgs g = cgb_args(a, I);
         CgScal s;
@@ -383,6 +417,7 @@ k_cg_batch(CgBatchArgs a) {
     constexpr int NW = CGB_NW;
     __shared__ CgBInst sh[CGB_MAX_INST];
     __shared__ long long pref[CGB_MAX_INST + 1];
+    __shared__ int tile_h;  // the phase's tile height (order 1)
     __shared__ int sflag;
 #if defined(__CUDA_ARCH__)
     extern __shared__ __align__(16) double cg_ring_mem[];
@@ -425,15 +460,13 @@ k_cg_batch(CgBatchArgs a) {
         S.status = kCgActive;
         S.ny = I.D.ny;
         S.strips = I.cg_strips_x;
-        S.units = (long long)I.cg_strips_x *
-                  ((a.order == 0) ? I.D.ny : (I.D.ny + a.rows - 1) / a.rows);
     }
     __syncthreads();
     auto is_active = [](const CgBInst& S) { return S.status == kCgActive; };
 
     // ---- right-hand side: r0 = b, p0 = z0 = b/d; |b|^2, b.z0, p0.A p0
-    cgb_prefix(sh, a.ninst, pref, is_active);
-    cgb_phase<0, 3>(a, sh, pref, wsum, ring, 0, dir, part(phase));
+    int h = cgb_prefix(a, sh, pref, &tile_h, is_active);
+    cgb_phase<0, 3>(a, sh, pref, h, wsum, ring, 0, dir, part(phase));
     if (!barrier_or_quit()) return;
     for (int li = wid; li < a.ninst; li += NW) {
         double v[3];
@@ -457,12 +490,13 @@ k_cg_batch(CgBatchArgs a) {
 
     for (int k = 0;; ++k) {
         // ---- iteration k: p_k, q_k, x_{k+1}, r_{k+1}; r.r, r.z, z.Az, z.q_k
-        cgb_prefix(sh, a.ninst, pref, is_active);
+        h = cgb_prefix(a, sh, pref, &tile_h, is_active);
         // (all instances run iteration k together, so k's x mode is the same for all of them)
-        if (k == 0) cgb_phase<1, 4, kXSkip>(a, sh, pref, wsum, ring, k, dir, part(phase));
-        else if (cg_xmode(k) == kXSkip) cgb_phase<2, 4, kXSkip>(a, sh, pref, wsum, ring, k, dir, part(phase));
-        else if (cg_xmode(k) == kXPairFirst) cgb_phase<2, 4, kXPairFirst>(a, sh, pref, wsum, ring, k, dir, part(phase));
-        else cgb_phase<2, 4, kXPair>(a, sh, pref, wsum, ring, k, dir, part(phase));
+        if (k == 0) cgb_phase<1, 4, kXSkip>(a, sh, pref, h, wsum, ring, k, dir, part(phase));
+        else if (cg_xmode(k) == kXSkip) cgb_phase<2, 4, kXSkip>(a, sh, pref, h, wsum, ring, k, dir, part(phase));
+        else if (cg_xmode(k) == kXPairFirst)
+            cgb_phase<2, 4, kXPairFirst>(a, sh, pref, h, wsum, ring, k, dir, part(phase));
+        else cgb_phase<2, 4, kXPair>(a, sh, pref, h, wsum, ring, k, dir, part(phase));
         if (!barrier_or_quit()) return;
         int active = 0;
         for (int li = wid; li < a.ninst; li += NW) {
@@ -497,10 +531,10 @@ k_cg_batch(CgBatchArgs a) {
     }
 
     // x = 0 for a vanished right-hand side (Eigen returns the zero vector) and on breakdown
-    cgb_prefix(sh, a.ninst, pref, [](const CgBInst& S) {
+    h = cgb_prefix(a, sh, pref, &tile_h, [](const CgBInst& S) {
         return S.status == kCgZero || S.status == kCgBreakdown || (S.status == kCgCapped && S.products == 0);
     });
-    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+    cgb_segments(a, sh, pref, h, [&](int li, int sx, int r0, int r1) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const int nx = I.D.nx;
         const int i = sx * CG_W - CG_HALO + lane;
@@ -510,10 +544,10 @@ k_cg_batch(CgBatchArgs a) {
     // solutions whose last iteration was even (an odd number of products) still lack that
     // iteration's alpha_k p_k (x moves every second iteration, see mhd_cg_sweep.cuh)
     __syncthreads();  // every warp is done with the prefix above
-    cgb_prefix(sh, a.ninst, pref, [](const CgBInst& S) {
+    h = cgb_prefix(a, sh, pref, &tile_h, [](const CgBInst& S) {
         return (S.status == kCgConverged || S.status == kCgCapped) && (S.products & 1) == 1;
     });
-    cgb_segments(a, sh, pref, [&](int li, int sx, int r0, int r1) {
+    cgb_segments(a, sh, pref, h, [&](int li, int sx, int r0, int r1) {
         const BatchInst& I = a.insts[a.inst0 + li];
         const CgBInst& S = sh[li];
         const double* pl = ((S.products - 1) & 1) ? I.p[1] : I.p[0];
