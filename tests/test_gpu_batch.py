@@ -192,7 +192,8 @@ def test_autotune_restores_state_and_keeps_parity(m):
     before = [b.get_state(i) for i in range(len(insts))]
     cfl_before = [b.cfl_dt(i) for i in range(len(insts))]
     t = b.autotune()
-    assert t["stage_rows"] >= 1 and t["cg_rows"] >= 1 and t["cg_order"] in (0, 1)
+    assert t["stage_rows"] >= 1 and t["cg_order"] in (0, 1)
+    assert t["cg_rows"] >= 1 or (t["cg_rows"] == 0 and t["cg_order"] == 1)  # 0: heights per phase
     assert t["stage_ms"] > 0 and t["cg_ms"] > 0
     for i in range(len(insts)):
         for f0, f1 in zip(before[i], b.get_state(i)):
@@ -209,7 +210,7 @@ def test_autotune_restores_state_and_keeps_parity(m):
 
 
 @pytest.mark.parametrize("stage_rows,cg_rows,cg_order,tail", [(1, 1, 0, 0), (7, 3, 1, 0), (300, 300, 0, 0),
-                                                            (16, 8, 0, 5), (64, 32, 1, 3)])
+                                                            (16, 8, 0, 5), (64, 32, 1, 3), (48, 0, 1, 0)])
 def test_every_decomposition_gives_the_same_step(m, stage_rows, cg_rows, cg_order, tail):
     insts = _instances(SPECS)
     b = _batch(m, insts)
@@ -223,6 +224,15 @@ def test_every_decomposition_gives_the_same_step(m, stage_rows, cg_rows, cg_orde
         o.step(1e-3)
         err = _max_err(b.get_state(i), o.get_state())
         assert err <= STEP_TOL, (i, err)
+
+
+def test_phase_chosen_tile_height_needs_tiles(m):
+    """cg_rows = 0 (a tile height chosen phase by phase) exists for the tile order only."""
+    b = _batch(m, _instances(SPECS[:2]))
+    with pytest.raises(m.MHDError):
+        b.set_tuning(64, 0, 0, 0)
+    b.set_tuning(64, 0, 1, 0)
+    assert b.tuning()["cg_rows"] == 0
 
 
 def test_nonfinite_instance_is_reported_alone(m):
