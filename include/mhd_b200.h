@@ -420,7 +420,9 @@ enum {
     MHD_SUBCG_ALPHA_PREV = 10, /* single-sweep form: alpha of the previous iteration */
     MHD_SUBCG_K_LAST = 11,    /* single-sweep form: the last iteration swept (-1: none) */
     MHD_SUBCG_ALPHA_LAST = 12, /* single-sweep form: its alpha */
-    MHD_SUBCG_ZERO = 13       /* single-sweep form: 1 when the solution is x = 0 */
+    MHD_SUBCG_ZERO = 13,      /* single-sweep form: 1 when the solution is x = 0 */
+    MHD_SUBCG_DT = 14,        /* the step of the last mhd_subcg_cfl_step */
+    MHD_SUBCG_CFL_NONFINITE = 15 /* 1 when that step's scan met a non-finite value */
 };
 enum { MHD_SUBCG_OK = 0, MHD_SUBCG_NOT_CONVERGED = 1, MHD_SUBCG_NONFINITE = 2 };
 typedef struct mhd_subcg mhd_subcg;
@@ -451,6 +453,14 @@ mhd_status mhd_subcg_decide_on(mhd_subcg* g, mhd_subdomain* const* subs, int pha
                                long long max_products);
 mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
                              long long max_products, int tag);
+/* The CFL step of every subdomain (at most 64, of one grid: equal spacing and eta) on the device:
+ * the largest interior signal speed of all of them (diagnostics.hpp:60-78), dt by
+ * diagnostics.hpp:82-86 with `courant` and `safety` (the host driver's arithmetic), and each
+ * subdomain's step set to dt with the reference driver's matrix alpha = (dt eta) g, as
+ * mhd_sub_set_step would. dt lands in ctl[MHD_SUBCG_DT] and a non-finite state in
+ * ctl[MHD_SUBCG_CFL_NONFINITE], read with the next mhd_subcg_post/read. Ordered after the
+ * subdomains' work so far and before their later work; no host wait. */
+mhd_status mhd_subcg_cfl_step(mhd_subcg* g, mhd_subdomain* const* subs, double courant, double safety);
 /* The single-sweep form of the decomposed solve: the single context's solver (one sweep per
  * product forming q = A p, r, z and the sums r.r, r.z, z.Az, z.q, with p.Ap carried by a
  * recurrence, and the solution moved every second iteration) on each subdomain's interior.

@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <math_constants.h>
 #include <cmath>
 #include <cstring>
 #include <atomic>
@@ -98,9 +99,8 @@ __global__ void k_sub_final(const double* __restrict__ part, int nblocks, double
 // The step's coefficients and the implicit matrix (I - alpha L) of the solves: off-diagonal
 // cx = alpha/dx^2, cy = alpha/dy^2, diagonal 1 + 2 (cx + cy) (solvers.hpp:404-443), on the device
 // so that a captured solve reads this step's matrix.
-__global__ void k_sub_set_coeffs(StepCoeffs* C, SubScal* sc, double dt, double alpha, double g, double d,
-                                 double dx, double dy) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void sub_set_coeffs(StepCoeffs* C, SubScal* sc, double dt, double alpha, double g,
+                                               double d, double dx, double dy) {
     C->dt = dt;
     C->c_g = dt * g;
     C->c_d = dt * d;
@@ -113,6 +113,43 @@ __global__ void k_sub_set_coeffs(StepCoeffs* C, SubScal* sc, double dt, double a
     sc->cy = cy;
     sc->diag = diag;
     sc->invdiag = (diag == 0.0) ? 1.0 : 1.0 / diag;
+}
+
+__global__ void k_sub_set_coeffs(StepCoeffs* C, SubScal* sc, double dt, double alpha, double g, double d,
+                                 double dx, double dy) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    sub_set_coeffs(C, sc, dt, alpha, g, d, dx, dy);
+}
+
+// The CFL step of P x Q subdomains on the device (diagnostics.hpp:82-86 from the largest interior
+// signal speed of all of them, as the host driver computes it) and each subdomain's step
+// coefficients and matrix for that dt, alpha = (dt eta) g; dt goes to ctl[MHD_SUBCG_DT] and a
+// non-finite state to ctl[MHD_SUBCG_CFL_NONFINITE].
+constexpr int kSubCflMax = 64;
+struct SubCflTargets {
+    const unsigned long long* speed[kSubCflMax];  // each subdomain's (max speed bits, non-finite flag)
+    StepCoeffs* coeffs[kSubCflMax];
+    SubScal* sc[kSubCflMax];
+};
+
+__global__ void k_subcg_cfl_step(SubCflTargets t, int count, double dx, double dy, double eta, double courant,
+                                 double safety, double g, double d, double* ctl) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long bits = 0, bad = 0;
+    for (int i = 0; i < count; ++i) {
+        bits = bits > t.speed[i][0] ? bits : t.speed[i][0];  // non-negative doubles order as their bits
+        bad |= t.speed[i][1];
+    }
+    double smaxv = __longlong_as_double((long long)bits);
+    if (smaxv < 1e-8) smaxv = 1e-8;
+    const double hmin = dx < dy ? dx : dy;
+    const double dt_res = (eta == 0.0) ? CUDART_INF : hmin * hmin / (4.0 * eta);
+    const double dt_hyp = courant * hmin / smaxv;
+    const double dt = (dt_res < dt_hyp ? dt_res : dt_hyp) * safety;
+    const double alpha = (dt * eta) * g;
+    for (int i = 0; i < count; ++i) sub_set_coeffs(t.coeffs[i], t.sc[i], dt, alpha, g, d, dx, dy);
+    ctl[MHD_SUBCG_DT] = dt;
+    ctl[MHD_SUBCG_CFL_NONFINITE] = bad ? 1.0 : 0.0;
 }
 
 // Copy the rectangle [x0, x0 + w) x [y0, y0 + h) of np extended planes (row pitch nxe) into buf
@@ -624,6 +661,7 @@ struct mhd_subdomain {
     CgSweepArgs cga{};  // the single-sweep solve's sweep: the interior's strips and row segments
     int cg_blocks = 0;
     unsigned* arrivals = nullptr;  // blocks of the running sweep that have published their sums
+    unsigned long long* cfl = nullptr;  // the device CFL step's scan: max speed bits, non-finite flag
     int pending_sums = 0;  // sums enqueued by a CG phase without an output pointer
     cudaEvent_t ev_ready = nullptr;  // in-process exchange: this subdomain's strips may be read
     cudaEvent_t ev_done = nullptr;   // in-process exchange: this subdomain's rings are filled
@@ -928,6 +966,7 @@ mhd_status mhd_sub_create(const mhd_params* p, void* stream, mhd_subdomain** out
         cudaMalloc(&s->scratch_status, sizeof(DeviceStatus)) != cudaSuccess ||
         cudaMalloc(&s->sc, sizeof(SubScal)) != cudaSuccess ||
         cudaMalloc(&s->arrivals, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&s->cfl, 2 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&s->part, (size_t)4 * kSubMaxBlocks * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&s->dev_out, 8 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&s->host_out, 8 * sizeof(double)) != cudaSuccess) {
@@ -1002,6 +1041,7 @@ mhd_status mhd_sub_destroy(mhd_subdomain* s) {
     cudaFree(s->scratch_status);
     cudaFree(s->sc);
     cudaFree(s->arrivals);
+    cudaFree(s->cfl);
     cudaFree(s->part);
     cudaFree(s->dev_out);
     if (s->host_out) cudaFreeHost(s->host_out);
@@ -1512,6 +1552,36 @@ mhd_status replay(mhd_subcg* g, mhd_subdomain* const* subs, cudaGraphExec_t exec
     return subs_after_group(g, subs);
 }
 }  // namespace
+
+mhd_status mhd_subcg_cfl_step(mhd_subcg* g, mhd_subdomain* const* subs, double courant, double safety) {
+    if (!g || !subs || g->count > kSubCflMax || !(courant > 0) || !(safety > 0)) return MHD_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < g->count; ++i) {
+        if (!subs[i] || subs[i]->device != g->device) return MHD_ERR_INVALID_ARGUMENT;
+        const mhd_params& a = subs[i]->prm;
+        const mhd_params& b = subs[0]->prm;
+        if (a.dx != b.dx || a.dy != b.dy || a.eta != b.eta) return MHD_ERR_INVALID_ARGUMENT;
+    }
+    MHD_TRY(cudaSetDevice(g->device));
+    SubCflTargets t{};
+    for (int i = 0; i < g->count; ++i) {
+        mhd_subdomain* s = subs[i];
+        MHD_TRY(cudaMemsetAsync(s->cfl, 0, 2 * sizeof(unsigned long long), s->stream));
+        CPlanes u;
+        for (int k = 0; k < 6; ++k) u.f[k] = s->S[k];
+        k_sub_cfl<<<s->blocks, kSubNT, 0, s->stream>>>(s->iv, u, s->cfl);
+        MHD_TRY(cudaGetLastError());
+        t.speed[i] = s->cfl;
+        t.coeffs[i] = s->coeffs;
+        t.sc[i] = s->sc;
+    }
+    mhd_status st = group_after_subs(g, subs);
+    if (st != MHD_OK) return st;
+    const mhd_subdomain* s0 = subs[0];
+    k_subcg_cfl_step<<<1, 32, 0, g->stream>>>(t, g->count, s0->prm.dx, s0->prm.dy, s0->prm.eta, courant, safety,
+                                              s0->g, s0->d, g->ctl);
+    MHD_TRY(cudaGetLastError());
+    return subs_after_group(g, subs);
+}
 
 mhd_status mhd_subcg_product(mhd_subcg* g, mhd_subdomain* const* subs, int P, int Q, double tol,
                              long long max_products, int tag) {

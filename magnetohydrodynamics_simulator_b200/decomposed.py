@@ -56,6 +56,7 @@ ARS_G = (2.0 - math.sqrt(2.0)) / 2.0  # solvers.hpp:41
 # control block of the device-resident decisions (MHD_SUBCG_* of include/mhd_b200.h)
 SUBCG_CTL = 16
 CG_ACTIVE, CG_STATUS, CG_PRODUCTS, CG_ALPHA, CG_BETA = 0, 1, 2, 6, 7
+CG_DT, CG_CFL_NONFINITE = 14, 15
 CG_OK, CG_NOT_CONVERGED, CG_NONFINITE = 0, 1, 2
 
 
@@ -293,6 +294,10 @@ class DeviceCgGroup:
         _check(self.lib.mhd_subcg_sweep_product(self.h, handles, P, Q, tol, max_products, k, tag),
                "mhd_subcg_sweep_product")
 
+    def cfl_step(self, handles, courant: float, safety: float):
+        """The CFL step of all subdomains and their step coefficients, on the device."""
+        _check(self.lib.mhd_subcg_cfl_step(self.h, handles, courant, safety), "mhd_subcg_cfl_step")
+
     def post(self, tag: int):
         _check(self.lib.mhd_subcg_post(self.h, tag), "mhd_subcg_post")
 
@@ -393,6 +398,7 @@ def _bind(lib):
     lib.mhd_subcg_product.argtypes = [vp, ctypes.POINTER(vp), ip, ip, ctypes.c_double, ctypes.c_longlong, ip]
     lib.mhd_subcg_sweep_product.argtypes = [vp, ctypes.POINTER(vp), ip, ip, ctypes.c_double, ctypes.c_longlong,
                                             ip, ip]
+    lib.mhd_subcg_cfl_step.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_double, ctypes.c_double]
     lib.mhd_sub_cg_sweep_rhs_dev.argtypes = [vp, ip, vp]
     lib.mhd_sub_cg_sweep_iter_dev.argtypes = [vp, vp, vp]
     lib.mhd_sub_cg_sweep_finish_dev.argtypes = [vp, vp]
@@ -628,6 +634,7 @@ class DecomposedRun:
         self.max_iters = cg_max_iters if cg_max_iters > 0 else 2 * part.nx * part.ny
         self.status = "ok"
         self.last_products = (0, 0)
+        self._last_ctl = None
 
     def _own_indices(self):
         if isinstance(self.tr, LocalTransport):
@@ -752,11 +759,14 @@ class DecomposedRun:
                 for s in own:
                     s.cg_direction_dev(ctl)
                 g.post(tag)
-            if g.read(tag - 1)[CG_ACTIVE] == 0.0:
-                break
+            c = g.read(tag - 1)
+            if c[CG_ACTIVE] == 0.0:
+                break  # the solve ended: later iterations change nothing in the control block
+        else:
+            c = g.read(tag)
+        self._last_ctl = c
         for s in own:
             s.cg_finish_dev(ctl)
-        c = g.read(tag)
         st = int(c[CG_STATUS])
         if st == CG_NONFINITE:
             self.status = "nonfinite"
@@ -781,11 +791,14 @@ class DecomposedRun:
                     s.cg_sweep_iter_dev(ctl, sl)
                 decide(4)
                 g.post(tag)
-            if g.read(tag - 1)[CG_ACTIVE] == 0.0:
-                break
+            c = g.read(tag - 1)
+            if c[CG_ACTIVE] == 0.0:
+                break  # the solve ended: later iterations change nothing in the control block
+        else:
+            c = g.read(tag)
+        self._last_ctl = c
         for s in own:
             s.cg_sweep_finish_dev(ctl)
-        c = g.read(tag)
         st = int(c[CG_STATUS])
         if st == CG_NONFINITE:
             self.status = "nonfinite"
@@ -802,13 +815,20 @@ class DecomposedRun:
     def step(self, dt: float = 0.0, alpha: float | None = None):
         """One IMEX step; dt <= 0 takes the CFL step. alpha defaults to (dt * eta) * g (the matrix
         the reference driver builds for this dt). Returns (dt, (products of the two solves))."""
-        if dt <= 0.0:
-            dt = self.cfl_dt()
-        if alpha is None:
-            alpha = (dt * self.eta) * ARS_G
         own = self.tr.own
-        for s in own:
-            s.set_step(dt, alpha)
+        handles = getattr(self.tr, "_handles", None)
+        device_cfl = (dt <= 0.0 and alpha is None and isinstance(self._group, DeviceCgGroup)
+                      and handles is not None)
+        if device_cfl:
+            # dt and the step's coefficients on the device; dt comes back with the solve's polls
+            self._group.cfl_step(handles, self.courant, self.safety)
+        else:
+            if dt <= 0.0:
+                dt = self.cfl_dt()
+            if alpha is None:
+                alpha = (dt * self.eta) * ARS_G
+            for s in own:
+                s.set_step(dt, alpha)
         for s in own:
             s.stage(1)
         self.tr.exchange(SET_PREDICTOR, HALO)
@@ -823,6 +843,10 @@ class DecomposedRun:
             s.finalize()
         self.tr.exchange(SET_STATE, HALO)
         self.last_products = (k1, k2)
+        if device_cfl:
+            dt = float(self._last_ctl[CG_DT])
+            if self._last_ctl[CG_CFL_NONFINITE] != 0.0:
+                self.status = "nonfinite"
         return dt, (k1, k2)
 
     def divb(self):

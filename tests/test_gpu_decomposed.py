@@ -296,6 +296,13 @@ def test_decomposed_solve_reports_nonfinite(m, device):
     run, subs = _decomposed(m, nx, ny, dx, dy, eta, 2, 2, ic, device=device)
     run.step(1e-3)
     assert run.status == "nonfinite"
+    # the CFL step of the same state (on the device with device decisions) flags it too
+    run2, subs2 = _decomposed(m, nx, ny, dx, dy, eta, 2, 2, ic, device=device)
+    run2.step()
+    assert run2.status == "nonfinite"
+    run2.close()
+    for s in subs2:
+        s.close()
     ctx = m.Context(nx, ny, dx, dy, eta)
     ctx.set_state(ic)
     ctx.step(1e-3)
