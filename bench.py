@@ -374,6 +374,20 @@ def run_gpu_arm(args):
     s1.synchronize()
     e2e_sync_ms = max_over_ranks(dist, s0.elapsed_time(s1), "cuda")
     status2 = ctx.synchronize_status()
+    # both transfer modes are public calls; a host link that does not overlap its two directions
+    # gains nothing from the pipelined one, so the line reports the faster mode of this box
+    e2e_modes = {
+        "pipelined": {"value": e2e_value, "ms_per_step": e2e_ms / e2e_steps,
+                      "how": "mhd_set_state_async + mhd_step + mhd_get_state_async per step from pinned "
+                             "host planes (read-back and next upload overlap piece by piece)"},
+        "synchronous": {"value": world * zones * e2e_steps / (e2e_sync_ms * 1e-3),
+                        "ms_per_step": e2e_sync_ms / e2e_steps,
+                        "how": "mhd_set_state + mhd_step + mhd_get_state per step from pinned host planes"},
+    }
+    e2e_mode = max(e2e_modes, key=lambda k: e2e_modes[k]["value"])
+    e2e = {"value": e2e_modes[e2e_mode]["value"], "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
+           "d2h_bytes_per_step": int(6 * zones * 8), "steps": e2e_steps, "mode": e2e_mode,
+           "how": e2e_modes[e2e_mode]["how"], "modes": e2e_modes}
 
     # ---- roofline of the dominant kernel (per-kernel CUDA events over the timed region)
     peak, peak_kind = load_peaks()
@@ -510,13 +524,7 @@ def run_gpu_arm(args):
                    "parallelism": f"replicas{world}", "l2": "inputs exceed L2 (805 MB state)",
                    "cg_products_last_step": list(prods),
                    "cg_products_mean_per_step": [k1, k2]},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(6 * zones * 8),
-                "d2h_bytes_per_step": int(6 * zones * 8), "steps": e2e_steps,
-                "how": "mhd_set_state_async + mhd_step + mhd_get_state_async per step from pinned "
-                       "host planes (read-back and next upload overlap piece by piece)",
-                "synchronous": {"value": world * zones * e2e_steps / (e2e_sync_ms * 1e-3),
-                                "ms_per_step": e2e_sync_ms / e2e_steps,
-                                "how": "mhd_set_state + mhd_step + mhd_get_state per step"}},
+        "e2e": e2e,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "parity": parity,
