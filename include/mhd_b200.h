@@ -401,7 +401,7 @@ mhd_status mhd_sub_sums(mhd_subdomain* s, double* out, int n);
  * decisions of the host driver, with the same arithmetic: the results are bit-identical. The
  * subdomains and the group's stream must be ordered by the caller (one shared stream in one
  * process). mhd_subcg_post(g, tag) enqueues a copy of the control block to pinned memory and
- * mhd_subcg_read(g, tag, out) waits for it (two copies in flight: tags of one parity share one).
+ * mhd_subcg_read(g, tag, out) waits for it (four copies in flight: tags equal modulo 4 share one).
  * cg_finish_dev zeroes x after a solve that met a non-finite value (as cg_zero_solution).
  * mhd_subcg_decide_host applies the same rules to host arrays (no device needed). Phases 3 and 4
  * are those of the single-sweep form below. */

@@ -670,7 +670,9 @@ struct mhd_subdomain {
 };
 
 // Device-resident decisions of one decomposed solve (mhd_subcg_*): the control block, the
-// subdomains' sum slots, and two pinned copies of the control block for the host to poll.
+// subdomains' sum slots, and four pinned copies of the control block for the host to poll (the
+// host may read a copy posted up to three posts earlier).
+constexpr int kPostSlots = 4;
 struct mhd_subcg {
     int count = 0;
     int device = 0;
@@ -687,8 +689,8 @@ struct mhd_subcg {
     double* ctl = nullptr;    // device, MHD_SUBCG_CTL doubles
     double* slots = nullptr;  // device, count x 4
     bool own_slots = false;
-    double* host = nullptr;   // pinned, 2 x MHD_SUBCG_CTL
-    cudaEvent_t ev[2]{};
+    double* host = nullptr;   // pinned, kPostSlots x MHD_SUBCG_CTL
+    cudaEvent_t ev[4]{};      // one per posted copy (tags modulo kPostSlots)
 };
 
 namespace {
@@ -1432,9 +1434,11 @@ mhd_status mhd_subcg_create(int count, void* stream, double* slots, mhd_subcg** 
     g->own_slots = slots == nullptr;
     if (cudaMalloc(&g->ctl, MHD_SUBCG_CTL * sizeof(double)) != cudaSuccess ||
         (g->own_slots && cudaMalloc(&g->slots, (size_t)4 * count * sizeof(double)) != cudaSuccess) ||
-        cudaMallocHost(&g->host, 2 * MHD_SUBCG_CTL * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&g->host, kPostSlots * MHD_SUBCG_CTL * sizeof(double)) != cudaSuccess ||
         cudaEventCreateWithFlags(&g->ev[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&g->ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->ev[2], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->ev[3], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&g->ev_decided, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         mhd_subcg_destroy(g);
@@ -1483,7 +1487,7 @@ mhd_status mhd_subcg_decide(mhd_subcg* g, int phase, double tol, long long max_p
 mhd_status mhd_subcg_post(mhd_subcg* g, int tag) {
     if (!g || tag < 0) return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaSetDevice(g->device));
-    const int b = tag & 1;
+    const int b = tag % kPostSlots;
     MHD_TRY(cudaMemcpyAsync(g->host + b * MHD_SUBCG_CTL, g->ctl, MHD_SUBCG_CTL * sizeof(double),
                             cudaMemcpyDeviceToHost, g->stream));
     MHD_TRY(cudaEventRecord(g->ev[b], g->stream));
@@ -1493,7 +1497,7 @@ mhd_status mhd_subcg_post(mhd_subcg* g, int tag) {
 mhd_status mhd_subcg_read(mhd_subcg* g, int tag, double* out) {
     if (!g || tag < 0 || !out) return MHD_ERR_INVALID_ARGUMENT;
     MHD_TRY(cudaSetDevice(g->device));
-    const int b = tag & 1;
+    const int b = tag % kPostSlots;
     MHD_TRY(cudaEventSynchronize(g->ev[b]));
     memcpy(out, g->host + b * MHD_SUBCG_CTL, MHD_SUBCG_CTL * sizeof(double));
     return MHD_OK;

@@ -327,7 +327,7 @@ class HostCgGroup:
         self.count = count
         self.ctl = np.zeros(SUBCG_CTL)
         self.slots = np.zeros(4 * count)
-        self._posted = [None, None]
+        self._posted = [None] * 4
 
     def slot(self, i: int):
         return self.slots[4 * i:4 * i + 4]
@@ -338,10 +338,10 @@ class HostCgGroup:
                                               self.count, phase, tol, max_products), "mhd_subcg_decide_host")
 
     def post(self, tag: int):
-        self._posted[tag & 1] = self.ctl.copy()
+        self._posted[tag % 4] = self.ctl.copy()
 
     def read(self, tag: int):
-        return [float(v) for v in self._posted[tag & 1]]
+        return [float(v) for v in self._posted[tag % 4]]
 
     def close(self):
         pass
@@ -613,12 +613,17 @@ class DecomposedRun:
 
     def __init__(self, part: Partition, transport, dx: float, dy: float, eta: float, *,
                  courant: float = 0.5, safety: float = 0.9, cg_tol: float = 0.0, cg_max_iters: int = 0,
-                 device_decisions: bool = True, cg_form: str | None = None):
+                 device_decisions: bool = True, cg_form: str | None = None, poll_lag: int = 1):
         """device_decisions: take the solve's decisions on the device (DeviceCgGroup) where the
         transport allows it; False keeps them on the host (both give bit-identical results).
         cg_form: "sweep", the single context's single-sweep solver on every subdomain (GPU
         subdomains with device decisions; the default there), or "two_sweep" (a matrix product
-        and an update per product; every other case)."""
+        and an update per product; every other case). poll_lag (1-3): with device decisions the
+        host reads the control block posted poll_lag iterations back, so that many iterations
+        stay queued (each solve then runs poll_lag no-op iterations after its end)."""
+        if not 1 <= poll_lag <= 3:
+            raise ValueError("poll_lag must be 1, 2 or 3")
+        self.poll_lag = poll_lag
         self.part, self.tr = part, transport
         self._group = transport.cg_group() if device_decisions else None
         self._slots = transport.own_slots(self._group) if self._group is not None else None
@@ -759,7 +764,9 @@ class DecomposedRun:
                 for s in own:
                     s.cg_direction_dev(ctl)
                 g.post(tag)
-            c = g.read(tag - 1)
+            if tag < self.poll_lag:
+                continue
+            c = g.read(tag - self.poll_lag)
             if c[CG_ACTIVE] == 0.0:
                 break  # the solve ended: later iterations change nothing in the control block
         else:
@@ -791,7 +798,9 @@ class DecomposedRun:
                     s.cg_sweep_iter_dev(ctl, sl)
                 decide(4)
                 g.post(tag)
-            c = g.read(tag - 1)
+            if tag < self.poll_lag:
+                continue
+            c = g.read(tag - self.poll_lag)
             if c[CG_ACTIVE] == 0.0:
                 break  # the solve ended: later iterations change nothing in the control block
         else:

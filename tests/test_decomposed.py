@@ -80,15 +80,17 @@ def test_control_block_decisions_are_the_hosts():
     ic = smooth_state(NX, NY, dx, dy, seed=5)
     part = Partition(NX, NY, 2, 2)
     res = []
-    for mode in (True, False):
+    for mode, lag in ((True, 1), (False, 1), (True, 3)):
         subs = [OracleSubdomain(*part.shape(i), dx, dy, ETA) for i in range(part.count)]
-        run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, ETA, device_decisions=mode)
+        run = DecomposedRun(part, LocalTransport(part, subs), dx, dy, ETA, device_decisions=mode,
+                            poll_lag=lag)
         run.set_state(ic)
         steps = [run.step() for _ in range(3)]
         res.append((steps, run.get_state()))
-    assert res[0][0] == res[1][0]
-    for a, b in zip(res[0][1], res[1][1]):
-        assert np.array_equal(a, b)
+    for other in res[1:]:
+        assert res[0][0] == other[0]
+        for a, b in zip(res[0][1], other[1]):
+            assert np.array_equal(a, b)
 
 
 def test_control_block_rules():
