@@ -311,3 +311,29 @@ def test_decomposed_solve_reports_nonfinite(m, device):
     run.close()
     for s in subs:
         s.close()
+
+
+def test_decomposed_orszag_tang_2048_matches_single_context(m):
+    """At a benchmarked size: Orszag-Tang 2048^2 split 2 x 2 (the default single-sweep solve,
+    decisions and CFL step on the device), 3 CFL steps against the single context on the same
+    dts: 1e-12 relative per field, the same products, |div B|_inf <= 1e-12."""
+    n = 2048
+    dx = m.problems.grid_spacing(n)
+    ic = m.problems.orszag_tang(n, n, dx, dx)
+    run, subs = _decomposed(m, n, n, dx, dx, 1e-4, 2, 2, ic)
+    ctx = m.Context(n, n, dx, dx, 1e-4)
+    ctx.set_state(ic)
+    for _ in range(3):
+        dt, prods = run.step()
+        assert abs(ctx.cfl_dt() - dt) <= 1e-14 * dt
+        ctx.step(dt)
+        ctx.synchronize()
+        assert tuple(prods) == tuple(ctx.last_cg_products())
+    assert run.status == "ok"
+    errs = [rel_linf(g, w, 1.0) for g, w in zip(run.get_state(), ctx.get_state())]
+    assert max(errs) <= 1e-12, errs
+    assert run.divb()[1] <= 1e-12
+    ctx.close()
+    run.close()
+    for s in subs:
+        s.close()
