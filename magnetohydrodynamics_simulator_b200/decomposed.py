@@ -782,6 +782,9 @@ class DecomposedRun:
         return int(c[CG_PRODUCTS])
 
     def _sweep_solve(self, index, g, own, slots, decide, graph, handles) -> int:
+        """The single-sweep form of _solve_device: the right-hand side sweep and decision 3,
+        then per iteration the sweep (reading the cells around each interior from the
+        neighbours in the graphs, from the exchanged rings otherwise) and decision 4."""
         ctl, maxp, tol = g.ctl, self.max_iters, self.tol
         for s, sl in zip(own, slots):
             s.cg_sweep_rhs_dev(index, sl)
